@@ -1,0 +1,104 @@
+"""Build oracle/_ref/libaxr_ref.so: the reference's own OpenCL C kernels for
+the rasterizer hot path, compiled for the CPU.  TEST INFRASTRUCTURE ONLY.
+
+The kernels are read where they lie in the reference checkout
+(PyOpenCL27C/Pipe/*.c, PyOpenCL27C/Shaders/*.c), passed through a small
+mechanical rewrite that maps OpenCL C syntax onto C++ (vector literals
+`(float3)(a, b, c)` -> `make_float3(a, b, c)`, address-space qualifiers,
+`__local` -> thread-local arrays the harness can preload), and piped into
+g++ on stdin, so no copy of the reference source is written anywhere.  Only
+object files and the shared library land in oracle/_ref/ (git-ignored).
+
+The harness (oracle/ref_harness.cpp) restates the host orchestration of
+PyOpenCL27C/Ops0.py (CLDraw.drawAll) and Ops.py (CLDraw.shadowMap) and runs
+each kernel work-item by work-item.
+
+Usage: python oracle/build_ref.py [--reference /path/to/AXI_Visualizer]
+Exit status 0 with a message when the reference checkout is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+LIB = os.path.join(OUT, "libaxr_ref.so")
+
+# (namespace, path inside the reference checkout)
+KERNELS = [
+    ("ref_trisetup", "PyOpenCL27C/Pipe/trisetup.c"),
+    ("ref_trisetup_cull", "PyOpenCL27C/Pipe/trisetup_cull.c"),
+    ("ref_trisetup_ortho", "PyOpenCL27C/Pipe/trisetupOrtho.c"),
+    ("ref_gather", "PyOpenCL27C/Pipe/gather.c"),
+    ("ref_coarse", "PyOpenCL27C/Pipe/coarse.c"),
+    ("ref_draw", "PyOpenCL27C/Shaders/drawtexcolsmp.c"),
+    ("ref_draw_alpha", "PyOpenCL27C/Shaders/drawtexcolsmpalpha.c"),
+    ("ref_drawmin", "PyOpenCL27C/Shaders/drawmin.c"),
+    ("ref_drawmin_alpha", "PyOpenCL27C/Shaders/drawminalpha.c"),
+    ("ref_clearzb", "PyOpenCL27C/Shaders/clearzb.c"),
+    ("ref_gamma", "PyOpenCL27C/Shaders/Post/gamma.c"),
+]
+
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+            "-fopenmp", "-w", "-DBLOCK_SIZE=128"]
+
+_VEC_LIT = re.compile(r"\((float|int|ushort|uchar)([234])\)\s*\(")
+_LOCAL_DECL = re.compile(r"__local\s+(\w+)\s+(\w+)\s*(\[[^\]]*\])?\s*;")
+
+
+def translate(src: str, ns: str) -> str:
+    """Mechanical OpenCL C -> C++ rewrite of one kernel file."""
+    locals_ = _LOCAL_DECL.findall(src)
+    body = _VEC_LIT.sub(lambda m: f"make_{m.group(1)}{m.group(2)}(", src)
+    body = _LOCAL_DECL.sub(lambda m: f"extern thread_local {m.group(1)} {m.group(2)}{m.group(3) or ''};", body)
+    body = re.sub(r"\b__kernel\b", "", body)
+    body = re.sub(r"\b__global\b", "", body)
+    body = re.sub(r"\b__constant\b", "", body)
+    defs = "".join(f"thread_local {t} {n}{dim};\n" for t, n, dim in locals_)
+    getters = ""
+    for t, n, dim in locals_:
+        getters += f"{t} *local_{n}() {{ return {'' if dim else '&'}{n}; }}\n"
+    return (f'#include "ref_shim.h"\nnamespace cl_shim {{ namespace {ns} {{\n'
+            f"{body}\n{defs}{getters}}} }}\n")
+
+
+def build(reference: str, verbose: bool = False) -> str | None:
+    if not os.path.isdir(os.path.join(reference, "PyOpenCL27C")):
+        print(f"build_ref: reference checkout not found at {reference}; skipped")
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    objs = []
+    for ns, rel in KERNELS:
+        path = os.path.join(reference, rel)
+        with open(path) as f:
+            src = translate(f.read(), ns)
+        obj = os.path.join(OUT, ns + ".o")
+        cmd = ["g++", *CXXFLAGS, "-I", HERE, "-x", "c++", "-c", "-", "-o", obj]
+        if verbose:
+            print(" ".join(cmd), "<", rel)
+        subprocess.run(cmd, input=src.encode(), check=True)
+        objs.append(obj)
+    harness = os.path.join(HERE, "ref_harness.cpp")
+    hobj = os.path.join(OUT, "ref_harness.o")
+    subprocess.run(["g++", *CXXFLAGS, "-I", HERE, "-c", harness, "-o", hobj], check=True)
+    subprocess.run(["g++", "-shared", "-fopenmp", "-o", LIB, hobj, *objs], check=True)
+    return LIB
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("AXR_REFERENCE", "/root/reference"))
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args()
+    lib = build(a.reference, a.verbose)
+    if lib:
+        print("built", lib)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

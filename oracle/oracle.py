@@ -1,0 +1,329 @@
+"""ctypes bindings for the CPU oracle (liboracle_axr.so) and for the
+reference kernels compiled for the CPU (oracle/_ref/libaxr_ref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py.  The product package never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle_axr.so")
+REF_SO = os.path.join(HERE, "_ref", "libaxr_ref.so")
+
+CFLAGS = ["-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-fopenmp"]
+
+
+def build_oracle(force: bool = False) -> str:
+    src = os.path.join(HERE, "axr_oracle.c")
+    if force or not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "axr_oracle.h"))):
+        subprocess.run(["gcc", *CFLAGS, "-o", ORACLE_SO, src, "-lm"], check=True)
+    return ORACLE_SO
+
+
+class OrcGroup(C.Structure):
+    _fields_ = [("ntris", C.c_int), ("xyz", C.c_void_p), ("vn", C.c_void_p), ("uv", C.c_void_p),
+                ("li", C.c_void_p), ("tr", C.c_void_p), ("tg", C.c_void_p), ("tb", C.c_void_p),
+                ("tex_size", C.c_int), ("flags", C.c_int), ("alpha_index", C.c_int), ("mip_bias", C.c_float)]
+
+
+class OrcAlpha(C.Structure):
+    _fields_ = [("mask", C.c_void_p), ("len", C.c_int)]
+
+
+class OrcShadow(C.Structure):
+    _fields_ = [("map", C.c_void_p), ("dim", C.c_int), ("scale", C.c_float),
+                ("pos", C.c_float * 3), ("vv", C.c_float * 9)]
+
+
+class OrcFrame(C.Structure):
+    _fields_ = [("w", C.c_int), ("h", C.c_int), ("pos", C.c_float * 3), ("vv", C.c_float * 9),
+                ("sscale", C.c_float), ("cax", C.c_float), ("cay", C.c_float),
+                ("lint", C.c_float * 3), ("ldir", C.c_float * 3), ("amb", C.c_float),
+                ("ro", C.c_void_p), ("go", C.c_void_p), ("bo", C.c_void_p), ("db", C.c_void_p),
+                ("tri_id", C.c_void_p), ("cov", C.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_draw_all.restype = C.c_int
+        L.orc_draw_all.argtypes = [C.POINTER(OrcFrame), C.POINTER(OrcGroup), C.c_int, C.c_void_p,
+                                   C.POINTER(OrcAlpha), C.c_int, C.POINTER(OrcShadow), C.c_int, C.c_int]
+        L.orc_shadow_map.restype = C.c_int
+        L.orc_shadow_map.argtypes = [C.POINTER(OrcShadow), C.POINTER(OrcGroup), C.c_int, C.c_void_p,
+                                     C.POINTER(OrcAlpha), C.c_int, C.c_float, C.c_int]
+        L.orc_clear_depth.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.orc_gamma.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float]
+        L.orc_setup_persp.argtypes = [C.POINTER(OrcGroup), C.POINTER(OrcFrame), C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_coarse_counts.restype = C.c_long
+        L.orc_coarse_counts.argtypes = [C.POINTER(OrcGroup), C.POINTER(OrcFrame), C.c_void_p]
+        L.orc_log2f.restype = C.c_float
+        L.orc_log2f.argtypes = [C.c_float]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None else None
+
+
+class Frame:
+    """Host framebuffers for one view (reference layout: u16 planes, f32 depth)."""
+
+    def __init__(self, w, h):
+        self.w, self.h = w, h
+        self.ro = np.ones((h, w), np.uint16)
+        self.go = np.ones((h, w), np.uint16)
+        self.bo = np.ones((h, w), np.uint16)
+        self.db = np.full((h, w), 65535.0, np.float32)
+        self.tri_id = np.full((h, w), -1, np.int32)
+        self.cov = np.zeros((h, w), np.uint8)
+
+
+def _groups(scene):
+    arr = (OrcGroup * len(scene.groups))()
+    keep = []
+    for k, g in enumerate(scene.groups):
+        r, gg, b = g.tex
+        keep += [g.xyz, g.vn, g.uv, g.li, r, gg, b]
+        arr[k] = OrcGroup(g.ntris, _ptr(g.xyz), _ptr(g.vn), _ptr(g.uv), _ptr(g.li), _ptr(r), _ptr(gg), _ptr(b),
+                          g.tex_size, g.flags, g.alpha_index, g.mip_bias)
+    return arr, keep
+
+
+def _alphas(scene):
+    n = max(1, len(scene.alphas))
+    arr = (OrcAlpha * n)()
+    keep = []
+    for k, (m, ln) in enumerate(scene.alphas):
+        m = np.ascontiguousarray(m, np.uint8)
+        keep.append(m)
+        arr[k] = OrcAlpha(_ptr(m), ln)
+    return arr, keep
+
+
+def _shadow_struct(sc, m):
+    s = OrcShadow()
+    s.map = _ptr(m)
+    s.dim = sc.dim
+    s.scale = sc.scale
+    s.pos[:] = [float(x) for x in sc.pos]
+    s.vv[:] = [float(x) for x in np.asarray(sc.vv, np.float32).reshape(-1)]
+    return s
+
+
+def new_shadow_map(dim):
+    return np.full((dim, dim), 65535.0, np.float32)
+
+
+def shadow_map(scene, k, smap, cast=None, nthreads=1):
+    """CLDraw.shadowMap(k, ...) on the oracle; smap is updated in place."""
+    L = lib()
+    sc = scene.shadows[k]
+    s = _shadow_struct(sc, smap)
+    g, keep = _groups(scene)
+    a, keep2 = _alphas(scene)
+    if cast is None:
+        cast = [gr.cast for gr in scene.groups]
+    cast = np.asarray(cast, np.uint8)
+    rc = L.orc_shadow_map(C.byref(s), g, len(scene.groups), _ptr(cast), a, len(scene.alphas),
+                          C.c_float(scene.bias), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"orc_shadow_map failed: {rc}")
+    return smap
+
+
+def _frame_struct(fr, view, scene):
+    f = OrcFrame()
+    f.w, f.h = view.w, view.h
+    f.pos[:] = [float(x) for x in view.pos]
+    f.vv[:] = [float(x) for x in np.asarray(view.vv, np.float32).reshape(-1)]
+    f.sscale, f.cax, f.cay = view.sscale, view.cax, view.cay
+    f.lint[:] = [float(x) for x in scene.lint]
+    f.ldir[:] = [float(x) for x in scene.ldir]
+    f.amb = scene.amb
+    f.ro, f.go, f.bo, f.db = _ptr(fr.ro), _ptr(fr.go), _ptr(fr.bo), _ptr(fr.db)
+    f.tri_id, f.cov = _ptr(fr.tri_id), _ptr(fr.cov)
+    return f
+
+
+def draw_all(scene, view, fr, smaps=(), mask=None, nthreads=1):
+    """CLDraw.drawAll on the oracle: updates `fr` (a Frame) in place."""
+    L = lib()
+    f = _frame_struct(fr, view, scene)
+    g, keep = _groups(scene)
+    a, keep2 = _alphas(scene)
+    n_sh = len(smaps)
+    sh = (OrcShadow * max(1, n_sh))()
+    for k in range(n_sh):
+        sh[k] = _shadow_struct(scene.shadows[k], smaps[k])
+    m = None if mask is None else np.asarray(mask, np.uint8)
+    rc = L.orc_draw_all(C.byref(f), g, len(scene.groups), _ptr(m), a, len(scene.alphas), sh, n_sh, nthreads)
+    if rc != 0:
+        raise RuntimeError(f"orc_draw_all failed: {rc}")
+    return fr
+
+
+def clear_depth(db, lenP=4):
+    h, w = db.shape
+    lib().orc_clear_depth(_ptr(db), w, h, lenP)
+
+
+def gamma(fr, exposure=1.0):
+    lib().orc_gamma(_ptr(fr.ro), _ptr(fr.go), _ptr(fr.bo), fr.w, fr.h, C.c_float(exposure))
+
+
+def render(scene, view, nthreads=1, with_shadows=True):
+    """Full frame on the oracle: shadow maps, clear, drawAll.  Returns
+    (Frame, shadow maps)."""
+    smaps = []
+    if with_shadows:
+        for k, sc in enumerate(scene.shadows):
+            m = new_shadow_map(sc.dim)
+            shadow_map(scene, k, m, nthreads=nthreads)
+            smaps.append(m)
+    fr = Frame(view.w, view.h)
+    clear_depth(fr.db)
+    draw_all(scene, view, fr, smaps, nthreads=nthreads)
+    return fr, smaps
+
+
+def setup_persp(scene, gi, view):
+    L = lib()
+    g, keep = _groups(scene)
+    fr = Frame(view.w, view.h)
+    f = _frame_struct(fr, view, scene)
+    n = scene.groups[gi].ntris
+    cls = np.zeros(n, np.uint8)
+    sp = np.zeros((n * 3, 2), np.float32)
+    zz = np.zeros(n * 3, np.float32)
+    L.orc_setup_persp(C.byref(g[gi]), C.byref(f), _ptr(cls), _ptr(sp), _ptr(zz))
+    return cls, sp, zz
+
+
+def coarse_counts(scene, gi, view):
+    L = lib()
+    g, keep = _groups(scene)
+    fr = Frame(view.w, view.h)
+    f = _frame_struct(fr, view, scene)
+    counts = np.zeros((view.h // 16) * (view.w // 16), np.int32)
+    total = L.orc_coarse_counts(C.byref(g[gi]), C.byref(f), _ptr(counts))
+    return total, counts
+
+
+# ---------------------------------------------------------------- reference kernels on the CPU
+
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        R = C.CDLL(REF_SO)
+        R.ref_create.restype = C.c_void_p
+        R.ref_create.argtypes = [C.c_int, C.c_int]
+        R.ref_destroy.argtypes = [C.c_void_p]
+        R.ref_add_group.restype = C.c_int
+        R.ref_add_group.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 3 + [C.c_long, C.c_int]
+        R.ref_add_alpha.restype = C.c_int
+        R.ref_add_alpha.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        R.ref_set_view.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float]
+        R.ref_set_light.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        R.ref_clear_zbuffer.argtypes = [C.c_void_p]
+        R.ref_set_depth.argtypes = [C.c_void_p, C.c_void_p]
+        R.ref_draw_all.restype = C.c_int
+        R.ref_draw_all.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        R.ref_get_frame.argtypes = [C.c_void_p] + [C.c_void_p] * 4
+        R.ref_set_frame.argtypes = [C.c_void_p] + [C.c_void_p] * 3
+        R.ref_add_shadow_map.restype = C.c_int
+        R.ref_add_shadow_map.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float]
+        R.ref_place_shadow_map.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        R.ref_clear_shadow_map.argtypes = [C.c_void_p, C.c_int]
+        R.ref_shadow_map.restype = C.c_int
+        R.ref_shadow_map.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_int]
+        R.ref_get_shadow_map.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        R.ref_gamma.argtypes = [C.c_void_p, C.c_float]
+        R.ref_overflow.restype = C.c_int
+        R.ref_overflow.argtypes = [C.c_void_p]
+        _ref = R
+    return _ref
+
+
+class RefDraw:
+    """The reference's CLDraw, run through its own kernels on the CPU."""
+
+    def __init__(self, scene, view):
+        self.R = ref_lib()
+        self.scene, self.view = scene, view
+        self.h = self.R.ref_create(view.w, view.h)
+        self._keep = []
+        for g in scene.groups:
+            r, gg, b = g.tex
+            self.R.ref_add_group(self.h, _ptr(g.xyz), _ptr(g.uv), _ptr(g.vn), _ptr(g.li), g.ntris,
+                                 _ptr(r), _ptr(gg), _ptr(b), r.size, g.tex_size)
+        for m, ln in scene.alphas:
+            m = np.ascontiguousarray(m, np.uint8)
+            self.R.ref_add_alpha(self.h, _ptr(m), ln)
+        pos = np.asarray(view.pos, np.float32)
+        vv = np.ascontiguousarray(view.vv, np.float32)
+        self.R.ref_set_view(self.h, _ptr(pos), _ptr(vv), view.sscale, view.cax, view.cay)
+        self.R.ref_set_light(self.h, _ptr(np.asarray(scene.lint, np.float32)), _ptr(np.asarray(scene.ldir, np.float32)))
+        self.flags = np.array([g.flags for g in scene.groups], np.int32)
+        self.aidx = np.array([g.alpha_index for g in scene.groups], np.int32)
+
+    def __del__(self):
+        try:
+            self.R.ref_destroy(self.h)
+        except Exception:
+            pass
+
+    def clear_zbuffer(self):
+        self.R.ref_clear_zbuffer(self.h)
+
+    def draw_all(self, mask=None, nthreads=1):
+        m = None if mask is None else np.asarray(mask, np.uint8)
+        rc = self.R.ref_draw_all(self.h, _ptr(self.flags), _ptr(self.aidx), _ptr(m), len(self.flags), nthreads)
+        return rc
+
+    def get_frame(self):
+        w, h = self.view.w, self.view.h
+        r = np.empty((h, w), np.uint16); g = np.empty((h, w), np.uint16); b = np.empty((h, w), np.uint16)
+        db = np.empty((h, w), np.float32)
+        self.R.ref_get_frame(self.h, _ptr(r), _ptr(g), _ptr(b), _ptr(db))
+        return r, g, b, db
+
+    def shadow_map(self, k, cast=None, nthreads=1):
+        sc = self.scene.shadows[k]
+        self.R.ref_add_shadow_map(self.h, k, sc.dim, sc.scale)
+        self.R.ref_place_shadow_map(self.h, k, _ptr(np.asarray(sc.pos, np.float32)),
+                                    _ptr(np.ascontiguousarray(sc.vv, np.float32)))
+        self.R.ref_clear_shadow_map(self.h, k)
+        if cast is None:
+            cast = [g.cast for g in self.scene.groups]
+        cast = np.asarray(cast, np.uint8)
+        rc = self.R.ref_shadow_map(self.h, k, _ptr(cast), _ptr(self.flags), _ptr(self.aidx), len(self.flags),
+                                   self.scene.bias, nthreads)
+        out = np.empty((sc.dim, sc.dim), np.float32)
+        self.R.ref_get_shadow_map(self.h, k, _ptr(out))
+        return rc, out
+
+    def gamma(self, ex=1.0):
+        self.R.ref_gamma(self.h, ex)

@@ -1,0 +1,438 @@
+// ref_harness.cpp -- host side of oracle/_ref (TEST INFRASTRUCTURE ONLY).
+//
+// Restates the host orchestration of the reference's CLDraw
+// (PyOpenCL27C/Ops0.py:93-910, drawAll at :471-648; shadowMap in
+// PyOpenCL27C/Ops.py:1089-1141) with the reference's device buffer layouts
+// (float3 as 16 bytes, SP/ZZ/TIA/TIB/TNA/TNB/TOA/TOB/IBUF/NBUF/AL), and runs
+// the reference's own kernels (compiled by build_ref.py) one work-item at a
+// time.  Serial mode (nthreads == 1) runs work-groups in order and work-items
+// in id order, which is the canonical semantics the oracle restates; the only
+// adjustment is that a tile's local depth copy is loaded before the tile's
+// first triangle, and that the bin count the tile kernel resets at its end is
+// seen by all of its work-items.  Threaded mode runs one work-group per
+// OpenMP thread (used only for timing).
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include <omp.h>
+#include "ref_shim.h"
+
+namespace cl_shim {
+thread_local int g_group[2];
+thread_local int g_local[2];
+
+namespace ref_trisetup {
+void setup(float3 *XYZ, float3 *VN, int *TIA, int *TIB, int *TNA, int *TNB, float2 *XY, float *ZZ,
+           float *Vpos, float3 *VV, const float sScale, const int wF, const int hF, const float cAX,
+           const float cAY, const int lenP);
+}
+namespace ref_trisetup_cull {
+void setup(float3 *XYZ, float3 *VN, int *TIA, int *TIB, int *TNA, int *TNB, float2 *XY, float *ZZ,
+           float *Vpos, float3 *VV, const float sScale, const int wF, const int hF, const float cAX,
+           const float cAY, const int lenP);
+}
+namespace ref_trisetup_ortho {
+void setup(float3 *XYZ, int *TI, int *TN, int2 *XY, float *ZZ, float *Vpos, float3 *VV, const float shBias,
+           const float sScale, const int wF, const int hF, const float cAX, const float cAY, const int lenP);
+}
+namespace ref_gather {
+void setup(int *TI, int *TN, int *TO, int *AL, const int tn, const int numBlocks);
+}
+namespace ref_coarse {
+void draw(int *TO, int *F, int *FN, float2 *P, int wF, int hF, int lenP);
+}
+namespace ref_draw {
+void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+          float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, ushort *TR, ushort *TG, ushort *TB,
+          const int lenT, const int wF, const int hF);
+void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+               float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, ushort *TR, ushort *TG,
+               ushort *TB, const int lenT, const int wF, const int hF, const int lenP);
+float *local_ZBuf();
+}
+namespace ref_draw_alpha {
+void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+          float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, ushort *TR, ushort *TG, ushort *TB,
+          const int lenT, bool *TA, const int wF, const int hF);
+void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+               float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, ushort *TR, ushort *TG,
+               ushort *TB, const int lenT, bool *TA, const int wF, const int hF, const int lenP);
+float *local_ZBuf();
+}
+namespace ref_drawmin {
+void draw(int *TO, float *F, int2 *P, float *Z, int wF, int hF, int lenP);
+}
+namespace ref_drawmin_alpha {
+void draw(int *TO, float *F, int2 *P, float *Z, float2 *UV, bool *TA, int lenT, int wF, int hF, int lenP);
+}
+namespace ref_clearzb {
+void clearFrame(float *F, const int wF, const int hF, const int BS, const int lenP);
+}
+namespace ref_gamma {
+void g(ushort *Ro, ushort *Go, ushort *Bo, const float exposure, const int wF, const int hF, const int BS,
+       const int stepW, const int stepH);
+}
+}  // namespace cl_shim
+
+using namespace cl_shim;
+
+static const int BS = 128;      // BLOCK_SIZE = TILE_BUF (Ops0.py:19-21)
+static const int TILE_BUF = 128;
+
+namespace {
+
+struct Group {
+  int V = 0, T = 0;
+  std::vector<float3> xyz, vn, li;
+  std::vector<float2> uv, sp;
+  std::vector<float> zz;
+  std::vector<int> tia, tib, tna, tnb, toa, tob;
+  std::vector<ushort> tr, tg, tb;
+  int tex_size = 0;
+};
+
+struct Shadow {
+  std::vector<float> map;
+  int dim = 0;
+  float scale = 1;
+  float pos[3] = {0, 0, 0};
+  float3 vec[3];
+};
+
+struct Ctx {
+  int W, H, WC, HC;
+  std::vector<Group> groups;
+  std::vector<std::vector<uint8_t>> alphas;
+  std::vector<int> alpha_len;
+  std::vector<ushort> ro, go, bo;
+  std::vector<float> db;
+  std::vector<int> ibuf, nbuf, al;
+  float vpos[3] = {0, 0, 0};
+  float3 vmat[3];
+  float sscale = 1, cax = 1, cay = 1;
+  float3 lint[1], ldir[1];
+  Shadow shadows[8];
+  int overflow = 0;
+};
+
+// run kernel `fn(bx, tx)` over a 1-D grid of `ng` groups of BS items
+template <class F>
+void grid1(int ng, int nthreads, F fn) {
+  if (nthreads <= 1) {
+    for (int bx = 0; bx < ng; bx++) {
+      g_group[0] = bx; g_group[1] = 0;
+      for (int tx = 0; tx < BS; tx++) {
+        g_local[0] = tx; g_local[1] = 0;
+        fn(bx, tx);
+      }
+    }
+  } else {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int bx = 0; bx < ng; bx++) {
+      g_group[0] = bx; g_group[1] = 0;
+      for (int tx = 0; tx < BS; tx++) {
+        g_local[0] = tx; g_local[1] = 0;
+        fn(bx, tx);
+      }
+    }
+  }
+}
+
+float3 f3(const float *p) { return make_float3(p[0], p[1], p[2]); }
+
+}  // namespace
+
+extern "C" {
+
+void *ref_create(int w, int h) {
+  Ctx *c = new Ctx();
+  c->W = w; c->H = h; c->WC = w / 16; c->HC = h / 16;
+  c->ro.assign((size_t)w * h, 1); c->go.assign((size_t)w * h, 1); c->bo.assign((size_t)w * h, 1);
+  c->db.assign((size_t)w * h, 65535.f);
+  c->ibuf.assign((size_t)c->WC * c->HC * TILE_BUF + TILE_BUF * 64, -1);
+  c->nbuf.assign((size_t)c->WC * c->HC, 0);
+  c->al.assign(64, 0);
+  return c;
+}
+
+void ref_destroy(void *h) { delete (Ctx *)h; }
+
+// CLDraw.addTextureGroup (Ops0.py:276-322) plus the LI buffer vertLight fills
+int ref_add_group(void *h, const float *xyz, const float *uv, const float *vn, const float *li, int ntris,
+                  const uint16_t *r, const uint16_t *g, const uint16_t *b, long ntexels, int tex_size) {
+  Ctx *c = (Ctx *)h;
+  Group G;
+  G.T = ntris; G.V = ntris * 3;
+  G.xyz.resize(G.V); G.vn.resize(G.V); G.li.resize(G.V); G.uv.resize(G.V);
+  for (int v = 0; v < G.V; v++) {
+    G.xyz[v] = f3(xyz + 3 * (size_t)v);
+    G.vn[v] = f3(vn + 3 * (size_t)v);
+    G.li[v] = f3(li + 3 * (size_t)v);
+    G.uv[v] = make_float2(uv[2 * (size_t)v], uv[2 * (size_t)v + 1]);
+  }
+  G.sp.assign(G.V, make_float2(0, 0));
+  G.zz.assign(G.V, 0);
+  int gs = G.T / BS + 1;
+  G.tia.assign((size_t)gs * BS, 0); G.tib.assign((size_t)gs * BS, 0);
+  G.tna.assign(gs, 0); G.tnb.assign(gs, 0);
+  G.toa.assign((size_t)gs * BS, 0); G.tob.assign((size_t)gs * BS, 0);
+  G.tr.assign(r, r + ntexels); G.tg.assign(g, g + ntexels); G.tb.assign(b, b + ntexels);
+  G.tex_size = tex_size;
+  c->groups.push_back(std::move(G));
+  return (int)c->groups.size() - 1;
+}
+
+int ref_add_alpha(void *h, const uint8_t *mask, int len) {
+  Ctx *c = (Ctx *)h;
+  c->alphas.emplace_back(mask, mask + (size_t)len * len);
+  c->alpha_len.push_back(len);
+  return (int)c->alphas.size() - 1;
+}
+
+void ref_set_view(void *h, const float *pos, const float *vv, float sscale, float cax, float cay) {
+  Ctx *c = (Ctx *)h;
+  for (int i = 0; i < 3; i++) c->vpos[i] = pos[i];
+  for (int i = 0; i < 3; i++) c->vmat[i] = f3(vv + 3 * i);
+  c->sscale = sscale; c->cax = cax; c->cay = cay;
+}
+
+void ref_set_light(void *h, const float *lint, const float *ldir) {
+  Ctx *c = (Ctx *)h;
+  c->lint[0] = f3(lint);
+  c->ldir[0] = f3(ldir);
+}
+
+// clearZBuffer: clearzb.clearFrame over a 2x2 grid of 2x2 work-items (Ops0.py:650-653)
+void ref_clear_zbuffer(void *h) {
+  Ctx *c = (Ctx *)h;
+  const int s = 2, t = 2;
+  for (int by = 0; by < s; by++)
+    for (int bx = 0; bx < s; bx++)
+      for (int ty = 0; ty < t; ty++)
+        for (int tx = 0; tx < t; tx++) {
+          g_group[0] = bx; g_group[1] = by; g_local[0] = tx; g_local[1] = ty;
+          ref_clearzb::clearFrame(c->db.data(), c->W, c->H, t, s * t);
+        }
+}
+
+void ref_set_depth(void *h, const float *db) {
+  Ctx *c = (Ctx *)h;
+  memcpy(c->db.data(), db, sizeof(float) * c->db.size());
+}
+
+// CLDraw.drawAll (Ops0.py:471-648): flags bit 1 = alpha, bit 3 = cull
+int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_t *mask, int n, int nthreads) {
+  Ctx *c = (Ctx *)h;
+  int ng = (int)c->groups.size();
+  if (n != ng) return -1;
+  c->overflow = 0;
+  std::vector<int> gsn(ng, 0);
+  for (int tn = 0; tn < ng; tn++) {
+    if (mask && mask[tn]) continue;
+    Group &G = c->groups[tn];
+    int gs = G.T / BS + 1;
+    gsn[tn] = gs;
+    bool cull = (flags[tn] & 8) != 0;
+    grid1(gs, nthreads, [&](int, int) {
+      if (cull)
+        ref_trisetup_cull::setup(G.xyz.data(), G.vn.data(), G.tia.data(), G.tib.data(), G.tna.data(),
+                                 G.tnb.data(), G.sp.data(), G.zz.data(), c->vpos, c->vmat, c->sscale, c->W,
+                                 c->H, c->cax, c->cay, G.T);
+      else
+        ref_trisetup::setup(G.xyz.data(), G.vn.data(), G.tia.data(), G.tib.data(), G.tna.data(), G.tnb.data(),
+                            G.sp.data(), G.zz.data(), c->vpos, c->vmat, c->sscale, c->W, c->H, c->cax, c->cay,
+                            G.T);
+    });
+  }
+  // small
+  for (int tn = 0; tn < ng; tn++) {
+    if (mask && mask[tn]) continue;
+    Group &G = c->groups[tn];
+    grid1(gsn[tn], 1, [&](int, int) {
+      ref_gather::setup(G.tia.data(), G.tna.data(), G.toa.data(), c->al.data(), tn, gsn[tn]);
+    });
+  }
+  std::vector<int> newSize(c->al.begin(), c->al.end());
+  for (int tn = 0; tn < ng; tn++) {
+    if (mask && mask[tn]) continue;
+    Group &G = c->groups[tn];
+    int ns = newSize[tn] / BS + 1;
+    if (newSize[tn] <= 0) continue;
+    bool alpha = (flags[tn] & 2) != 0;
+    bool *TA = alpha ? (bool *)c->alphas[alpha_index[tn]].data() : nullptr;
+    grid1(ns, nthreads, [&](int, int) {
+      if (alpha)
+        ref_draw_alpha::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(),
+                                  G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(),
+                                  c->lint, c->ldir, G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, TA, c->W,
+                                  c->H, newSize[tn]);
+      else
+        ref_draw::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(), G.sp.data(),
+                            G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), c->lint, c->ldir,
+                            G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, c->W, c->H, newSize[tn]);
+    });
+  }
+  // large
+  for (int tn = 0; tn < ng; tn++) {
+    if (mask && mask[tn]) continue;
+    Group &G = c->groups[tn];
+    grid1(gsn[tn], 1, [&](int, int) {
+      ref_gather::setup(G.tib.data(), G.tnb.data(), G.tob.data(), c->al.data(), tn, gsn[tn]);
+    });
+  }
+  newSize.assign(c->al.begin(), c->al.end());
+  for (int tn = 0; tn < ng; tn++) {
+    if (mask && mask[tn]) continue;
+    Group &G = c->groups[tn];
+    if (newSize[tn] <= 0) continue;
+    int ns = newSize[tn] / BS + 1;
+    grid1(ns, nthreads, [&](int, int) {
+      ref_coarse::draw(G.tob.data(), c->ibuf.data(), c->nbuf.data(), G.sp.data(), c->WC, c->HC, newSize[tn]);
+    });
+    for (int t = 0; t < c->WC * c->HC; t++)
+      if (c->nbuf[t] > TILE_BUF) c->overflow = 1;
+    if (c->overflow) return -2;  // the reference's bins overflow: result undefined
+    bool alpha = (flags[tn] & 2) != 0;
+    bool *TA = alpha ? (bool *)c->alphas[alpha_index[tn]].data() : nullptr;
+    int ntiles = c->WC * c->HC;
+    auto tile = [&](int bx) {
+      float *zb = alpha ? ref_draw_alpha::local_ZBuf() : ref_draw::local_ZBuf();
+      int tileX = bx % c->WC, tileY = bx / c->WC;
+      for (int r = 0; r < 16; r++)
+        for (int i = 0; i < 16; i++) zb[r * 16 + i] = c->db[(size_t)c->W * (tileY * 16 + r) + tileX * 16 + i];
+      int nb = c->nbuf[bx];
+      g_group[0] = bx; g_group[1] = 0;
+      for (int tx = 0; tx < BS; tx++) {
+        c->nbuf[bx] = nb;
+        g_local[0] = tx; g_local[1] = 0;
+        if (alpha)
+          ref_draw_alpha::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
+                               c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),
+                               G.xyz.data(), c->lint, c->ldir, G.tr.data(), G.tg.data(), G.tb.data(),
+                               G.tex_size, TA, c->W, c->H);
+        else
+          ref_draw::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(),
+                         G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), c->lint,
+                         c->ldir, G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, c->W, c->H);
+      }
+      c->nbuf[bx] = 0;  // what work-item 0 leaves behind (Templates.py:188)
+    };
+    if (nthreads <= 1) {
+      for (int bx = 0; bx < ntiles; bx++) tile(bx);
+    } else {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+      for (int bx = 0; bx < ntiles; bx++) tile(bx);
+    }
+  }
+  return 0;
+}
+
+void ref_get_frame(void *h, uint16_t *r, uint16_t *g, uint16_t *b, float *db) {
+  Ctx *c = (Ctx *)h;
+  size_t n = (size_t)c->W * c->H;
+  memcpy(r, c->ro.data(), n * 2); memcpy(g, c->go.data(), n * 2); memcpy(b, c->bo.data(), n * 2);
+  memcpy(db, c->db.data(), n * 4);
+}
+
+void ref_set_frame(void *h, const uint16_t *r, const uint16_t *g, const uint16_t *b) {
+  Ctx *c = (Ctx *)h;
+  size_t n = (size_t)c->W * c->H;
+  memcpy(c->ro.data(), r, n * 2); memcpy(c->go.data(), g, n * 2); memcpy(c->bo.data(), b, n * 2);
+}
+
+// addShadowMap / placeShadowMap / clearShadowMap (Ops.py:1031-1087)
+int ref_add_shadow_map(void *h, int i, int size, float scale) {
+  Ctx *c = (Ctx *)h;
+  if (i < 0 || i >= 8) return -1;
+  Shadow &s = c->shadows[i];
+  s.map.assign((size_t)size * size, 65535.f);
+  s.dim = size; s.scale = scale;
+  return 0;
+}
+
+void ref_place_shadow_map(void *h, int i, const float *pos, const float *vv) {
+  Ctx *c = (Ctx *)h;
+  Shadow &s = c->shadows[i];
+  for (int k = 0; k < 3; k++) s.pos[k] = pos[k];
+  for (int k = 0; k < 3; k++) s.vec[k] = f3(vv + 3 * k);
+}
+
+void ref_clear_shadow_map(void *h, int i) {
+  Ctx *c = (Ctx *)h;
+  Shadow &s = c->shadows[i];
+  const int sg = 4, t = 4;
+  for (int by = 0; by < sg; by++)
+    for (int bx = 0; bx < sg; bx++)
+      for (int ty = 0; ty < t; ty++)
+        for (int tx = 0; tx < t; tx++) {
+          g_group[0] = bx; g_group[1] = by; g_local[0] = tx; g_local[1] = ty;
+          ref_clearzb::clearFrame(s.map.data(), s.dim, s.dim, t, sg * t);
+        }
+}
+
+// CLDraw.shadowMap (Ops.py:1089-1141)
+int ref_shadow_map(void *h, int i, const uint8_t *cast, const int *flags, const int *alpha_index, int n,
+                   float bias, int nthreads) {
+  Ctx *c = (Ctx *)h;
+  Shadow &s = c->shadows[i];
+  int ng = (int)c->groups.size();
+  if (n != ng) return -1;
+  std::vector<int> tsn, gsn;
+  for (int tn = 0; tn < ng; tn++) {
+    if (!cast[tn]) continue;
+    Group &G = c->groups[tn];
+    int gs = G.T / BS + 1;
+    tsn.push_back(tn); gsn.push_back(gs);
+    grid1(gs, nthreads, [&](int, int) {
+      ref_trisetup_ortho::setup(G.xyz.data(), G.tia.data(), G.tna.data(), (int2 *)G.sp.data(), G.zz.data(),
+                                s.pos, s.vec, bias, s.scale, s.dim, s.dim, c->cax, c->cay, G.T);
+    });
+  }
+  for (size_t k = 0; k < tsn.size(); k++) {
+    Group &G = c->groups[tsn[k]];
+    int gs = gsn[k];
+    int tn = tsn[k];
+    grid1(gs, 1, [&](int, int) { ref_gather::setup(G.tia.data(), G.tna.data(), G.toa.data(), c->al.data(), tn, gs); });
+  }
+  std::vector<int> newSize(c->al.begin(), c->al.end());
+  for (size_t k = 0; k < tsn.size(); k++) {
+    int tn = tsn[k];
+    Group &G = c->groups[tn];
+    if (newSize[tn] <= 0) continue;
+    int ns = newSize[tn] / BS + 1;
+    bool alpha = (flags[tn] & 2) != 0;
+    grid1(ns, nthreads, [&](int, int) {
+      if (!alpha)
+        ref_drawmin::draw(G.toa.data(), s.map.data(), (int2 *)G.sp.data(), G.zz.data(), s.dim, s.dim, newSize[tn]);
+      else
+        ref_drawmin_alpha::draw(G.toa.data(), s.map.data(), (int2 *)G.sp.data(), G.zz.data(), G.uv.data(),
+                                (bool *)c->alphas[alpha_index[tn]].data(), c->alpha_len[alpha_index[tn]], s.dim,
+                                s.dim, newSize[tn]);
+    });
+  }
+  return 0;
+}
+
+void ref_get_shadow_map(void *h, int i, float *out) {
+  Ctx *c = (Ctx *)h;
+  memcpy(out, c->shadows[i].map.data(), sizeof(float) * c->shadows[i].map.size());
+}
+
+// CLDraw.gamma (Ops0.py:654-660): 4x4 groups of 4x4 items
+void ref_gamma(void *h, float ex) {
+  Ctx *c = (Ctx *)h;
+  const int s = 4, t = 4;
+  int stepH = (c->H + s * t - 1) / (s * t);
+  for (int by = 0; by < s; by++)
+    for (int bx = 0; bx < s; bx++)
+      for (int ty = 0; ty < t; ty++)
+        for (int tx = 0; tx < t; tx++) {
+          g_group[0] = bx; g_group[1] = by; g_local[0] = tx; g_local[1] = ty;
+          ref_gamma::g(c->ro.data(), c->go.data(), c->bo.data(), ex, c->W, c->H, t, s * t, stepH);
+        }
+}
+
+int ref_overflow(void *h) { return ((Ctx *)h)->overflow; }
+
+}  // extern "C"
