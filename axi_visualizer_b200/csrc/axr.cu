@@ -1,0 +1,638 @@
+// axr.cu -- libaxr.so: handle, device memory and the C ABI of include/axr.h.
+//
+// Layout in HBM per handle: framebuffers as the reference keeps them (three
+// uint16 planes and a float depth plane, [h][w]) plus one 64-bit visibility
+// word per pixel; per material group the vertex streams (xyz, normal, uv,
+// light I as packed float triplets/pairs, 3 vertices per triangle) and the
+// texture planes (mip chain smallest level first); work queues sized by the
+// triangle count (small/large lists) and a grow-only tile-unit queue.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/axr.h"
+#include "kernels.cuh"
+
+using namespace axr;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(x)                                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = (x);                                                              \
+    if (e_ != cudaSuccess) return fail(AXR_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+struct Group {
+  float *xyz = nullptr, *vn = nullptr, *uv = nullptr, *li = nullptr;
+  uint16_t *tr = nullptr, *tg = nullptr, *tb = nullptr;
+  int ntris = 0, tri_base = 0, tex_size = 0, mip_side = 0;
+  long ntexels = 0;
+};
+
+struct Alpha {
+  uint8_t *mask = nullptr;
+  int side = 0;
+};
+
+struct Shadow {
+  float *map = nullptr;
+  int dim = 0;
+  float scale = 1;
+  float pos[3] = {0, 0, 0};
+  float vv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+};
+
+constexpr int MAX_GROUPS = 64;
+constexpr int MAX_SHADOWS = 16;
+
+}  // namespace
+
+struct axr_ctx {
+  int device = 0, w = 0, h = 0, sms = 148;
+  cudaStream_t stream = nullptr;
+  std::vector<Group> groups;
+  std::vector<Alpha> alphas;
+  int total_tris = 0;
+  float sscale = 1, cax = 1, cay = 1;
+  float pos[3] = {0, 0, 0};
+  float vm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  float lint[3] = {1, 1, 1}, ldir[3] = {0, -1, 0};
+  float amb = 0.2f;
+  uint16_t *ro = nullptr, *go = nullptr, *bo = nullptr;
+  float *db = nullptr;
+  uint64_t *keys = nullptr;
+  uint32_t *small_list = nullptr, *large_list = nullptr, *sh_list = nullptr;
+  uint32_t cap_list = 0;
+  uint2 *units = nullptr;
+  uint32_t cap_units = 0;
+  uint32_t *ctr = nullptr;
+  uint32_t *h_ctr = nullptr;  // pinned copy of the counters of the last drawAll
+  GroupDev *d_groups = nullptr;
+  Shadow shadows[MAX_SHADOWS];
+  int64_t last_kernels = 0;
+  bool pending = false;
+};
+
+namespace {
+
+int ensure_lists(axr_ctx *c) {
+  uint32_t need = (uint32_t)std::max(c->total_tris, 1);
+  if (need <= c->cap_list) return 0;
+  uint32_t cap = std::max(need, c->cap_list * 2);
+  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->sh_list);
+  c->small_list = c->large_list = c->sh_list = nullptr;
+  if (cudaMalloc(&c->small_list, sizeof(uint32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&c->large_list, sizeof(uint32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&c->sh_list, sizeof(uint32_t) * cap) != cudaSuccess)
+    return fail(AXR_ENOMEM, "triangle lists of %u entries", cap);
+  c->cap_list = cap;
+  return 0;
+}
+
+int grow_units(axr_ctx *c, uint32_t need) {
+  if (need <= c->cap_units) return 0;
+  uint64_t cap = std::max<uint64_t>((uint64_t)need + need / 4, (uint64_t)c->cap_units * 2);
+  if (cap > 0x7fffffffull) cap = 0x7fffffffull;
+  cudaFree(c->units);
+  c->units = nullptr;
+  if (cudaMalloc(&c->units, sizeof(uint2) * cap) != cudaSuccess)
+    return fail(AXR_ENOMEM, "tile-unit queue of %llu entries", (unsigned long long)cap);
+  c->cap_units = (uint32_t)cap;
+  return 0;
+}
+
+// Reads the counters of the last drawAll; grows the unit queue after an
+// overflow (that frame was completed by the fallback kernel).
+int settle(axr_ctx *c) {
+  if (!c->pending) return 0;
+  CK(cudaStreamSynchronize(c->stream));
+  c->pending = false;
+  if (c->h_ctr[CTR_OVERFLOW]) return grow_units(c, c->h_ctr[CTR_UNITS]);
+  return 0;
+}
+
+int check_ctx(axr_ctx *c) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  CK(cudaSetDevice(c->device));
+  return 0;
+}
+
+template <class T>
+int upload(axr_ctx *c, T **dst, const T *src, size_t n) {
+  if (cudaMalloc(dst, sizeof(T) * std::max<size_t>(n, 1)) != cudaSuccess)
+    return fail(AXR_ENOMEM, "device allocation of %zu bytes", sizeof(T) * n);
+  if (n) CK(cudaMemcpyAsync(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+bool is_pow2(long v) { return v > 0 && (v & (v - 1)) == 0; }
+
+ViewDev make_view(const axr_ctx *c) {
+  ViewDev v;
+  v.w = c->w; v.h = c->h;
+  memcpy(v.pos, c->pos, sizeof v.pos);
+  memcpy(v.vv, c->vm, sizeof v.vv);
+  v.sscale = c->sscale; v.cax = c->cax; v.cay = c->cay;
+  return v;
+}
+
+int grid_for(axr_ctx *c, long n, int block, int per_sm) {
+  long g = (n + block - 1) / block;
+  long cap = (long)c->sms * per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// Builds the per-call group table on the device.
+int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *enabled_mask,
+                  bool mask_means_enabled, int ngroups) {
+  GroupDev tab[MAX_GROUPS];
+  memset(tab, 0, sizeof tab);
+  for (int g = 0; g < ngroups; g++) {
+    const Group &G = c->groups[g];
+    GroupDev &d = tab[g];
+    d.xyz = G.xyz; d.vn = G.vn; d.uv = G.uv; d.li = G.li;
+    d.tr = G.tr; d.tg = G.tg; d.tb = G.tb;
+    d.ntris = G.ntris; d.tri_base = G.tri_base; d.tex_size = G.tex_size;
+    d.flags = flags ? flags[g] : 0;
+    d.mip_bias = 0.f;
+    bool on = true;
+    if (enabled_mask) on = mask_means_enabled ? enabled_mask[g] != 0 : enabled_mask[g] == 0;
+    d.enabled = on ? 1 : 0;
+    if ((d.flags & F_MIP) && G.mip_side == 0)
+      return fail(AXR_EINVAL, "group %d: mip flag on a group added without a mip chain", g);
+    if (!(d.flags & F_MIP) && G.mip_side != 0)
+      return fail(AXR_EINVAL, "group %d: group has a mip chain but the mip flag is not set", g);
+    if (d.flags & F_ALPHA) {
+      int ai = alpha_index ? alpha_index[g] : 0;
+      if (ai < 0 || ai >= (int)c->alphas.size())
+        return fail(AXR_EINVAL, "group %d: alpha index %d out of range (%zu masks)", g, ai, c->alphas.size());
+      int base_len = (d.flags & F_MIP) ? (1 << G.tex_size) : G.tex_size;
+      if (c->alphas[ai].side != base_len)
+        return fail(AXR_EINVAL, "group %d: alpha mask side %d differs from texture side %d", g, c->alphas[ai].side,
+                    base_len);
+      d.amask = c->alphas[ai].mask;
+      d.alen = c->alphas[ai].side;
+    }
+  }
+  CK(cudaMemcpyAsync(c->d_groups, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *axr_last_error(void) { return g_err.c_str(); }
+
+int axr_create(int w, int h, int device, axr_ctx **out) {
+  if (!out) return fail(AXR_EINVAL, "out is null");
+  *out = nullptr;
+  if (w <= 0 || h <= 0 || w % TILE != 0) return fail(AXR_EINVAL, "framebuffer %dx%d: width must be a positive multiple of 16", w, h);
+  if ((long)w * h > (1L << 28)) return fail(AXR_EINVAL, "framebuffer %dx%d too large", w, h);
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(AXR_EINVAL, "device %d of %d", device, ndev);
+  CK(cudaSetDevice(device));
+  axr_ctx *c = new axr_ctx();
+  c->device = device; c->w = w; c->h = h;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  size_t n = (size_t)w * h;
+  int rc = 0;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->ro, n * 2) != cudaSuccess || cudaMalloc(&c->go, n * 2) != cudaSuccess ||
+      cudaMalloc(&c->bo, n * 2) != cudaSuccess || cudaMalloc(&c->db, n * 4) != cudaSuccess ||
+      cudaMalloc(&c->keys, n * 8) != cudaSuccess || cudaMalloc(&c->ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
+      cudaMalloc(&c->d_groups, sizeof(GroupDev) * MAX_GROUPS) != cudaSuccess ||
+      cudaMallocHost(&c->h_ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess) {
+    rc = fail(AXR_ENOMEM, "framebuffers for %dx%d", w, h);
+  }
+  if (!rc) rc = grow_units(c, 1u << 22);
+  if (rc) {
+    axr_destroy(c);
+    return rc;
+  }
+  // reference initial state: colour planes of ones (Ops0.py:111-113), depth cleared
+  std::vector<uint16_t> ones(n, 1);
+  cudaMemcpyAsync(c->ro, ones.data(), n * 2, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(c->go, ones.data(), n * 2, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(c->bo, ones.data(), n * 2, cudaMemcpyHostToDevice, c->stream);
+  k_clear_depth<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(c->db, w, h, 1);
+  cudaMemsetAsync(c->keys, 0xff, n * 8, c->stream);
+  cudaMemsetAsync(c->ctr, 0, sizeof(uint32_t) * CTR_N, c->stream);
+  memset(c->h_ctr, 0, sizeof(uint32_t) * CTR_N);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    axr_destroy(c);
+    return fail(AXR_ECUDA, "initialising framebuffers");
+  }
+  *out = c;
+  return 0;
+}
+
+int axr_destroy(axr_ctx *c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &g : c->groups) {
+    cudaFree(g.xyz); cudaFree(g.vn); cudaFree(g.uv); cudaFree(g.li);
+    cudaFree(g.tr); cudaFree(g.tg); cudaFree(g.tb);
+  }
+  for (auto &a : c->alphas) cudaFree(a.mask);
+  for (auto &s : c->shadows) cudaFree(s.map);
+  cudaFree(c->ro); cudaFree(c->go); cudaFree(c->bo); cudaFree(c->db); cudaFree(c->keys);
+  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->sh_list); cudaFree(c->units);
+  cudaFree(c->ctr); cudaFree(c->d_groups);
+  if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int axr_set_scale_cull(axr_ctx *c, float s, float cax, float cay) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  c->sscale = s; c->cax = cax; c->cay = cay;
+  return 0;
+}
+
+int axr_add_texture_group(axr_ctx *c, const float *xyz, const float *uv, const float *vn, int ntris,
+                          const uint16_t *r, const uint16_t *g, const uint16_t *b, long ntexels, int mip_side,
+                          int *out_id) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!xyz || !uv || !vn || !r || !g || !b || ntris < 0) return fail(AXR_EINVAL, "null input or negative count");
+  if ((int)c->groups.size() >= MAX_GROUPS) return fail(AXR_EINVAL, "at most %d groups", MAX_GROUPS);
+  if ((long)c->total_tris + ntris >= (1L << 30) - 1) return fail(AXR_EINVAL, "more than 2^30 triangles");
+  Group G;
+  G.ntris = ntris;
+  G.tri_base = c->total_tris;
+  G.ntexels = ntexels;
+  G.mip_side = mip_side;
+  if (mip_side > 0) {
+    if (!is_pow2(mip_side)) return fail(AXR_EINVAL, "mip side %d is not a power of two", mip_side);
+    long need = ((long)mip_side * mip_side * 4 - 1) / 3;
+    if (ntexels != need) return fail(AXR_EINVAL, "mip chain of side %d needs %ld texels, got %ld", mip_side, need, ntexels);
+    int lg = 0;
+    while ((1 << lg) < mip_side) lg++;
+    G.tex_size = lg;
+    if (lg < 1) return fail(AXR_EINVAL, "mip side must be at least 2");
+  } else {
+    long side = 1;
+    while (side * side < ntexels) side++;
+    if (side * side != ntexels || !is_pow2(side)) return fail(AXR_EINVAL, "texture of %ld texels is not a power-of-two square", ntexels);
+    G.tex_size = (int)side;
+  }
+  size_t nv = (size_t)ntris * 3;
+  if ((rc = upload(c, &G.xyz, xyz, nv * 3)) || (rc = upload(c, &G.vn, vn, nv * 3)) || (rc = upload(c, &G.uv, uv, nv * 2)) ||
+      (rc = upload(c, &G.tr, r, (size_t)ntexels)) || (rc = upload(c, &G.tg, g, (size_t)ntexels)) ||
+      (rc = upload(c, &G.tb, b, (size_t)ntexels)))
+    return rc;
+  if (cudaMalloc(&G.li, sizeof(float) * std::max<size_t>(nv * 3, 1)) != cudaSuccess) return fail(AXR_ENOMEM, "LI buffer");
+  CK(cudaMemsetAsync(G.li, 0, sizeof(float) * nv * 3, c->stream));
+  c->groups.push_back(G);
+  c->total_tris += ntris;
+  if ((rc = ensure_lists(c))) return rc;
+  CK(cudaStreamSynchronize(c->stream));   // host arrays are borrowed only for the call
+  if (out_id) *out_id = (int)c->groups.size() - 1;
+  return 0;
+}
+
+int axr_set_vert_light(axr_ctx *c, int group, const float *li) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (group < 0 || group >= (int)c->groups.size() || !li) return fail(AXR_EINVAL, "group %d", group);
+  CK(cudaMemcpyAsync(c->groups[group].li, li, sizeof(float) * 9 * (size_t)c->groups[group].ntris,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int axr_vert_light(axr_ctx *c, const uint8_t *mask, int ngroups, const float *dir_int, const float *dir_dir, int ndirs,
+                   float amb) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (ngroups != (int)c->groups.size() || ndirs < 0 || ndirs > 64 || (ndirs && (!dir_int || !dir_dir)))
+    return fail(AXR_EINVAL, "vert_light arguments");
+  float *d = nullptr;
+  if (cudaMalloc(&d, sizeof(float) * 6 * std::max(ndirs, 1)) != cudaSuccess) return fail(AXR_ENOMEM, "light table");
+  cudaMemcpyAsync(d, dir_int, sizeof(float) * 3 * ndirs, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(d + 3 * ndirs, dir_dir, sizeof(float) * 3 * ndirs, cudaMemcpyHostToDevice, c->stream);
+  for (int g = 0; g < ngroups; g++) {
+    if (mask && !mask[g]) continue;
+    int nv = c->groups[g].ntris * 3;
+    if (!nv) continue;
+    k_vert_light<<<grid_for(c, nv, 256, 8), 256, 0, c->stream>>>(c->groups[g].vn, c->groups[g].li, nv, d, d + 3 * ndirs,
+                                                                    ndirs, amb);
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(AXR_ECUDA, "vert_light: %s", cudaGetErrorString(e));
+  c->amb = amb;
+  return 0;
+}
+
+int axr_copy_to(axr_ctx *c, int group, const float *xyz, const float *vn, int tri_start, int ntris) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (group < 0 || group >= (int)c->groups.size()) return fail(AXR_EINVAL, "group %d", group);
+  Group &G = c->groups[group];
+  if (tri_start < 0 || ntris < 0 || tri_start + ntris > G.ntris) return fail(AXR_EINVAL, "range out of group");
+  size_t off = (size_t)tri_start * 9, n = (size_t)ntris * 9;
+  if (xyz) CK(cudaMemcpyAsync(G.xyz + off, xyz, n * 4, cudaMemcpyHostToDevice, c->stream));
+  if (vn) CK(cudaMemcpyAsync(G.vn + off, vn, n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int axr_add_tex_alpha(axr_ctx *c, const uint8_t *mask, int side, int *out_id) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!mask || !is_pow2(side)) return fail(AXR_EINVAL, "alpha mask side %d is not a power of two", side);
+  Alpha a;
+  a.side = side;
+  std::vector<uint8_t> b((size_t)side * side);
+  for (size_t i = 0; i < b.size(); i++) b[i] = mask[i] ? 1 : 0;
+  if ((rc = upload(c, &a.mask, b.data(), b.size()))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->alphas.push_back(a);
+  if (out_id) *out_id = (int)c->alphas.size() - 1;
+  return 0;
+}
+
+int axr_set_primary_light(axr_ctx *c, const float i[3], const float d[3]) {
+  if (!c || !i || !d) return fail(AXR_EINVAL, "null argument");
+  memcpy(c->lint, i, sizeof c->lint);
+  memcpy(c->ldir, d, sizeof c->ldir);
+  return 0;
+}
+
+int axr_set_pos(axr_ctx *c, const float p[3]) {
+  if (!c || !p) return fail(AXR_EINVAL, "null argument");
+  memcpy(c->pos, p, sizeof c->pos);
+  return 0;
+}
+
+int axr_set_vm(axr_ctx *c, const float vm[9]) {
+  if (!c || !vm) return fail(AXR_EINVAL, "null argument");
+  memcpy(c->vm, vm, sizeof c->vm);
+  return 0;
+}
+
+int axr_clear_zbuffer(axr_ctx *c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  k_clear_depth<<<grid_for(c, (long)c->w * c->h, 256, 8), 256, 0, c->stream>>>(c->db, c->w, c->h, 4);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *mask, int ngroups,
+                 const int32_t *shadow_ids, int nshadow) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (ngroups != (int)c->groups.size()) return fail(AXR_EINVAL, "drawAll with %d groups, handle has %zu", ngroups, c->groups.size());
+  if (nshadow < 0 || nshadow > 2) return fail(AXR_EINVAL, "at most two shadow cascades");
+  if ((rc = settle(c))) return rc;
+  DrawParams P;
+  memset(&P, 0, sizeof P);
+  bool any_shadow = false;
+  for (int g = 0; g < ngroups; g++)
+    if ((!mask || !mask[g]) && flags && (flags[g] & F_SHADOW)) any_shadow = true;
+  P.nsh = nshadow;
+  for (int k = 0; k < nshadow; k++) {
+    int id = shadow_ids[k];
+    if (id < 0 || id >= MAX_SHADOWS || !c->shadows[id].map) return fail(AXR_ESTATE, "shadow map %d does not exist", id);
+    Shadow &s = c->shadows[id];
+    P.sh[k].map = s.map; P.sh[k].dim = s.dim; P.sh[k].scale = s.scale;
+    memcpy(P.sh[k].pos, s.pos, sizeof s.pos);
+    memcpy(P.sh[k].vv, s.vv, sizeof s.vv);
+  }
+  if (any_shadow && nshadow == 0) return fail(AXR_ESTATE, "shadow materials drawn with no shadow map");
+  if ((rc = upload_groups(c, flags, alpha_index, mask, false, ngroups))) return rc;
+  P.groups = c->d_groups;
+  P.ngroups = ngroups;
+  P.total_tris = c->total_tris;
+  P.view = make_view(c);
+  memcpy(P.light.lint, c->lint, sizeof c->lint);
+  memcpy(P.light.ldir, c->ldir, sizeof c->ldir);
+  P.light.amb = c->amb;
+  P.keys = c->keys; P.ro = c->ro; P.go = c->go; P.bo = c->bo; P.db = c->db;
+  P.small_list = c->small_list; P.large_list = c->large_list;
+  P.units = c->units; P.ctr = c->ctr;
+  P.cap_list = c->cap_list; P.cap_units = c->cap_units;
+  long npix = (long)c->w * c->h;
+  cudaStream_t s = c->stream;
+  int64_t nk = 0;
+  k_init_keys<<<grid_for(c, npix, 256, 16), 256, 0, s>>>(c->db, c->keys, (int)npix, c->ctr); nk++;
+  if (c->total_tris > 0) {
+    k_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, s>>>(P); nk++;
+    k_raster_small<<<c->sms * 8, 128, 0, s>>>(P); nk++;
+    k_coarse<<<c->sms * 4, 128, 0, s>>>(P); nk++;
+    k_raster_tiled<<<c->sms * 8, 128, 0, s>>>(P); nk++;
+    k_raster_tiled_fallback<<<c->sms * 2, 128, 0, s>>>(P); nk++;
+  }
+  dim3 sb(16, 16), sgd((c->w + 15) / 16, (c->h + 15) / 16);
+  k_shade<<<sgd, sb, 0, s>>>(P); nk++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->h_ctr, c->ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
+  c->pending = true;
+  c->last_kernels = nk;
+  return 0;
+}
+
+int axr_get_frame(axr_ctx *c, uint16_t *r, uint16_t *g, uint16_t *b, float *depth) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  size_t n = (size_t)c->w * c->h;
+  if (r) CK(cudaMemcpyAsync(r, c->ro, n * 2, cudaMemcpyDeviceToHost, c->stream));
+  if (g) CK(cudaMemcpyAsync(g, c->go, n * 2, cudaMemcpyDeviceToHost, c->stream));
+  if (b) CK(cudaMemcpyAsync(b, c->bo, n * 2, cudaMemcpyDeviceToHost, c->stream));
+  if (depth) CK(cudaMemcpyAsync(depth, c->db, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return settle(c);
+}
+
+int axr_get_ids(axr_ctx *c, int32_t *tri_id, uint8_t *cov) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  size_t n = (size_t)c->w * c->h;
+  int32_t *dt = nullptr;
+  uint8_t *dc = nullptr;
+  if (cudaMalloc(&dt, n * 4) != cudaSuccess || cudaMalloc(&dc, n) != cudaSuccess) {
+    cudaFree(dt);
+    return fail(AXR_ENOMEM, "id buffers");
+  }
+  k_ids<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(c->keys, (int)n, dt, dc);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && tri_id) e = cudaMemcpyAsync(tri_id, dt, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && cov) e = cudaMemcpyAsync(cov, dc, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(dt);
+  cudaFree(dc);
+  if (e != cudaSuccess) return fail(AXR_ECUDA, "get_ids: %s", cudaGetErrorString(e));
+  return settle(c);
+}
+
+int axr_set_frame(axr_ctx *c, const uint16_t *r, const uint16_t *g, const uint16_t *b, const float *depth) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  size_t n = (size_t)c->w * c->h;
+  if (r) CK(cudaMemcpyAsync(c->ro, r, n * 2, cudaMemcpyHostToDevice, c->stream));
+  if (g) CK(cudaMemcpyAsync(c->go, g, n * 2, cudaMemcpyHostToDevice, c->stream));
+  if (b) CK(cudaMemcpyAsync(c->bo, b, n * 2, cudaMemcpyHostToDevice, c->stream));
+  if (depth) CK(cudaMemcpyAsync(c->db, depth, n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int axr_gamma(axr_ctx *c, float ex) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  long n = (long)c->w * c->h;
+  k_gamma<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, ex);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_add_shadow_map(axr_ctx *c, int i, int size, float scale, float amb) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (i < 0 || i >= MAX_SHADOWS || size < 4 || size > 16384) return fail(AXR_EINVAL, "shadow map %d of size %d", i, size);
+  Shadow &s = c->shadows[i];
+  if (s.map && s.dim != size) { CK(cudaStreamSynchronize(c->stream)); cudaFree(s.map); s.map = nullptr; }
+  if (!s.map && cudaMalloc(&s.map, sizeof(float) * (size_t)size * size) != cudaSuccess)
+    return fail(AXR_ENOMEM, "shadow map %dx%d", size, size);
+  s.dim = size;
+  s.scale = scale;
+  // a fresh map holds 65535 (Ops.py:1049)
+  k_clear_depth<<<grid_for(c, (long)size * size, 256, 8), 256, 0, c->stream>>>(s.map, size, size, 1);
+  CK(cudaGetLastError());
+  c->amb = amb;
+  return 0;
+}
+
+int axr_place_shadow_map(axr_ctx *c, int i, const float pos[3], const float vm[9], float amb) {
+  if (!c || !pos || !vm) return fail(AXR_EINVAL, "null argument");
+  if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
+  memcpy(c->shadows[i].pos, pos, sizeof(float) * 3);
+  memcpy(c->shadows[i].vv, vm, sizeof(float) * 9);
+  if (amb >= 0) c->amb = amb;
+  return 0;
+}
+
+int axr_clear_shadow_map(axr_ctx *c, int i) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
+  Shadow &s = c->shadows[i];
+  k_clear_depth<<<grid_for(c, (long)s.dim * s.dim, 256, 8), 256, 0, c->stream>>>(s.map, s.dim, s.dim, 16);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags, const int32_t *alpha_index, int ngroups,
+                   float bias) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
+  if (ngroups != (int)c->groups.size() || !cast) return fail(AXR_EINVAL, "shadowMap arguments");
+  if ((rc = settle(c))) return rc;
+  // alpha casters use the alpha mask's own side as lenT (drawminalpha.c:86-96)
+  std::vector<int32_t> fl(ngroups, 0);
+  for (int g = 0; g < ngroups; g++) fl[g] = flags ? (flags[g] & (F_ALPHA | F_MIP)) : 0;
+  GroupDev tab[MAX_GROUPS];
+  memset(tab, 0, sizeof tab);
+  for (int g = 0; g < ngroups; g++) {
+    const Group &G = c->groups[g];
+    GroupDev &d = tab[g];
+    d.xyz = G.xyz; d.uv = G.uv; d.ntris = G.ntris; d.tri_base = G.tri_base; d.tex_size = G.tex_size;
+    d.flags = fl[g] & F_ALPHA;
+    d.enabled = cast[g] ? 1 : 0;
+    if (d.flags & F_ALPHA) {
+      int ai = alpha_index ? alpha_index[g] : 0;
+      if (ai < 0 || ai >= (int)c->alphas.size()) return fail(AXR_EINVAL, "group %d: alpha index %d", g, ai);
+      d.amask = c->alphas[ai].mask;
+      d.alen = c->alphas[ai].side;
+    }
+  }
+  CK(cudaMemcpyAsync(c->d_groups, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, c->stream));
+  Shadow &sm = c->shadows[i];
+  ShadowParams S;
+  memset(&S, 0, sizeof S);
+  S.groups = c->d_groups; S.ngroups = ngroups; S.total_tris = c->total_tris;
+  S.sh.map = sm.map; S.sh.dim = sm.dim; S.sh.scale = sm.scale;
+  memcpy(S.sh.pos, sm.pos, sizeof sm.pos);
+  memcpy(S.sh.vv, sm.vv, sizeof sm.vv);
+  S.map = sm.map; S.bias = bias; S.list = c->sh_list; S.ctr = c->ctr;
+  if (c->total_tris == 0) return 0;
+  CK(cudaMemsetAsync(c->ctr + CTR_SH_LIST, 0, sizeof(uint32_t) * 2, c->stream));
+  k_shadow_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, c->stream>>>(S);
+  k_shadow_raster<<<c->sms * 8, 128, 0, c->stream>>>(S);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_get_shadow_map(axr_ctx *c, int i, float *out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
+  if (!out) return fail(AXR_EINVAL, "null output");
+  Shadow &s = c->shadows[i];
+  CK(cudaMemcpyAsync(out, s.map, sizeof(float) * (size_t)s.dim * s.dim, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return settle(c);
+}
+
+int axr_sync(axr_ctx *c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return settle(c);
+}
+
+int axr_get_stream(axr_ctx *c, void **stream) {
+  if (!c || !stream) return fail(AXR_EINVAL, "null argument");
+  *stream = (void *)c->stream;
+  return 0;
+}
+
+int axr_frame_device_ptrs(axr_ctx *c, void **r, void **g, void **b, void **depth, void **keys) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  if (r) *r = c->ro;
+  if (g) *g = c->go;
+  if (b) *b = c->bo;
+  if (depth) *depth = c->db;
+  if (keys) *keys = c->keys;
+  return 0;
+}
+
+int axr_last_stats(axr_ctx *c, int64_t *kernels, int64_t *n_small, int64_t *n_large, int64_t *n_units) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if ((rc = axr_sync(c))) return rc;
+  if (kernels) *kernels = c->last_kernels;
+  if (n_small) *n_small = c->h_ctr[CTR_SMALL];
+  if (n_large) *n_large = c->h_ctr[CTR_LARGE];
+  if (n_units) *n_units = c->h_ctr[CTR_UNITS];
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,1061 @@
+// kernels.cuh -- CUDA kernels of the rasterizer hot path (sm_100a).
+//
+// Frame = visibility then shading:
+//   k_init_keys    one 64-bit visibility word per pixel from the depth buffer
+//   k_setup        per triangle: projection, rejection, small/large split
+//                  (trisetup.c), warp-ballot compaction into two lists
+//   k_raster_small persistent; warps take 32 small triangles, each lane walks
+//                  its rows (drawSmall, Templates.py:250-323) and the warp
+//                  fills the queued spans pixel-parallel; fragment = 64-bit
+//                  atomicMin(depth key | ~order) in the L2-resident buffer
+//   k_coarse       per large triangle: tile binning of coarse.c, written as
+//                  (triangle, tile) units with warp-scan offsets
+//   k_raster_tiled persistent over units: per-tile restart of the tiled
+//                  `draw` (Templates.py:93-185), same span queue
+//   k_shade        per pixel: decode the winner, replay its row interpolants
+//                  and shade once (bilinear/trilinear, alpha, shadow)
+// The packed key makes the result independent of scheduling: smallest depth
+// wins, equal depths go to the later fragment of the reference's serial
+// order (small pass < large pass, material, triangle, bottom < top half).
+#pragma once
+#include "raster.cuh"
+
+namespace axr {
+
+struct DrawParams {
+  const GroupDev *groups;
+  int ngroups;
+  int total_tris;
+  ViewDev view;
+  LightDev light;
+  ShadowDev sh[2];
+  int nsh;
+  uint64_t *keys;
+  uint16_t *ro, *go, *bo;
+  float *db;
+  uint32_t *small_list, *large_list;
+  uint2 *units;
+  uint32_t *ctr;       // see CTR_*
+  uint32_t cap_list, cap_units;
+};
+
+enum { CTR_SMALL = 0, CTR_LARGE = 1, CTR_UNITS = 2, CTR_WORK_SMALL = 3, CTR_WORK_UNITS = 4, CTR_OVERFLOW = 5,
+       CTR_WORK_LARGE = 6, CTR_SH_LIST = 7, CTR_SH_WORK = 8, CTR_N = 16 };
+
+// ------------------------------------------------------------ helpers
+
+__device__ __forceinline__ int find_group(const GroupDev *__restrict__ gs, int ng, uint32_t gtri) {
+  int lo = 0, hi = ng - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if ((uint32_t)gs[mid].tri_base <= gtri) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// count of x in [ax0, ...] with (float)x <= bound, clipped to [0, w)
+__device__ __forceinline__ void span_clip(int ax0, float bound, int w, int &lo, int &cnt) {
+  lo = ax0 < 0 ? 0 : ax0;
+  if (bound != bound) { cnt = 0; return; }
+  float fb = floorf(bound);
+  int hi = fb >= (float)(w - 1) ? w - 1 : f2i(fb);
+  cnt = hi >= lo ? hi - lo + 1 : 0;
+}
+
+// ------------------------------------------------------------ keys / clear
+
+__global__ void k_init_keys(const float *__restrict__ db, uint64_t *__restrict__ keys, int n, uint32_t *ctr) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < CTR_N && blockIdx.x == 0) ctr[i] = 0;
+  for (; i < n; i += gridDim.x * blockDim.x) keys[i] = ((uint64_t)depth_key(db[i]) << 32) | 0xffffffffull;
+}
+
+// clearzb.c:10-22 over lenP x lenP work-items of (w/lenP) x (h/lenP) blocks
+__global__ void k_clear_depth(float *__restrict__ f, int w, int h, int lenP) {
+  int bw = (w / lenP) * lenP, bh = (h / lenP) * lenP;
+  int n = bw * bh;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int y = i / bw, x = i - y * bw;
+    f[(size_t)w * y + x] = 65535.f;
+  }
+}
+
+// Post/gamma.c:38-52
+__global__ void k_gamma(uint16_t *r, uint16_t *g, uint16_t *b, int n, float exposure) {
+  float e8 = 8 * exposure;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float jx = sqrtf(e8 * (float)r[i]) / 1.1f;
+    float jy = sqrtf(e8 * (float)g[i]) / 1.1f;
+    float jz = sqrtf(e8 * (float)b[i]) / 1.1f;
+    float m = fmaxf(jx, fmaxf(jy, jz)) / 255.f;
+    if (m > 1.f) {
+      float sm = sqrtf(m);
+      jx = jx / sm; jy = jy / sm; jz = jz / sm;
+    }
+    r[i] = (uint16_t)f2i(fminf(255.f, jx));
+    g[i] = (uint16_t)f2i(fminf(255.f, jy));
+    b[i] = (uint16_t)f2i(fminf(255.f, jz));
+  }
+}
+
+// vert.c:38-87 (directional lights 1..n-1; light 0 is shaded per pixel)
+__global__ void k_vert_light(const float *__restrict__ vn, float *__restrict__ li, int nv,
+                             const float *__restrict__ dints, const float *__restrict__ ddirs, int ndirs,
+                             float amb) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    V3 n = ld3(vn + (size_t)v * 3);
+    V3 light{0.f, 0.f, 0.f};
+    for (int i = 1; i < ndirs; i++) {
+      V3 d{ddirs[3 * i], ddirs[3 * i + 1], ddirs[3 * i + 2]};
+      V3 it{dints[3 * i], dints[3 * i + 1], dints[3 * i + 2]};
+      float s = fmaxf(0.f, dot3(n, d) + 0.5f) * 0.66f;
+      light = add3(light, smul3(s, it));
+    }
+    li[(size_t)v * 3 + 0] = fmaxf(light.x, amb);
+    li[(size_t)v * 3 + 1] = fmaxf(light.y, amb);
+    li[(size_t)v * 3 + 2] = fmaxf(light.z, amb);
+  }
+}
+
+// ------------------------------------------------------------ setup
+
+// one thread per triangle of every enabled group; lists hold global ids
+__global__ void __launch_bounds__(256) k_setup(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < P.total_tris; base += gridDim.x * blockDim.x) {
+    int t = base + threadIdx.x;
+    int cls = 0;
+    if (t < P.total_tris) {
+      int g = find_group(sg, P.ngroups, (uint32_t)t);
+      const GroupDev &G = sg[g];
+      if (G.enabled) {
+        float sx[3], sy[3], sz[3];
+        cls = project_persp(G, t - G.tri_base, P.view, sx, sy, sz);
+      }
+    }
+    unsigned ms = __ballot_sync(FULL, cls == 1), ml = __ballot_sync(FULL, cls == 2);
+    uint32_t bs = 0, bl = 0;
+    if (lane == 0) {
+      if (ms) bs = atomicAdd(&P.ctr[CTR_SMALL], __popc(ms));
+      if (ml) bl = atomicAdd(&P.ctr[CTR_LARGE], __popc(ml));
+    }
+    bs = __shfl_sync(FULL, bs, 0);
+    bl = __shfl_sync(FULL, bl, 0);
+    unsigned lt = (1u << lane) - 1;
+    if (cls == 1) P.small_list[bs + __popc(ms & lt)] = (uint32_t)t;
+    if (cls == 2) P.large_list[bl + __popc(ml & lt)] = (uint32_t)t;
+  }
+}
+
+// ------------------------------------------------------------ span queue
+
+struct SpanV {
+  int cy, lo, cnt;
+  uint32_t ord;
+  float cx1, cx2, cz1, cz2;
+  float u1x, u1y, u2x, u2y;
+  int g, alen;
+  int pad0, pad1;
+};
+
+// Per-fragment visibility: alpha test (av_draw_alpha.c:80-97) then the
+// packed depth/order atomicMin.
+__device__ __forceinline__ void vis_fragment(const DrawParams &P, const GroupDev *sg, const SpanV &s, int ax) {
+  float t = ((float)ax - s.cx2) / (s.cx1 - s.cx2);
+  t = clamp_t(t);
+  float tz = 1.0f / ((1 - t) * s.cz2 + t * s.cz1);
+  if (tz != tz) return;
+  if (s.g >= 0) {
+    float omt = 1 - t;
+    V2 uvi{omt * s.u2x + t * s.u1x, omt * s.u2y + t * s.u1y};
+    Taps q = make_taps(uvi, tz, s.alen, 0);
+    float ca = bilerp_bool(q, sg[s.g].amask);
+    if (!(ca > 0.5f)) return;
+  }
+  atomicMin((unsigned long long *)&P.keys[(size_t)P.view.w * s.cy + ax], (unsigned long long)frag_key(tz, s.ord));
+}
+
+// Drain one round of spans (one per lane) cooperatively across the warp.
+__device__ __forceinline__ void warp_fill(const DrawParams &P, const GroupDev *sg, SpanV *q, int *pre, int lane,
+                                          const SpanV &mine) {
+  int c = mine.cnt;
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int v = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += v;
+  }
+  int total = __shfl_sync(FULL, incl, 31);
+  if (total == 0) return;
+  q[lane] = mine;
+  pre[lane] = incl - c;
+  __syncwarp();
+  for (int p = lane; p < total; p += 32) {
+    int s = 0;
+#pragma unroll
+    for (int step = 16; step; step >>= 1)
+      if (pre[s + step] <= p) s += step;
+    vis_fragment(P, sg, q[s], q[s].lo + (p - pre[s]));
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------ small triangles
+
+struct SmallLane {
+  int g, alen;
+  uint32_t gtri;
+  int x1, x2, x3, y1, y2, y3;
+  float z1, z2, z3, x4, z4;
+  V2 uv1, uv2, uv3, uv4;
+  int half, cy;
+  float s1, s2, sz1, sz2, cx1, cx2, cz1, cz2;
+  V2 su1, su2, cu1, cu2;
+  bool alpha;
+
+  __device__ __forceinline__ void start_half0() {
+    half = 0;
+    float yd = 1.0f / (float)(y2 - y1);
+    s1 = (float)(x2 - x1) * yd;
+    s2 = (x4 - (float)x1) * yd;
+    sz1 = (z2 - z1) * yd;
+    sz2 = (z4 - z1) * yd;
+    cx1 = cx2 = (float)x1;
+    cz1 = cz2 = z1;
+    if (alpha) {
+      su1 = mul2(sub2(uv2, uv1), yd);
+      su2 = mul2(sub2(uv4, uv1), yd);
+      cu1 = cu2 = uv1;
+    }
+    if (s1 < s2) {
+      float t = s1; s1 = s2; s2 = t;
+      t = sz1; sz1 = sz2; sz2 = t;
+      V2 tv = su1; su1 = su2; su2 = tv;
+    }
+    cy = y1;
+  }
+  __device__ __forceinline__ void start_half1() {
+    half = 1;
+    float yd = 1.0f / (float)(y3 - y2);
+    s1 = (float)(x3 - x2) * yd;
+    s2 = ((float)x3 - x4) * yd;
+    sz1 = (z3 - z2) * yd;
+    sz2 = (z3 - z4) * yd;
+    cx1 = cx2 = (float)x3;
+    cz1 = cz2 = z3;
+    if (alpha) {
+      su1 = mul2(neg2(sub2(uv2, uv3)), yd);
+      su2 = mul2(neg2(sub2(uv4, uv3)), yd);
+      cu1 = cu2 = uv3;
+    }
+    if (s1 < s2) {
+      float t = s1; s1 = s2; s2 = t;
+      t = sz1; sz1 = sz2; sz2 = t;
+      V2 tv = su1; su1 = su2; su2 = tv;
+    }
+    cy = y3;
+  }
+
+  __device__ __forceinline__ void init(const DrawParams &P, const GroupDev *sg, uint32_t t) {
+    gtri = t;
+    g = find_group(sg, P.ngroups, t);
+    const GroupDev &G = sg[g];
+    int tri = (int)(t - G.tri_base);
+    float sx[3], sy[3], sz[3];
+    project_persp(G, tri, P.view, sx, sy, sz);
+    int ix[3], iy[3];
+    float z[3];
+    Attr<false> a[3];
+    alpha = (G.flags & F_ALPHA) != 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      ix[k] = f2i(sx[k]); iy[k] = f2i(sy[k]); z[k] = sz[k];
+      if (alpha) a[k] = a_load<false>(G, tri, k, sz[k]);
+    }
+#define SW(i, j) { int ti = iy[i]; iy[i] = iy[j]; iy[j] = ti; ti = ix[i]; ix[i] = ix[j]; ix[j] = ti; \
+                   float tf = z[i]; z[i] = z[j]; z[j] = tf; Attr<false> ta = a[i]; a[i] = a[j]; a[j] = ta; }
+    if (iy[0] > iy[1]) SW(0, 1);
+    if (iy[1] > iy[2]) SW(1, 2);
+    if (iy[0] > iy[1]) SW(0, 1);
+#undef SW
+    x1 = ix[0]; x2 = ix[1]; x3 = ix[2]; y1 = iy[0]; y2 = iy[1]; y3 = iy[2];
+    z1 = z[0]; z2 = z[1]; z3 = z[2];
+    float yd = (float)(y2 - y1) / (float)(y3 - y1);
+    x4 = (float)x1 + yd * (float)(x3 - x1);
+    z4 = z1 + yd * (z3 - z1);
+    if (alpha) {
+      uv4 = add2(a[0].uv, smul2(yd, sub2(a[2].uv, a[0].uv)));
+      int num_mip = (G.flags & F_MIP) ? G.tex_size : 0;
+      if (G.flags & F_MIP) mip_setup<false>(a, z, true, ix, iy, nullptr, nullptr, num_mip, G.mip_bias);
+      uv1 = a[0].uv; uv2 = a[1].uv; uv3 = a[2].uv;
+      alen = G.alen;
+    }
+    start_half0();
+  }
+
+  // emits the span of the current row and advances; returns false when done
+  __device__ __forceinline__ bool step(const DrawParams &P, SpanV &s) {
+    s.cnt = 0;
+    s.cy = cy;
+    s.ord = make_order(0, gtri, half);
+    s.cx1 = cx1; s.cx2 = cx2; s.cz1 = cz1; s.cz2 = cz2;
+    s.g = alpha ? g : -1;
+    s.alen = alen;
+    if (alpha) { s.u1x = cu1.x; s.u1y = cu1.y; s.u2x = cu2.x; s.u2y = cu2.y; }
+    if (cy >= 0 && cy < P.view.h) {
+      if (half == 0) span_clip(f2i(cx2), cx1, P.view.w, s.lo, s.cnt);
+      else span_clip(f2i(cx1), cx2, P.view.w, s.lo, s.cnt);
+    }
+    if (half == 0) {
+      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
+      if (alpha) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
+      cy++;
+      if (cy > y2) start_half1();
+      return true;
+    }
+    cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
+    if (alpha) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
+    cy--;
+    return cy >= y2;
+  }
+};
+
+__global__ void __launch_bounds__(128) k_raster_small(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  __shared__ SpanV q[4][32];
+  __shared__ int pre[4][33];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
+  __syncthreads();
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t n = P.ctr[CTR_SMALL];
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&P.ctr[CTR_WORK_SMALL], 32u);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= n) break;
+    SmallLane L;
+    bool live = base + lane < n;
+    if (live) L.init(P, sg, P.small_list[base + lane]);
+    while (__any_sync(FULL, live)) {
+      SpanV s;
+      s.cnt = 0;
+      if (live) live = L.step(P, s);
+      warp_fill(P, sg, q[w], pre[w], lane, s);
+    }
+  }
+}
+
+// ------------------------------------------------------------ coarse binning
+
+// coarse.c:17-125 in tile units; calls emit(tile) for every bin entry
+template <class F>
+__device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3], int wc, int hc, F emit) {
+  float x1 = sx[0] / 16.f - 0.5f, x2 = sx[1] / 16.f - 0.5f, x3 = sx[2] / 16.f - 0.5f;
+  float y1 = sy[0] / 16.f - 0.5f, y2 = sy[1] / 16.f - 0.5f, y3 = sy[2] / 16.f - 0.5f;
+  float t;
+  if (y1 > y2) { t = y1; y1 = y2; y2 = t; t = x1; x1 = x2; x2 = t; }
+  if (y2 > y3) { t = y2; y2 = y3; y3 = t; t = x2; x2 = x3; x3 = t; }
+  if (y1 > y2) { t = y1; y1 = y2; y2 = t; t = x1; x1 = x2; x2 = t; }
+  float x4 = (x1 + ((y2 - y1) / (y3 - y1)) * (x3 - x1));
+  float y4 = y2;
+  float s1 = (x2 - x1) / (y2 - y1);
+  float s2 = (x4 - x1) / (y4 - y1);
+  float cx1 = x1, cx2 = x1;
+  if (s1 < s2) { t = s1; s1 = s2; s2 = t; }
+  float sbias = 1.f + floorf(y1) - y1;
+  float wcm1 = (float)wc - 1;
+  if (y1 != y2) {
+    for (int cy = f2i(floorf(y1)); (float)cy <= ceilf(y2); cy++) {
+      float mx1 = cx1 + sbias * s1;
+      if (s1 < 0) mx1 -= s1;
+      float mx2 = cx2 + sbias * s2;
+      if (s2 > 0) mx2 -= s2;
+      mx1 = fminf(mx1, wcm1);
+      mx2 = fmaxf(mx2, 0.f);
+      if (cy >= 0 && cy < hc) {
+        int a1 = f2i(floorf(mx2));
+        float hb = ceilf(mx1);
+        for (int ax = a1; (float)ax <= hb; ax++) emit(wc * cy + ax);
+      }
+      cx1 += s1;
+      cx2 += s2;
+    }
+  }
+  s1 = (x3 - x2) / (y3 - y2);
+  s2 = (x3 - x4) / (y3 - y4);
+  cx1 = x3; cx2 = x3;
+  if (s1 < s2) { t = s1; s1 = s2; s2 = t; }
+  sbias = y3 - floorf(y3);
+  if (y2 != y3) {
+    for (int cy = f2i(ceilf(y3)); (float)cy >= floorf(y2); cy--) {
+      float mx1 = cx1 - sbias * s1;
+      if (s1 < 0) mx1 += s1;
+      float mx2 = cx2 - sbias * s2;
+      if (s2 > 0) mx2 += s2;
+      mx2 = fminf(mx2, wcm1);
+      mx1 = fmaxf(mx1, 0.f);
+      if (cy >= 0 && cy < hc) {
+        int a1 = f2i(floorf(mx1));
+        float hb = ceilf(mx2);
+        for (int ax = a1; (float)ax <= hb; ax++) emit(wc * cy + ax);
+      }
+      cx1 -= s1;
+      cx2 -= s2;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  uint32_t n = P.ctr[CTR_LARGE];
+  int wc = P.view.w / TILE, hc = P.view.h / TILE;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&P.ctr[CTR_WORK_LARGE], 32u);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= n) break;
+    bool live = base + lane < n;
+    float sx[3], sy[3], sz[3];
+    uint32_t gt = 0;
+    int cnt = 0;
+    if (live) {
+      gt = P.large_list[base + lane];
+      const GroupDev &G = sg[find_group(sg, P.ngroups, gt)];
+      project_persp(G, (int)(gt - G.tri_base), P.view, sx, sy, sz);
+      coarse_walk(sx, sy, wc, hc, [&](int) { cnt++; });
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += v;
+    }
+    uint32_t total = (uint32_t)__shfl_sync(FULL, incl, 31);
+    uint32_t off = 0;
+    if (lane == 31 && total) off = atomicAdd(&P.ctr[CTR_UNITS], total);
+    off = __shfl_sync(FULL, off, 31) + (uint32_t)(incl - cnt);
+    if (live && cnt) {
+      if ((uint64_t)off + (uint64_t)cnt > (uint64_t)P.cap_units) {
+        atomicOr(&P.ctr[CTR_OVERFLOW], 1u);
+      } else {
+        uint2 *u = P.units + off;
+        int k = 0;
+        coarse_walk(sx, sy, wc, hc, [&](int tile) { u[k++] = make_uint2(gt, (uint32_t)tile); });
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ tiled (large) raster
+
+struct TileLane {
+  int g, alen;
+  uint32_t gtri;
+  float x1, x2, x3, y1, y2, y3, z1, z2, z3, x4, z4;
+  V2 uv1, uv2, uv3, uv4;
+  float xMin, xMax, yMin, yMax;
+  int half, cy;
+  bool live_half;
+  float ybound;
+  float s1, s2, sz1, sz2, cx1, cx2, cz1, cz2;
+  V2 su1, su2, cu1, cu2;
+  bool alpha;
+
+  __device__ __forceinline__ void start_half0() {
+    half = 0;
+    float yd = 1.0f / (y2 - y1);
+    s1 = (x2 - x1) * yd;
+    s2 = (x4 - x1) * yd;
+    sz1 = (z2 - z1) * yd;
+    sz2 = (z4 - z1) * yd;
+    if (alpha) { su1 = mul2(sub2(uv2, uv1), yd); su2 = mul2(sub2(uv4, uv1), yd); }
+    if (s1 < s2) {
+      float t = s1; s1 = s2; s2 = t;
+      t = sz1; sz1 = sz2; sz2 = t;
+      V2 tv = su1; su1 = su2; su2 = tv;
+    }
+    cy = f2i(clampf_(y1, yMin, yMax));
+    float dy = (float)cy - y1;
+    cx1 = x1 + dy * s1; cx2 = x1 + dy * s2;
+    cz1 = z1 + dy * sz1; cz2 = z1 + dy * sz2;
+    if (alpha) { cu1 = add2(uv1, smul2(dy, su1)); cu2 = add2(uv1, smul2(dy, su2)); }
+    ybound = clampf_(y2, yMin, yMax);
+    live_half = (y2 > yMin) && ((float)cy <= ybound);
+  }
+  __device__ __forceinline__ void start_half1() {
+    half = 1;
+    float yd = 1.0f / (y3 - y2);
+    s1 = (x3 - x2) * yd;
+    s2 = (x3 - x4) * yd;
+    sz1 = (z3 - z2) * yd;
+    sz2 = (z3 - z4) * yd;
+    if (alpha) { su1 = mul2(neg2(sub2(uv2, uv3)), yd); su2 = mul2(neg2(sub2(uv4, uv3)), yd); }
+    if (s1 < s2) {
+      float t = s1; s1 = s2; s2 = t;
+      t = sz1; sz1 = sz2; sz2 = t;
+      V2 tv = su1; su1 = su2; su2 = tv;
+    }
+    cy = f2i(clampf_(y3, yMin, yMax));
+    float dy = (float)cy - y3;
+    cx1 = x3 + dy * s1; cx2 = x3 + dy * s2;
+    cz1 = z3 + dy * sz1; cz2 = z3 + dy * sz2;
+    if (alpha) { cu1 = add2(uv3, smul2(dy, su1)); cu2 = add2(uv3, smul2(dy, su2)); }
+    ybound = clampf_(y2, yMin, yMax);
+    live_half = (y2 < yMax) && ((float)cy >= ybound);
+  }
+
+  // returns false if the unit has no rows at all
+  __device__ __forceinline__ bool init(const DrawParams &P, const GroupDev *sg, uint2 unit) {
+    gtri = unit.x;
+    int bx = (int)unit.y;
+    g = find_group(sg, P.ngroups, gtri);
+    const GroupDev &G = sg[g];
+    int tri = (int)(gtri - G.tri_base);
+    float sx[3], sy[3], sz[3];
+    project_persp(G, tri, P.view, sx, sy, sz);
+    alpha = (G.flags & F_ALPHA) != 0;
+    Attr<false> a[3];
+    float x[3], y[3], z[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      x[k] = sx[k]; y[k] = sy[k]; z[k] = sz[k];
+      if (alpha) a[k] = a_load<false>(G, tri, k, sz[k]);
+    }
+#define SW(i, j) { float tf = y[i]; y[i] = y[j]; y[j] = tf; tf = x[i]; x[i] = x[j]; x[j] = tf; \
+                   tf = z[i]; z[i] = z[j]; z[j] = tf; Attr<false> ta = a[i]; a[i] = a[j]; a[j] = ta; }
+    if (y[0] > y[1]) SW(0, 1);
+    if (y[1] > y[2]) SW(1, 2);
+    if (y[0] > y[1]) SW(0, 1);
+#undef SW
+    x1 = x[0]; x2 = x[1]; x3 = x[2]; y1 = y[0]; y2 = y[1]; y3 = y[2];
+    z1 = z[0]; z2 = z[1]; z3 = z[2];
+    float yd = (y2 - y1) / (y3 - y1);
+    x4 = x1 + yd * (x3 - x1);
+    z4 = z1 + yd * (z3 - z1);
+    if (alpha) {
+      uv4 = add2(a[0].uv, smul2(yd, sub2(a[2].uv, a[0].uv)));
+      if (G.flags & F_MIP) mip_setup<false>(a, z, false, nullptr, nullptr, x, y, G.tex_size, G.mip_bias);
+      uv1 = a[0].uv; uv2 = a[1].uv; uv3 = a[2].uv;
+      alen = G.alen;
+    }
+    int wc = P.view.w / TILE;
+    int tileX = bx % wc;
+    int tileY = f2i((float)bx / ((float)P.view.w / 16.f));
+    xMin = (float)tileX * 16.f;
+    xMax = ((float)tileX + 1.f) * 16.f - 1.f;
+    yMin = (float)tileY * 16.f;
+    yMax = ((float)tileY + 1.f) * 16.f - 1.f;
+    start_half0();
+    if (!live_half) start_half1();
+    return live_half;
+  }
+
+  __device__ __forceinline__ bool step(SpanV &s) {
+    s.cnt = 0;
+    s.cy = cy;
+    s.ord = make_order(1, gtri, half);
+    s.cx1 = cx1; s.cx2 = cx2; s.cz1 = cz1; s.cz2 = cz2;
+    s.g = alpha ? g : -1;
+    s.alen = alen;
+    if (alpha) { s.u1x = cu1.x; s.u1y = cu1.y; s.u2x = cu2.x; s.u2y = cu2.y; }
+    if (half == 0) {
+      if (cx2 < xMax && cx1 > xMin) {
+        s.lo = f2i(clampf_(cx2, xMin, xMax));
+        int hi = f2i(floorf(clampf_(cx1, xMin, xMax)));
+        s.cnt = hi >= s.lo ? hi - s.lo + 1 : 0;
+      }
+      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
+      if (alpha) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
+      cy++;
+      if ((float)cy <= ybound) return true;
+      start_half1();
+      return live_half;
+    }
+    if (cx1 < xMax && cx2 > xMin) {
+      s.lo = f2i(clampf_(cx1, xMin, xMax));
+      int hi = f2i(floorf(clampf_(cx2, xMin, xMax)));
+      s.cnt = hi >= s.lo ? hi - s.lo + 1 : 0;
+    }
+    cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
+    if (alpha) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
+    cy--;
+    return (float)cy >= ybound;
+  }
+};
+
+__global__ void __launch_bounds__(128) k_raster_tiled(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  __shared__ SpanV q[4][32];
+  __shared__ int pre[4][33];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
+  __syncthreads();
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t n = min(P.ctr[CTR_UNITS], P.cap_units);
+  if (P.ctr[CTR_OVERFLOW]) return;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&P.ctr[CTR_WORK_UNITS], 32u);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= n) break;
+    TileLane L;
+    bool live = false;
+    if (base + lane < n) live = L.init(P, sg, P.units[base + lane]);
+    while (__any_sync(FULL, live)) {
+      SpanV s;
+      s.cnt = 0;
+      if (live) live = L.step(s);
+      warp_fill(P, sg, q[w], pre[w], lane, s);
+    }
+  }
+}
+
+// ------------------------------------------------------------ shade
+
+// double-cascade 5-tap count: av_alpha_max.c:53-84 (shDist 2)
+__device__ __forceinline__ float shadow_light(const DrawParams &P, V3 p) {
+  int shadow = 0;
+  for (int k = 0; k < P.nsh; k++) {
+    const ShadowDev &s = P.sh[k];
+    int wS = s.dim / 2;
+    V3 pos = sub3(p, V3{s.pos[0], s.pos[1], s.pos[2]});
+    float depth = dot3(pos, V3{s.vv[0], s.vv[1], s.vv[2]});
+    int sx = f2i(dot3(pos, V3{s.vv[3], s.vv[4], s.vv[5]}) * s.scale) + wS;
+    int sy = f2i(dot3(pos, V3{s.vv[6], s.vv[7], s.vv[8]}) * -s.scale) + wS;
+    if (sx >= 2 && sx < 2 * wS - 2 && sy >= 2 && sy < 2 * wS - 2) {
+      const float *SD = s.map;
+      int r = 2 * wS;
+      if (__ldg(SD + r * sy + sx) < depth) shadow += 1;
+      if (__ldg(SD + r * (sy + 2) + sx) < depth) shadow += 1;
+      if (__ldg(SD + r * (sy - 2) + sx) < depth) shadow += 1;
+      if (__ldg(SD + r * sy + (sx + 2)) < depth) shadow += 1;
+      if (__ldg(SD + r * sy + (sx - 2)) < depth) shadow += 1;
+    }
+  }
+  shadow = min(5, shadow);
+  float light = (float)shadow * P.light.amb + (float)(5 - shadow);
+  return light * 0.2f;
+}
+
+template <class A>
+__device__ __forceinline__ void swap_(A &a, A &b) { A t = a; a = b; b = t; }
+
+// Replays the winning fragment of pixel (ax, cy) and shades it.
+__device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev *sg, int ax, int cy, uint64_t key) {
+  uint32_t ord = 0xffffffffu - (uint32_t)key;
+  if (ord == 0) return;
+  uint32_t o = ord - 1;
+  int phase = (int)(o >> 31);
+  uint32_t gtri = (o >> 1) & 0x3fffffffu;
+  int half = (int)(o & 1);
+  int g = find_group(sg, P.ngroups, gtri);
+  const GroupDev &G = sg[g];
+  int tri = (int)(gtri - G.tri_base);
+  float sx[3], sy[3], sz[3];
+  project_persp(G, tri, P.view, sx, sy, sz);
+  Attr<true> a[3];
+  float z[3], x[3], y[3];
+  int ix[3], iy[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    a[k] = a_load<true>(G, tri, k, sz[k]);
+    z[k] = sz[k];
+    x[k] = sx[k]; y[k] = sy[k];
+    ix[k] = f2i(sx[k]); iy[k] = f2i(sy[k]);
+  }
+  const bool mip = (G.flags & F_MIP) != 0;
+  MipSel ms;
+  ms.fmip = 0; ms.mip = 0; ms.len_mip = 1; ms.len_mip2 = 2; ms.start_mip = 0; ms.start_mip2 = 1;
+  float cx1, cx2, cz1, cz2;
+  Attr<true> c1, c2;
+  if (phase == 0) {
+    // direct path: integer vertices (Templates.py:230-231)
+    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(a[0], a[1]); }
+    if (iy[1] > iy[2]) { swap_(iy[1], iy[2]); swap_(ix[1], ix[2]); swap_(z[1], z[2]); swap_(a[1], a[2]); }
+    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(a[0], a[1]); }
+    int x1 = ix[0], x2 = ix[1], x3 = ix[2], y1 = iy[0], y2 = iy[1], y3 = iy[2];
+    float z1 = z[0], z2 = z[1], z3 = z[2];
+    float yd = (float)(y2 - y1) / (float)(y3 - y1);
+    float x4 = (float)x1 + yd * (float)(x3 - x1);
+    float z4 = z1 + yd * (z3 - z1);
+    Attr<true> a4 = a_add(a[0], a_smul(yd, a_sub(a[2], a[0])));
+    if (mip) ms = mip_setup<true>(a, z, true, ix, iy, nullptr, nullptr, G.tex_size, G.mip_bias);
+    float s1, s2, sz1, sz2;
+    Attr<true> sa1, sa2;
+    int n;
+    if (half == 0) {
+      float d = 1.0f / (float)(y2 - y1);
+      s1 = (float)(x2 - x1) * d; s2 = (x4 - (float)x1) * d;
+      sz1 = (z2 - z1) * d; sz2 = (z4 - z1) * d;
+      sa1 = a_mul(a_sub(a[1], a[0]), d); sa2 = a_mul(a_sub(a4, a[0]), d);
+      cx1 = cx2 = (float)x1; cz1 = cz2 = z1; c1 = c2 = a[0];
+      n = cy - y1;
+    } else {
+      float d = 1.0f / (float)(y3 - y2);
+      s1 = (float)(x3 - x2) * d; s2 = ((float)x3 - x4) * d;
+      sz1 = (z3 - z2) * d; sz2 = (z3 - z4) * d;
+      sa1 = a_mul(a_neg(a_sub(a[1], a[2])), d); sa2 = a_mul(a_neg(a_sub(a4, a[2])), d);
+      cx1 = cx2 = (float)x3; cz1 = cz2 = z3; c1 = c2 = a[2];
+      n = y3 - cy;
+    }
+    if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(sa1, sa2); }
+    if (half == 0) {
+      for (int r = 0; r < n; r++) {
+        cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2; c1 = a_add(c1, sa1); c2 = a_add(c2, sa2);
+      }
+    } else {
+      for (int r = 0; r < n; r++) {
+        cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2; c1 = a_sub(c1, sa1); c2 = a_sub(c2, sa2);
+      }
+    }
+  } else {
+    // tiled path: float vertices, per-tile restart (Templates.py:93-182)
+    if (y[0] > y[1]) { swap_(y[0], y[1]); swap_(x[0], x[1]); swap_(z[0], z[1]); swap_(a[0], a[1]); }
+    if (y[1] > y[2]) { swap_(y[1], y[2]); swap_(x[1], x[2]); swap_(z[1], z[2]); swap_(a[1], a[2]); }
+    if (y[0] > y[1]) { swap_(y[0], y[1]); swap_(x[0], x[1]); swap_(z[0], z[1]); swap_(a[0], a[1]); }
+    float x1 = x[0], x2 = x[1], x3 = x[2], y1 = y[0], y2 = y[1], y3 = y[2];
+    float z1 = z[0], z2 = z[1], z3 = z[2];
+    float yd = (y2 - y1) / (y3 - y1);
+    float x4 = x1 + yd * (x3 - x1);
+    float z4 = z1 + yd * (z3 - z1);
+    Attr<true> a4 = a_add(a[0], a_smul(yd, a_sub(a[2], a[0])));
+    if (mip) ms = mip_setup<true>(a, z, false, nullptr, nullptr, x, y, G.tex_size, G.mip_bias);
+    int tileY = cy / TILE;
+    float yMin = (float)tileY * 16.f, yMax = ((float)tileY + 1.f) * 16.f - 1.f;
+    float s1, s2, sz1, sz2;
+    Attr<true> sa1, sa2;
+    if (half == 0) {
+      float d = 1.0f / (y2 - y1);
+      s1 = (x2 - x1) * d; s2 = (x4 - x1) * d;
+      sz1 = (z2 - z1) * d; sz2 = (z4 - z1) * d;
+      sa1 = a_mul(a_sub(a[1], a[0]), d); sa2 = a_mul(a_sub(a4, a[0]), d);
+      if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(sa1, sa2); }
+      int cy0 = f2i(clampf_(y1, yMin, yMax));
+      float dy = (float)cy0 - y1;
+      cx1 = x1 + dy * s1; cx2 = x1 + dy * s2; cz1 = z1 + dy * sz1; cz2 = z1 + dy * sz2;
+      c1 = a_add(a[0], a_smul(dy, sa1)); c2 = a_add(a[0], a_smul(dy, sa2));
+      for (int r = cy0; r < cy; r++) {
+        cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2; c1 = a_add(c1, sa1); c2 = a_add(c2, sa2);
+      }
+    } else {
+      float d = 1.0f / (y3 - y2);
+      s1 = (x3 - x2) * d; s2 = (x3 - x4) * d;
+      sz1 = (z3 - z2) * d; sz2 = (z3 - z4) * d;
+      sa1 = a_mul(a_neg(a_sub(a[1], a[2])), d); sa2 = a_mul(a_neg(a_sub(a4, a[2])), d);
+      if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(sa1, sa2); }
+      int cy0 = f2i(clampf_(y3, yMin, yMax));
+      float dy = (float)cy0 - y3;
+      cx1 = x3 + dy * s1; cx2 = x3 + dy * s2; cz1 = z3 + dy * sz1; cz2 = z3 + dy * sz2;
+      c1 = a_add(a[2], a_smul(dy, sa1)); c2 = a_add(a[2], a_smul(dy, sa2));
+      for (int r = cy0; r > cy; r--) {
+        cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2; c1 = a_sub(c1, sa1); c2 = a_sub(c2, sa2);
+      }
+    }
+  }
+  float t = ((float)ax - cx2) / (cx1 - cx2);
+  t = clamp_t(t);
+  float tz = 1.0f / ((1 - t) * cz2 + t * cz1);
+  float omt = 1 - t;
+  V2 uvi = add2(smul2(omt, c2.uv), smul2(t, c1.uv));
+  float outR, outG, outB;
+  if (mip) {
+    // av_draw_normmap_mip.c:73-123
+    Taps q1 = make_taps(uvi, tz, ms.len_mip, ms.start_mip);
+    outR = bilerp_u16(q1, G.tr); outG = bilerp_u16(q1, G.tg); outB = bilerp_u16(q1, G.tb);
+    Taps q2 = make_taps(uvi, tz, ms.len_mip2, ms.start_mip2);
+    float ofm = 1 - ms.fmip;
+    outR = ofm * outR + ms.fmip * bilerp_u16(q2, G.tr);
+    outG = ofm * outG + ms.fmip * bilerp_u16(q2, G.tg);
+    outB = ofm * outB + ms.fmip * bilerp_u16(q2, G.tb);
+  } else {
+    Taps q = make_taps(uvi, tz, G.tex_size, 0);
+    outR = bilerp_u16(q, G.tr); outG = bilerp_u16(q, G.tg); outB = bilerp_u16(q, G.tb);
+  }
+  float light = 1;
+  if (G.flags & F_SHADOW) {
+    V3 p = mul3(add3(smul3(omt, c2.p), smul3(t, c1.p)), tz);
+    light = shadow_light(P, p);
+  }
+  V3 col = mul3(add3(smul3(omt, c2.li), smul3(t, c1.li)), tz);
+  V3 nrm = fast_normalize(mul3(add3(smul3(omt, c2.n), smul3(t, c1.n)), tz));
+  V3 ldir{P.light.ldir[0], P.light.ldir[1], P.light.ldir[2]};
+  V3 lint{P.light.lint[0], P.light.lint[1], P.light.lint[2]};
+  V3 dc = smul3(fmaxf(0.f, dot3(nrm, ldir)), lint);
+  float oml = 1 - light;
+  size_t pix = (size_t)P.view.w * cy + ax;
+  P.ro[pix] = u16sat(outR * (light * (dc.x + col.x) + oml * col.x));
+  P.go[pix] = u16sat(outG * (light * (dc.y + col.y) + oml * col.y));
+  P.bo[pix] = u16sat(outB * (light * (dc.z + col.z) + oml * col.z));
+  P.db[pix] = tz;
+}
+
+__global__ void __launch_bounds__(256) k_shade(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < P.ngroups; i += blockDim.x * blockDim.y)
+    sg[i] = P.groups[i];
+  __syncthreads();
+  int ax = blockIdx.x * blockDim.x + threadIdx.x;
+  int cy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ax >= P.view.w || cy >= P.view.h) return;
+  uint64_t key = P.keys[(size_t)P.view.w * cy + ax];
+  shade_pixel(P, sg, ax, cy, key);
+}
+
+// Tile-unit queue overflow: every large triangle is rasterized here instead,
+// one triangle per warp, its coarse tiles dealt round-robin to the lanes and
+// each lane filling its tiles on its own (slow, same fragments).
+__global__ void __launch_bounds__(128) k_raster_tiled_fallback(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  if (!P.ctr[CTR_OVERFLOW]) return;
+  int lane = threadIdx.x & 31;
+  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  uint32_t n = P.ctr[CTR_LARGE];
+  int wc = P.view.w / TILE, hc = P.view.h / TILE;
+  for (uint32_t i = gw; i < n; i += nw) {
+    uint32_t gt = P.large_list[i];
+    const GroupDev &G = sg[find_group(sg, P.ngroups, gt)];
+    float sx[3], sy[3], sz[3];
+    project_persp(G, (int)(gt - G.tri_base), P.view, sx, sy, sz);
+    int k = 0;
+    coarse_walk(sx, sy, wc, hc, [&](int tile) {
+      if ((k++ & 31) != lane) return;
+      TileLane L;
+      if (!L.init(P, sg, make_uint2(gt, (uint32_t)tile))) return;
+      bool more = true;
+      while (more) {
+        SpanV s;
+        more = L.step(s);
+        for (int j = 0; j < s.cnt; j++) vis_fragment(P, sg, s, s.lo + j);
+      }
+    });
+  }
+}
+
+__global__ void k_ids(const uint64_t *__restrict__ keys, int n, int32_t *tri_id, uint8_t *cov) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t ord = 0xffffffffu - (uint32_t)keys[i];
+    int32_t id = ord == 0 ? -1 : (int32_t)(((ord - 1) >> 1) & 0x3fffffffu);
+    if (tri_id) tri_id[i] = id;
+    if (cov) cov[i] = ord != 0;
+  }
+}
+
+// ------------------------------------------------------------ shadow depth pass
+
+struct ShadowParams {
+  const GroupDev *groups;
+  int ngroups;
+  int total_tris;
+  ShadowDev sh;
+  float *map;
+  float bias;
+  uint32_t *list;
+  uint32_t *ctr;
+};
+
+__global__ void __launch_bounds__(256) k_shadow_setup(ShadowParams S) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
+    int t = base + threadIdx.x;
+    bool ok = false;
+    if (t < S.total_tris) {
+      const GroupDev &G = sg[find_group(sg, S.ngroups, (uint32_t)t)];
+      if (G.enabled) {
+        int ix[3], iy[3];
+        float z[3];
+        ok = project_ortho(G, t - G.tri_base, S.sh, S.bias, ix, iy, z);
+      }
+    }
+    unsigned m = __ballot_sync(FULL, ok);
+    uint32_t b = 0;
+    if (lane == 0 && m) b = atomicAdd(&S.ctr[CTR_SH_LIST], __popc(m));
+    b = __shfl_sync(FULL, b, 0);
+    if (ok) S.list[b + __popc(m & ((1u << lane) - 1))] = (uint32_t)t;
+  }
+}
+
+__device__ __forceinline__ void atomic_min_depth(float *addr, float v) {
+  if (v >= 0.f) atomicMin((int *)addr, __float_as_int(v));
+  else atomicMax((unsigned int *)addr, __float_as_uint(v));
+}
+
+struct SpanS {
+  int cy, lo, cnt, alen;
+  float cx1, cx2, cz1, cz2;
+  float cu1, cv1, cu2, cv2;
+  const uint8_t *amask;
+};
+
+struct ShadowLane {
+  int x1, x2, x3, y1, y2, y3, x4;
+  float z1, z2, z3, z4, u1, u2, u3, u4, v1, v2, v3, v4;
+  int half, cy;
+  float s1, s2, sz1, sz2, su1, su2, sv1, sv2;
+  float cx1, cx2, cz1, cz2, cu1, cu2, cv1, cv2;
+  const uint8_t *amask;
+  int alen;
+
+  __device__ __forceinline__ void start_half0() {
+    half = 0;
+    float d = (float)(y2 - y1);
+    s1 = (float)(x2 - x1) / d;
+    s2 = (float)(x4 - x1) / d;
+    su1 = (u2 - u1) / d; sv1 = (v2 - v1) / d;
+    su2 = (u4 - u1) / d; sv2 = (v4 - v1) / d;
+    sz1 = (z2 - z1) / d; sz2 = (z4 - z1) / d;
+    cx1 = cx2 = (float)x1; cz1 = cz2 = z1;
+    cu1 = cu2 = u1; cv1 = cv2 = v1;
+    if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(su1, su2); swap_(sv1, sv2); }
+    cy = y1;
+  }
+  __device__ __forceinline__ void start_half1() {
+    half = 1;
+    float d = (float)(y3 - y2);
+    s1 = (float)(x3 - x2) / d;
+    s2 = (float)(x3 - x4) / d;
+    su1 = (u3 - u2) / d; sv1 = (v3 - v2) / d;
+    su2 = (u3 - u4) / d; sv2 = (v3 - v4) / d;
+    sz1 = (z3 - z2) / d; sz2 = (z3 - z4) / d;
+    cx1 = cx2 = (float)x3; cz1 = cz2 = z3;
+    cu1 = cu2 = u3; cv1 = cv2 = v3;
+    if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(su1, su2); swap_(sv1, sv2); }
+    cy = y3;
+  }
+
+  __device__ __forceinline__ bool init(const ShadowParams &S, const GroupDev *sg, uint32_t t) {
+    const GroupDev &G = sg[find_group(sg, S.ngroups, t)];
+    int tri = (int)(t - G.tri_base);
+    int ix[3], iy[3];
+    float z[3];
+    project_ortho(G, tri, S.sh, S.bias, ix, iy, z);
+    V2 uv[3] = {V2{0, 0}, V2{0, 0}, V2{0, 0}};
+    amask = (G.flags & F_ALPHA) ? G.amask : nullptr;
+    alen = G.alen;
+    if (amask) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) uv[k] = mul2(ld2(G.uv + ((size_t)tri * 3 + k) * 2), z[k]);
+    }
+    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(uv[0], uv[1]); }
+    if (iy[1] > iy[2]) { swap_(iy[1], iy[2]); swap_(ix[1], ix[2]); swap_(z[1], z[2]); swap_(uv[1], uv[2]); }
+    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(uv[0], uv[1]); }
+    x1 = ix[0]; x2 = ix[1]; x3 = ix[2]; y1 = iy[0]; y2 = iy[1]; y3 = iy[2];
+    z1 = z[0]; z2 = z[1]; z3 = z[2];
+    if (!((y1 < S.sh.dim) && (y3 >= 0))) return false;
+    u1 = uv[0].x; u2 = uv[1].x; u3 = uv[2].x; v1 = uv[0].y; v2 = uv[1].y; v3 = uv[2].y;
+    float q = (float)(y2 - y1) / (float)(y3 - y1);
+    x4 = f2i((float)x1 + q * (float)(x3 - x1));
+    z4 = z1 + q * (z3 - z1);
+    u4 = u1 + q * (u3 - u1);
+    v4 = v1 + q * (v3 - v1);
+    start_half0();
+    if (cy > y2) {               // no bottom rows
+      start_half1();
+      return cy > y2;
+    }
+    return true;
+  }
+
+  __device__ __forceinline__ bool step(int dim, SpanS &s) {
+    s.cnt = 0;
+    s.cy = cy;
+    s.cx1 = cx1; s.cx2 = cx2; s.cz1 = cz1; s.cz2 = cz2;
+    s.cu1 = cu1; s.cv1 = cv1; s.cu2 = cu2; s.cv2 = cv2;
+    s.amask = amask;
+    s.alen = alen;
+    if (cy >= 0 && cy < dim) {
+      int a0 = half == 0 ? f2i(cx2) : f2i(cx1);
+      int a1 = half == 0 ? f2i(cx1) : f2i(cx2);
+      int lo = a0 < 0 ? 0 : a0, hi = a1 > dim - 1 ? dim - 1 : a1;
+      s.lo = lo;
+      s.cnt = hi >= lo ? hi - lo + 1 : 0;
+    }
+    if (half == 0) {
+      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
+      cu1 += su1; cv1 += sv1; cu2 += su2; cv2 += sv2;
+      cy++;
+      if (cy <= y2) return true;
+      start_half1();
+      return cy > y2;
+    }
+    cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
+    cu1 -= su1; cv1 -= sv1; cu2 -= su2; cv2 -= sv2;
+    cy--;
+    return cy > y2;
+  }
+};
+
+__device__ __forceinline__ void shadow_fragment(float *map, int dim, const SpanS &s, int ax) {
+  float t = ((float)ax - s.cx2) / (s.cx1 - s.cx2);
+  t = clamp_t(t);
+  float tz = 1.0f / ((1 - t) * s.cz2 + t * s.cz1);
+  if (tz != tz) return;
+  if (s.amask) {
+    int len = s.alen;
+    float lm1 = (float)(len - 1);
+    int t1 = f2i((((1 - t) * s.cu2 + t * s.cu1) * tz) * lm1);
+    t1 = iabs_(t1) & (len - 1);
+    int t2 = f2i((lm1 * ((1 - t) * s.cv2 + t * s.cv1)) * tz);
+    t2 = iabs_(t2) & (len - 1);
+    if (!__ldg(s.amask + t1 + t2 * len)) return;
+  }
+  atomic_min_depth(map + (size_t)dim * s.cy + ax, tz);
+}
+
+__global__ void __launch_bounds__(128) k_shadow_raster(ShadowParams S) {
+  __shared__ GroupDev sg[64];
+  __shared__ SpanS q[4][32];
+  __shared__ int pre[4][33];
+  for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
+  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
+  __syncthreads();
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t n = S.ctr[CTR_SH_LIST];
+  int dim = S.sh.dim;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&S.ctr[CTR_SH_WORK], 32u);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= n) break;
+    ShadowLane L;
+    bool live = false;
+    if (base + lane < n) live = L.init(S, sg, S.list[base + lane]);
+    while (__any_sync(FULL, live)) {
+      SpanS s;
+      s.cnt = 0;
+      if (live) live = L.step(dim, s);
+      int c = s.cnt, incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int total = __shfl_sync(FULL, incl, 31);
+      if (total == 0) continue;
+      q[w][lane] = s;
+      pre[w][lane] = incl - c;
+      __syncwarp();
+      for (int p = lane; p < total; p += 32) {
+        int k = 0;
+#pragma unroll
+        for (int st = 16; st; st >>= 1)
+          if (pre[w][k + st] <= p) k += st;
+        shadow_fragment(S.map, dim, q[w][k], q[w][k].lo + (p - pre[w][k]));
+      }
+      __syncwarp();
+    }
+  }
+}
+
+}  // namespace axr

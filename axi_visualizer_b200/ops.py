@@ -1,0 +1,306 @@
+"""CLDraw: drop-in for the reference's draw runtime (PyOpenCL27C/Ops.py:127-1230,
+PyOpenCL27C/Ops0.py:93-910), backed by libaxr.so on a B200.
+
+Same method names, argument meanings and return types as the reference's
+class, which the engine holds as `ThreeDBackend.draw`
+(PyOpenCL27C/Compute.py:182-229,313-339,381-383,426-460).  Differences that
+a caller can see:
+  - errors raise `AxrError` (the reference raises pyopencl errors)
+  - `getIDs()` is new: triangle id and coverage of the last drawAll
+  - effects outside the rasterizer hot path (sky, particles, reflections,
+    SSR, cubemap re-layout, GI buffers, bones, waves) are not provided:
+    their methods raise NotImplementedError, except setSkyTex, which the
+    engine calls unconditionally and which is accepted and ignored.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import AxrError, check, lib
+from .scenes import flags_from_string, view_mat
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+class CLDraw:
+    def __init__(self, size_sky, max_uv, w, h, max_particles, device=0, pinned=False):
+        self.W, self.H = int(w), int(h)
+        self.WC, self.HC = self.W // 16, self.H // 16
+        self.LT = max_uv
+        self._L = lib()
+        h_ = C.c_void_p()
+        check(self._L.axr_create(self.W, self.H, int(device), C.byref(h_)), "axr_create")
+        self._h = h_
+        self.gSize = []           # vertex counts per group (reference name)
+        self.texSize = []
+        self._tex_alpha = 0
+        self.SHADOWMAP = {}
+        self.ambLight = np.float32(0.2)
+        self._pinned = pinned
+        self.hro = self._host((self.H, self.W), np.uint16)
+        self.hgo = self._host((self.H, self.W), np.uint16)
+        self.hbo = self._host((self.H, self.W), np.uint16)
+        self.hdb = self._host((self.H, self.W), np.float32)
+
+    def _host(self, shape, dtype):
+        if self._pinned:
+            import torch
+            t = torch.empty(shape, dtype={np.uint16: torch.uint16, np.float32: torch.float32,
+                                          np.int32: torch.int32, np.uint8: torch.uint8}[dtype], pin_memory=True)
+            self.__dict__.setdefault("_pins", []).append(t)
+            return t.numpy()
+        return np.ones(shape, dtype)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._L.axr_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ set-up
+    def setScaleCull(self, s, cx, cy):
+        self.sScale = np.float32(s)
+        self.caX, self.caY = np.float32(cx), np.float32(cy)
+        check(self._L.axr_set_scale_cull(self._h, float(self.sScale), float(self.caX), float(self.caY)), "setScaleCull")
+
+    def setSkyTex(self, r, g, b, size):
+        """Accepted for compatibility; the sky pass is outside this library."""
+        self.skyTexSize = np.int32(size)
+
+    def addTextureGroup(self, xyz, uv, vn, r, g, b, mip=False):
+        p = _f32(np.asarray(xyz).reshape(-1, 3))
+        n = _f32(np.asarray(vn).reshape(-1, 3))
+        t = _f32(np.asarray(uv).reshape(-1, 2))
+        if p.shape[0] % 3 or n.shape != p.shape or t.shape[0] != p.shape[0]:
+            raise AxrError("addTextureGroup: xyz, uv and vn must hold 3 vertices per triangle")
+        rr = np.ascontiguousarray(np.asarray(r).astype(np.uint16).reshape(-1))
+        gg = np.ascontiguousarray(np.asarray(g).astype(np.uint16).reshape(-1))
+        bb = np.ascontiguousarray(np.asarray(b).astype(np.uint16).reshape(-1))
+        out = C.c_int()
+        check(self._L.axr_add_texture_group(self._h, _p(p), _p(t), _p(n), p.shape[0] // 3, _p(rr), _p(gg), _p(bb),
+                                            rr.size, int(mip) if mip else 0, C.byref(out)), "addTextureGroup")
+        self.gSize.append(np.int32(p.shape[0]))
+        self.texSize.append(np.int32(np.log2(mip)) if mip else np.int32(int(round(rr.size ** 0.5))))
+        return out.value
+
+    def setVertLight(self, tn, li):
+        """Uploads the per-vertex light `I` of group tn (what vertLight computes)."""
+        a = _f32(np.asarray(li).reshape(-1, 3))
+        check(self._L.axr_set_vert_light(self._h, int(tn), _p(a)), "setVertLight")
+
+    def vertLight(self, mask, dirI, dirD, pointI=None, pointP=None, spotI=None, spotD=None, spotP=None):
+        """Per-vertex lighting from directional lights 1.. (vert.c vertL)."""
+        for extra in (pointI, spotI):
+            if extra is not None and not (isinstance(extra, int) and extra == 1) and len(np.atleast_1d(extra)):
+                raise NotImplementedError("point/spot lights of vertLight are outside this library")
+        i = _f32(np.asarray(dirI).reshape(-1, 3))
+        d = _f32(np.asarray(dirD).reshape(-1, 3))
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
+        check(self._L.axr_vert_light(self._h, _p(m), len(self.gSize), _p(i), _p(d), i.shape[0],
+                                     float(self.ambLight)), "vertLight")
+
+    def copyTo(self, tn, vp, vn, cstart=0):
+        p = _f32(np.asarray(vp).reshape(-1, 3))
+        n = _f32(np.asarray(vn).reshape(-1, 3))
+        check(self._L.axr_copy_to(self._h, int(tn), _p(p), _p(n), int(cstart), p.shape[0] // 3), "copyTo")
+
+    def addTexAlpha(self, a):
+        a = np.asarray(a)
+        m = np.ascontiguousarray(a.astype(bool).astype(np.uint8).reshape(-1))
+        side = a.shape[0] if a.ndim == 2 else int(round(m.size ** 0.5))
+        out = C.c_int()
+        check(self._L.axr_add_tex_alpha(self._h, _p(m), side, C.byref(out)), "addTexAlpha")
+        return out.value
+
+    def setPrimaryLight(self, dirI, dirD):
+        i = _f32(np.asarray(dirI).reshape(-1, 3)[0])
+        d = _f32(np.asarray(dirD).reshape(-1, 3)[0])
+        check(self._L.axr_set_primary_light(self._h, _p(i), _p(d)), "setPrimaryLight")
+
+    def setPos(self, vc):
+        check(self._L.axr_set_pos(self._h, _p(_f32(np.asarray(vc).reshape(3)))), "setPos")
+
+    def setVM(self, vM):
+        check(self._L.axr_set_vm(self._h, _p(_f32(np.asarray(vM)[:3, :3].reshape(9)))), "setVM")
+
+    # ------------------------------------------------------------ frame
+    def clearZBuffer(self):
+        check(self._L.axr_clear_zbuffer(self._h), "clearZBuffer")
+
+    def _material_args(self, shaders):
+        n = len(self.gSize)
+        if isinstance(shaders, dict):
+            shaders = [shaders.get(i, "") for i in range(n)]
+        if len(shaders) != n:
+            raise AxrError(f"drawAll: {len(shaders)} shaders for {n} groups")
+        flags = np.zeros(n, np.int32)
+        aidx = np.zeros(n, np.int32)
+        for i, s in enumerate(shaders):
+            flags[i] = flags_from_string(s)
+            if isinstance(s, dict) and "alpha" in s:
+                aidx[i] = int(s["alpha"])
+        return flags, aidx
+
+    def drawAll(self, shaders, mask=None, shadowIds=(0, 1), useOpacitySM=False):
+        flags, aidx = self._material_args(shaders)
+        m = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
+        ids = [int(i) for i in shadowIds if int(i) in self.SHADOWMAP][:2]
+        sid = np.asarray(ids + [0, 0], np.int32)[:2]
+        check(self._L.axr_draw_all(self._h, _p(flags), _p(aidx), _p(m), len(flags), _p(sid), len(ids)), "drawAll")
+
+    def getFrame(self):
+        check(self._L.axr_get_frame(self._h, _p(self.hro), _p(self.hgo), _p(self.hbo), _p(self.hdb)), "getFrame")
+        return (self.hro, self.hgo, self.hbo, self.hdb)
+
+    def getIDs(self):
+        tid = np.empty((self.H, self.W), np.int32)
+        cov = np.empty((self.H, self.W), np.uint8)
+        check(self._L.axr_get_ids(self._h, _p(tid), _p(cov)), "getIDs")
+        return tid, cov
+
+    def setFrame(self, r=None, g=None, b=None, depth=None):
+        arrs = [None if a is None else np.ascontiguousarray(a) for a in (r, g, b, depth)]
+        check(self._L.axr_set_frame(self._h, *[_p(a) for a in arrs]), "setFrame")
+
+    def gamma(self, ex):
+        check(self._L.axr_gamma(self._h, float(ex)), "gamma")
+
+    # ------------------------------------------------------------ shadows
+    def addShadowMap(self, i, size, scale, ambLight=None, useGI=False):
+        if useGI:
+            raise NotImplementedError("GI shadow buffers are outside this library")
+        if ambLight is not None:
+            self.ambLight = np.float32(ambLight)
+        check(self._L.axr_add_shadow_map(self._h, int(i), int(size), float(np.float32(scale)),
+                                         float(self.ambLight)), "addShadowMap")
+        self.SHADOWMAP[int(i)] = {"dim": np.int32(size), "dim2": np.int32(size / 2), "scale": np.float32(scale)}
+
+    def placeShadowMap(self, i, pos, facing, ambLight=None):
+        f = _f32(view_mat(*facing))
+        p = _f32(np.asarray(pos).reshape(3))
+        if ambLight is not None:
+            self.ambLight = np.float32(ambLight)
+        check(self._L.axr_place_shadow_map(self._h, int(i), _p(p), _p(f.reshape(9)), float(self.ambLight)),
+              "placeShadowMap")
+        self.SHADOWMAP[int(i)]["vecnp"] = f
+
+    def placeShadowMapBasis(self, i, pos, basis, ambLight=None):
+        """placeShadowMap with the 3x3 basis given directly (rows: depth, x, y)."""
+        p = _f32(np.asarray(pos).reshape(3))
+        f = _f32(np.asarray(basis).reshape(9))
+        if ambLight is not None:
+            self.ambLight = np.float32(ambLight)
+        check(self._L.axr_place_shadow_map(self._h, int(i), _p(p), _p(f), float(self.ambLight)), "placeShadowMap")
+
+    def clearShadowMap(self, i):
+        check(self._L.axr_clear_shadow_map(self._h, int(i)), "clearShadowMap")
+
+    def shadowMap(self, i, whichCast, shaders, bias, proj="ortho"):
+        if proj != "ortho":
+            raise NotImplementedError("only orthographic shadow maps")
+        n = len(self.gSize)
+        cast = np.ascontiguousarray(np.asarray([bool(c) for c in whichCast], np.uint8))
+        flags = np.zeros(n, np.int32)
+        aidx = np.zeros(n, np.int32)
+        for k in range(n):
+            s = shaders[k] if not isinstance(shaders, dict) else shaders.get(k, "")
+            if isinstance(s, (bool, int, np.integer)) and not isinstance(s, str):
+                # Ops0.shadowMap passes useAlpha: 0 or alpha index + 1
+                if int(s):
+                    flags[k] = 2
+                    aidx[k] = int(s) - 1
+            else:
+                flags[k] = flags_from_string(s)
+                if isinstance(s, dict) and "alpha" in s:
+                    aidx[k] = int(s["alpha"])
+        check(self._L.axr_shadow_map(self._h, int(i), _p(cast), _p(flags), _p(aidx), n, float(np.float32(bias))),
+              "shadowMap")
+
+    def getSHM(self, i):
+        d = int(self.SHADOWMAP[int(i)]["dim"])
+        out = np.empty((d, d), np.float32)
+        check(self._L.axr_get_shadow_map(self._h, int(i), _p(out)), "getSHM")
+        return out
+
+    # ------------------------------------------------------------ misc
+    def sync(self):
+        check(self._L.axr_sync(self._h), "sync")
+
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        check(self._L.axr_get_stream(self._h, C.byref(s)), "getStream")
+        return s.value or 0
+
+    def device_ptrs(self):
+        ptrs = [C.c_void_p() for _ in range(5)]
+        check(self._L.axr_frame_device_ptrs(self._h, *[C.byref(p) for p in ptrs]), "device_ptrs")
+        return [p.value for p in ptrs]
+
+    def lastStats(self):
+        vals = [C.c_int64() for _ in range(4)]
+        check(self._L.axr_last_stats(self._h, *[C.byref(v) for v in vals]), "lastStats")
+        return {"kernels": vals[0].value, "n_small": vals[1].value, "n_large": vals[2].value, "n_units": vals[3].value}
+
+    def __getattr__(self, name):
+        if name in ("addTexture", "setReflTex", "setHostSkyTex", "addBoneWeights", "initBoneTransforms",
+                    "setBoneTransform", "boneTransform", "rotate", "translate", "setupWave", "updateWave",
+                    "highlight", "blur", "drawDirectional", "getGIM", "addOpacityMap", "clearShadowOpMap",
+                    "shadowClouds", "shadowCloudsOpacity", "tonemap", "mipShadowMap", "setPSTex", "drawPS"):
+            raise NotImplementedError(f"CLDraw.{name} belongs to an effect outside the rasterizer hot path")
+        raise AttributeError(name)
+
+
+# ---------------------------------------------------------------- scene helper
+
+class SceneRenderer:
+    """Loads a scenes.Scene into a CLDraw and renders views of it."""
+
+    def __init__(self, scene, w, h, device=0, pinned=False):
+        self.scene = scene
+        self.draw = CLDraw(1, 64, w, h, 1, device=device, pinned=pinned)
+        for g in scene.groups:
+            r, gg, b = g.tex
+            mip = (1 << g.tex_size) if g.flags & 1 else False
+            self.draw.addTextureGroup(g.xyz, g.uv, g.vn, r, gg, b, mip=mip)
+        for k, g in enumerate(scene.groups):
+            self.draw.setVertLight(k, g.li)
+        for m, side in scene.alphas:
+            self.draw.addTexAlpha(np.asarray(m).reshape(side, side))
+        self.draw.setPrimaryLight(np.asarray(scene.lint)[None], np.asarray(scene.ldir)[None])
+        self.draw.ambLight = np.float32(scene.amb)
+        for k, sc in enumerate(scene.shadows):
+            self.draw.addShadowMap(k, sc.dim, sc.scale, scene.amb)
+            self.draw.placeShadowMapBasis(k, sc.pos, sc.vv, scene.amb)
+        self.flags = [g.flags for g in scene.groups]
+        self.shaders = [{"alpha": g.alpha_index, **{k: 1 for k, b in (("mip", 1), ("shadow", 4), ("cull", 8))
+                                                     if g.flags & b}} if g.flags & 2 else
+                        " ".join(k for k, b in (("mip", 1), ("shadow", 4), ("cull", 8)) if g.flags & b)
+                        for g in scene.groups]
+
+    def shadow_pass(self):
+        for k in range(len(self.scene.shadows)):
+            self.draw.clearShadowMap(k)
+            self.draw.shadowMap(k, [g.cast for g in self.scene.groups], self.shaders, self.scene.bias)
+
+    def set_view(self, view):
+        self.draw.setScaleCull(view.sscale, view.cax, view.cay)
+        self.draw.setPos(view.pos)
+        self.draw.setVM(view.vv)
+
+    def frame(self, view, shadows=True):
+        """shadow maps, clear, drawAll (the per-frame hot path)."""
+        if shadows:
+            self.shadow_pass()
+        self.set_view(view)
+        self.draw.clearZBuffer()
+        self.draw.drawAll(self.shaders, shadowIds=list(range(min(2, len(self.scene.shadows)))))

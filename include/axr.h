@@ -1,0 +1,161 @@
+/*
+ * axr.h -- C ABI of libaxr.so, the B200 (sm_100a) implementation of the
+ * AXI Visualizer rasterizer hot path: tiled scanline rasterization with
+ * depth test, perspective-correct textured shading (bilinear / trilinear
+ * mip, alpha test, double-cascade shadow lookup) and the shadow-map depth
+ * pass.
+ *
+ * The entry points replace the methods of the reference's draw runtime,
+ * class CLDraw in PyOpenCL27C/Ops.py (and Ops0.py), which the engine holds
+ * as ThreeDBackend.draw (PyOpenCL27C/Compute.py:182-187).  Each declaration
+ * cites the method it stands in for.  Plain pointers and sizes only; host
+ * pointers are borrowed for the duration of the call.
+ *
+ * Errors: every function returns 0 on success and a negative AXR_E* code on
+ * failure; axr_last_error() gives a message for the calling thread.  A
+ * handle is not thread-safe; separate handles may be used from separate
+ * threads.  All work of one handle runs in order on its own CUDA stream.
+ */
+#ifndef AXR_H
+#define AXR_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AXR_OK 0
+#define AXR_EINVAL -1   /* bad argument */
+#define AXR_ECUDA -2    /* CUDA runtime error */
+#define AXR_ENOMEM -3   /* device allocation failed */
+#define AXR_EOVERFLOW -4 /* a work queue overflowed; the call was not completed */
+#define AXR_ESTATE -5   /* call out of order (e.g. shading with no shadow map) */
+
+/* material flags: the substrings CLDraw.drawAll tests in the material
+ * strings (Ops.py:737-740,772-805; VertObjects.py:142-151) */
+#define AXR_MIP 1     /* "mip": trilinear mip chain, tex_size = log2(side) */
+#define AXR_ALPHA 2   /* "alpha": bilinear boolean alpha test before depth */
+#define AXR_SHADOW 4  /* "shadow": double-cascade 5-tap shadow lookup */
+#define AXR_CULL 8    /* "cull": back-face rejection (trisetup_cull.c:49-54) */
+
+typedef struct axr_ctx axr_ctx;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *axr_last_error(void);
+
+/* CLDraw.__init__(size_sky, max_uv, w, h, max_particles) (Ops.py:127-229):
+ * framebuffers of w x h (w a multiple of 16; the tile grid is w/16 x h/16,
+ * Ops.py:131-132) on CUDA device `device`. */
+int axr_create(int w, int h, int device, axr_ctx **out);
+
+/* Releases every device buffer of the handle (the reference never frees). */
+int axr_destroy(axr_ctx *ctx);
+
+/* CLDraw.setScaleCull(s, cx, cy) (Ops.py:231-233) */
+int axr_set_scale_cull(axr_ctx *ctx, float sscale, float cax, float cay);
+
+/* CLDraw.addTextureGroup(xyz, uv, vn, r, g, b, mip) (Ops.py:331-378):
+ * ntris triangles as 3*ntris vertices: xyz [3*ntris][3], uv [3*ntris][2],
+ * vn [3*ntris][3]; texture planes r, g, b of `ntexels` uint16 each (one
+ * side*side level, or the full mip chain smallest level first when
+ * mip_side > 0, Utils.createMips).  tex_size is the reference's texSize:
+ * side, or log2(side) for mip.  Returns the group id in *out_id. */
+int axr_add_texture_group(axr_ctx *ctx, const float *xyz, const float *uv, const float *vn, int ntris,
+                          const uint16_t *r, const uint16_t *g, const uint16_t *b, long ntexels,
+                          int mip_side, int *out_id);
+
+/* Per-vertex light `I` of a group ([3*ntris][3]); CLDraw.vertLight fills the
+ * same LI buffer on the device (Ops.py:552-612, vert.c:38-87).  Groups start
+ * with I = 0. */
+int axr_set_vert_light(axr_ctx *ctx, int group, const float *li);
+
+/* CLDraw.vertLight(mask, dirI, dirD) for directional lights only: computes
+ * I = max(sum_{i>=1} max(0, dot(n, dir_i) + 0.5) * 0.66 * int_i, ambLight)
+ * on the device for every group whose mask entry is non-zero
+ * (vert.c:38-87; light 0 is the per-pixel primary light). */
+int axr_vert_light(axr_ctx *ctx, const uint8_t *mask, int ngroups, const float *dir_int, const float *dir_dir,
+                   int ndirs, float amb);
+
+/* CLDraw.copyTo(tn, vp, vn, cstart) (Ops.py:448-452): overwrite vertices
+ * [3*tri_start, 3*(tri_start+ntris)) of a group. */
+int axr_copy_to(axr_ctx *ctx, int group, const float *xyz, const float *vn, int tri_start, int ntris);
+
+/* CLDraw.addTexAlpha(a) (Ops.py:454-456): boolean alpha mask side x side. */
+int axr_add_tex_alpha(axr_ctx *ctx, const uint8_t *mask, int side, int *out_id);
+
+/* CLDraw.setPrimaryLight(dirI, dirD) (Ops.py:1143-1151) */
+int axr_set_primary_light(axr_ctx *ctx, const float dir_int[3], const float dir_dir[3]);
+
+/* CLDraw.setPos(vc) / setVM(vM) (Ops.py:475-479): camera position and
+ * view basis rows [view vector, horizontal, vertical]. */
+int axr_set_pos(axr_ctx *ctx, const float pos[3]);
+int axr_set_vm(axr_ctx *ctx, const float vm[9]);
+
+/* CLDraw.clearZBuffer() (Ops0.py:650-653, clearzb.c): depth := 65535 on the
+ * [0, w/4*4) x [0, h/4*4) region the reference's 4x4 work-items cover. */
+int axr_clear_zbuffer(axr_ctx *ctx);
+
+/* CLDraw.drawAll(shaders, mask, shadowIds) (Ops0.py:471-648, Ops.py:716-937):
+ * flags[g] (AXR_*), alpha_index[g] (alpha mask of alpha groups; may be
+ * NULL = 0), mask[g] != 0 skips group g (may be NULL).  shadow_ids lists
+ * the shadow maps (cascades, at most 2) that AXR_SHADOW groups sample. */
+int axr_draw_all(axr_ctx *ctx, const int32_t *flags, const int32_t *alpha_index, const uint8_t *mask, int ngroups,
+                 const int32_t *shadow_ids, int nshadow);
+
+/* CLDraw.getFrame() (Ops.py:1224-1230): copies the three uint16 colour
+ * planes and the float depth ([h][w] each) into host buffers; any pointer
+ * may be NULL to skip that plane.  Synchronises the handle's stream. */
+int axr_get_frame(axr_ctx *ctx, uint16_t *r, uint16_t *g, uint16_t *b, float *depth);
+
+/* Visibility of the last drawAll (new outputs, not in the reference):
+ * tri_id = global triangle id (group base + index) of the visible fragment,
+ * -1 where drawAll wrote nothing; coverage = 1 where it wrote.  Either
+ * pointer may be NULL. */
+int axr_get_ids(axr_ctx *ctx, int32_t *tri_id, uint8_t *coverage);
+
+/* Uploads host depth/colour (tests and resume). Any pointer may be NULL. */
+int axr_set_frame(axr_ctx *ctx, const uint16_t *r, const uint16_t *g, const uint16_t *b, const float *depth);
+
+/* CLDraw.gamma(ex) (Ops0.py:654-660, Post/gamma.c) on the colour planes. */
+int axr_gamma(axr_ctx *ctx, float exposure);
+
+/* CLDraw.addShadowMap(i, size, scale, ambLight) (Ops.py:1048-1070) */
+int axr_add_shadow_map(axr_ctx *ctx, int i, int size, float scale, float amb_light);
+
+/* CLDraw.placeShadowMap(i, pos, facing, ambLight) (Ops.py:1078-1087): vm are
+ * the rows of Utils.viewMat(*facing). amb_light < 0 keeps the current one. */
+int axr_place_shadow_map(axr_ctx *ctx, int i, const float pos[3], const float vm[9], float amb_light);
+
+/* CLDraw.clearShadowMap(i) (Ops.py:1022-1028): 65535 over the 16x16 blocks. */
+int axr_clear_shadow_map(axr_ctx *ctx, int i);
+
+/* CLDraw.shadowMap(i, whichCast, shaders, bias) (Ops.py:1089-1141):
+ * ortho setup (trisetupOrtho.c) and depth-min raster (drawmin.c, or the
+ * alpha-tested drawminalpha.c for AXR_ALPHA groups) of every group with
+ * cast[g] != 0. */
+int axr_shadow_map(axr_ctx *ctx, int i, const uint8_t *cast, const int32_t *flags, const int32_t *alpha_index,
+                   int ngroups, float bias);
+
+/* CLDraw.getSHM(i) (Ops.py:1218-1222): copies the size x size depth map. */
+int axr_get_shadow_map(axr_ctx *ctx, int i, float *out);
+
+/* Blocks until all work queued on the handle has finished. */
+int axr_sync(axr_ctx *ctx);
+
+/* The handle's CUDA stream (a cudaStream_t), so callers can time or order
+ * work against it (e.g. torch.cuda.ExternalStream). */
+int axr_get_stream(axr_ctx *ctx, void **stream);
+
+/* Device pointers of the framebuffers ([h][w]; keys are the 64-bit
+ * depth/order visibility words of the last drawAll) for zero-copy users. */
+int axr_frame_device_ptrs(axr_ctx *ctx, void **r, void **g, void **b, void **depth, void **keys);
+
+/* Launch statistics of the last drawAll: number of kernels launched and
+ * work-queue sizes (small triangles, large triangles, tile units). */
+int axr_last_stats(axr_ctx *ctx, int64_t *kernels, int64_t *n_small, int64_t *n_large, int64_t *n_units);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
