@@ -18,7 +18,7 @@ EXPORTS = [
     "axr_set_pos", "axr_set_vm", "axr_clear_zbuffer", "axr_draw_all", "axr_get_frame", "axr_get_ids",
     "axr_set_frame", "axr_gamma", "axr_add_shadow_map", "axr_place_shadow_map", "axr_clear_shadow_map",
     "axr_shadow_map", "axr_get_shadow_map", "axr_sync", "axr_get_stream", "axr_frame_device_ptrs",
-    "axr_last_stats",
+    "axr_last_stats", "axr_launch_count", "axr_set_kernel_timing", "axr_kernel_times",
 ]
 
 vp = C.c_void_p
@@ -54,6 +54,10 @@ _SIGS = {
     "axr_frame_device_ptrs": (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "axr_last_stats": (i32, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                              C.POINTER(C.c_int64)]),
+    "axr_launch_count": (i32, [vp, C.POINTER(C.c_int64)]),
+    "axr_set_kernel_timing": (i32, [vp, i32]),
+    "axr_kernel_times": (i32, [vp, i32, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                               C.POINTER(i32)]),
 }
 
 _lib = None

@@ -89,6 +89,14 @@ struct axr_ctx {
   Shadow shadows[MAX_SHADOWS];
   int64_t last_kernels = 0;
   bool pending = false;
+  // launch accounting and optional per-kernel CUDA-event timing
+  int64_t launches = 0;
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  struct Pending { const char *name; cudaEvent_t a, b; };
+  std::vector<Pending> tpend;
+  struct Acc { std::string name; double ms; int64_t n; };
+  std::vector<Acc> tacc;
 };
 
 namespace {
@@ -119,9 +127,15 @@ int grow_units(axr_ctx *c, uint32_t need) {
   return 0;
 }
 
+void collect_times(axr_ctx *c);
+
 // Reads the counters of the last drawAll; grows the unit queue after an
 // overflow (that frame was completed by the fallback kernel).
 int settle(axr_ctx *c) {
+  if (!c->tpend.empty()) {
+    CK(cudaStreamSynchronize(c->stream));
+    collect_times(c);
+  }
   if (!c->pending) return 0;
   CK(cudaStreamSynchronize(c->stream));
   c->pending = false;
@@ -133,6 +147,51 @@ int check_ctx(axr_ctx *c) {
   if (!c) return fail(AXR_EINVAL, "null handle");
   CK(cudaSetDevice(c->device));
   return 0;
+}
+
+cudaEvent_t ev_get(axr_ctx *c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Launches one kernel through `f`, counting it and, when timing is on,
+// bracketing it with events on the handle's stream.
+template <class F>
+void launch(axr_ctx *c, const char *name, F f) {
+  cudaEvent_t a = nullptr;
+  if (c->timing) {
+    a = ev_get(c);
+    cudaEventRecord(a, c->stream);
+  }
+  f();
+  c->launches++;
+  if (c->timing) {
+    cudaEvent_t b = ev_get(c);
+    cudaEventRecord(b, c->stream);
+    c->tpend.push_back({name, a, b});
+  }
+}
+
+// Folds the finished event pairs into the per-kernel totals.
+void collect_times(axr_ctx *c) {
+  for (auto &p : c->tpend) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      bool found = false;
+      for (auto &acc : c->tacc)
+        if (acc.name == p.name) { acc.ms += ms; acc.n++; found = true; break; }
+      if (!found) c->tacc.push_back({p.name, (double)ms, 1});
+    }
+    c->ev_pool.push_back(p.a);
+    c->ev_pool.push_back(p.b);
+  }
+  c->tpend.clear();
 }
 
 template <class T>
@@ -262,6 +321,8 @@ int axr_destroy(axr_ctx *c) {
   cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->sh_list); cudaFree(c->units);
   cudaFree(c->ctr); cudaFree(c->d_groups);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  for (auto &p : c->tpend) { c->ev_pool.push_back(p.a); c->ev_pool.push_back(p.b); }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -399,7 +460,7 @@ int axr_set_vm(axr_ctx *c, const float vm[9]) {
 int axr_clear_zbuffer(axr_ctx *c) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  k_clear_depth<<<grid_for(c, (long)c->w * c->h, 256, 8), 256, 0, c->stream>>>(c->db, c->w, c->h, 4);
+  launch(c, "k_clear_depth", [&] { k_clear_depth<<<grid_for(c, (long)c->w * c->h, 256, 8), 256, 0, c->stream>>>(c->db, c->w, c->h, 4); });
   CK(cudaGetLastError());
   return 0;
 }
@@ -441,16 +502,16 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   long npix = (long)c->w * c->h;
   cudaStream_t s = c->stream;
   int64_t nk = 0;
-  k_init_keys<<<grid_for(c, npix, 256, 16), 256, 0, s>>>(c->db, c->keys, (int)npix, c->ctr); nk++;
+  launch(c, "k_init_keys", [&] { k_init_keys<<<grid_for(c, npix, 256, 16), 256, 0, s>>>(c->db, c->keys, (int)npix, c->ctr); }); nk++;
   if (c->total_tris > 0) {
-    k_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, s>>>(P); nk++;
-    k_raster_small<<<c->sms * 8, 128, 0, s>>>(P); nk++;
-    k_coarse<<<c->sms * 4, 128, 0, s>>>(P); nk++;
-    k_raster_tiled<<<c->sms * 8, 128, 0, s>>>(P); nk++;
-    k_raster_tiled_fallback<<<c->sms * 2, 128, 0, s>>>(P); nk++;
+    launch(c, "k_setup", [&] { k_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, s>>>(P); }); nk++;
+    launch(c, "k_raster_small", [&] { k_raster_small<<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
+    launch(c, "k_coarse", [&] { k_coarse<<<c->sms * 4, 128, 0, s>>>(P); }); nk++;
+    launch(c, "k_raster_tiled", [&] { k_raster_tiled<<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
+    launch(c, "k_raster_tiled_fallback", [&] { k_raster_tiled_fallback<<<c->sms * 2, 128, 0, s>>>(P); }); nk++;
   }
   dim3 sb(16, 16), sgd((c->w + 15) / 16, (c->h + 15) / 16);
-  k_shade<<<sgd, sb, 0, s>>>(P); nk++;
+  launch(c, "k_shade", [&] { k_shade<<<sgd, sb, 0, s>>>(P); }); nk++;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_ctr, c->ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
   c->pending = true;
@@ -507,7 +568,7 @@ int axr_gamma(axr_ctx *c, float ex) {
   int rc = check_ctx(c);
   if (rc) return rc;
   long n = (long)c->w * c->h;
-  k_gamma<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, ex);
+  launch(c, "k_gamma", [&] { k_gamma<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, ex); });
   CK(cudaGetLastError());
   return 0;
 }
@@ -543,7 +604,7 @@ int axr_clear_shadow_map(axr_ctx *c, int i) {
   if (rc) return rc;
   if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
   Shadow &s = c->shadows[i];
-  k_clear_depth<<<grid_for(c, (long)s.dim * s.dim, 256, 8), 256, 0, c->stream>>>(s.map, s.dim, s.dim, 16);
+  launch(c, "k_clear_shadow", [&] { k_clear_depth<<<grid_for(c, (long)s.dim * s.dim, 256, 8), 256, 0, c->stream>>>(s.map, s.dim, s.dim, 16); });
   CK(cudaGetLastError());
   return 0;
 }
@@ -584,8 +645,8 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   S.map = sm.map; S.bias = bias; S.list = c->sh_list; S.ctr = c->ctr;
   if (c->total_tris == 0) return 0;
   CK(cudaMemsetAsync(c->ctr + CTR_SH_LIST, 0, sizeof(uint32_t) * 2, c->stream));
-  k_shadow_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, c->stream>>>(S);
-  k_shadow_raster<<<c->sms * 8, 128, 0, c->stream>>>(S);
+  launch(c, "k_shadow_setup", [&] { k_shadow_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, c->stream>>>(S); });
+  launch(c, "k_shadow_raster", [&] { k_shadow_raster<<<c->sms * 8, 128, 0, c->stream>>>(S); });
   CK(cudaGetLastError());
   return 0;
 }
@@ -632,6 +693,40 @@ int axr_last_stats(axr_ctx *c, int64_t *kernels, int64_t *n_small, int64_t *n_la
   if (n_small) *n_small = c->h_ctr[CTR_SMALL];
   if (n_large) *n_large = c->h_ctr[CTR_LARGE];
   if (n_units) *n_units = c->h_ctr[CTR_UNITS];
+  return 0;
+}
+
+int axr_launch_count(axr_ctx *c, int64_t *total) {
+  if (!c || !total) return fail(AXR_EINVAL, "null argument");
+  *total = c->launches;
+  return 0;
+}
+
+int axr_set_kernel_timing(axr_ctx *c, int enable) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if ((rc = axr_sync(c))) return rc;
+  c->timing = enable != 0;
+  c->tacc.clear();
+  return 0;
+}
+
+int axr_kernel_times(axr_ctx *c, int max, char *names, int name_len, double *total_ms, int64_t *launches, int *n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if ((rc = axr_sync(c))) return rc;
+  int k = 0;
+  for (auto &acc : c->tacc) {
+    if (k >= max) break;
+    if (names && name_len > 0) {
+      strncpy(names + (size_t)k * name_len, acc.name.c_str(), name_len - 1);
+      names[(size_t)k * name_len + name_len - 1] = 0;
+    }
+    if (total_ms) total_ms[k] = acc.ms;
+    if (launches) launches[k] = acc.n;
+    k++;
+  }
+  if (n) *n = k;
   return 0;
 }
 

@@ -251,6 +251,28 @@ class CLDraw:
         check(self._L.axr_last_stats(self._h, *[C.byref(v) for v in vals]), "lastStats")
         return {"kernels": vals[0].value, "n_small": vals[1].value, "n_large": vals[2].value, "n_units": vals[3].value}
 
+    def launchCount(self) -> int:
+        v = C.c_int64()
+        check(self._L.axr_launch_count(self._h, C.byref(v)), "launchCount")
+        return v.value
+
+    def setKernelTiming(self, on=True):
+        check(self._L.axr_set_kernel_timing(self._h, 1 if on else 0), "setKernelTiming")
+
+    def kernelTimes(self):
+        """{kernel name: (total device ms, launches)} since timing was enabled."""
+        mx, nl = 64, 48
+        names = C.create_string_buffer(mx * nl)
+        ms = (C.c_double * mx)()
+        cnt = (C.c_int64 * mx)()
+        n = C.c_int()
+        check(self._L.axr_kernel_times(self._h, mx, names, nl, ms, cnt, C.byref(n)), "kernelTimes")
+        out = {}
+        for k in range(n.value):
+            nm = names.raw[k * nl:(k + 1) * nl].split(b"\0", 1)[0].decode()
+            out[nm] = (ms[k], cnt[k])
+        return out
+
     def __getattr__(self, name):
         if name in ("addTexture", "setReflTex", "setHostSkyTex", "addBoneWeights", "initBoneTransforms",
                     "setBoneTransform", "boneTransform", "rotate", "translate", "setupWave", "updateWave",

@@ -375,3 +375,22 @@ def scene_small(seed=3, terrain_n=16, spheres=24, nquads=40, tex=64, alpha_tex=6
 
 def default_view(w, h, pos=(0.0, 5.0, -25.0), target=(0.0, 0.0, 0.0), fov=70.0):
     return View.perspective(w, h, pos, target, fov)
+
+
+def reference_kernel_variant(scene):
+    """The same geometry with only what the reference's existing draw kernels
+    support (PyOpenCL27C/Shaders/drawtexcolsmp.c, drawtexcolsmpalpha.c):
+    mip groups sample their full-resolution level bilinearly and no shadow
+    lookup is made.  Used to run the reference's own kernels on a scene."""
+    groups = []
+    for g in scene.groups:
+        r, gg, b = g.tex
+        ts = g.tex_size
+        if g.flags & MIP:
+            side = 1 << g.tex_size
+            base = (side * side - 1) // 3            # texels of the smaller levels
+            r, gg, b = (np.ascontiguousarray(x[base:base + side * side]) for x in (r, gg, b))
+            ts = side
+        groups.append(Group(g.xyz, g.uv, g.vn, g.li, (r, gg, b), ts, g.flags & ~(MIP | SHADOW),
+                            g.alpha_index, g.mip_bias, g.cast))
+    return Scene(groups, scene.alphas, scene.lint, scene.ldir, scene.amb, scene.shadows, scene.bias)

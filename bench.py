@@ -1,0 +1,374 @@
+"""Benchmark of the rasterizer hot path on the 1080p / 1M-triangle scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl axr|reference]
+
+One step = one frame of the plain single-view workload: both 2048^2 shadow
+cascades (clear + ortho setup + depth raster) and the 1920x1080 main view
+(clear + drawAll: setup, small/large raster, shading with trilinear mips,
+alpha test and the double-cascade lookup) over 1,044,288 triangles in 5
+materials.  Synthetic seeded scene (no dataset).
+
+Prints one JSON line (rank 0).  `value` = frames/s with the scene resident in
+HBM, timed with CUDA events on the library's stream (max over ranks); `e2e`
+= frames/s through the public API with the camera pose uploaded and the
+frame (3 x u16 colour planes + f32 depth) read back into pinned host memory
+every step.  Multi-GPU runs are replicas (one scene per GPU, weak scaling,
+no data-path collective).  `--impl reference` times the reference's own
+OpenCL kernels compiled for the host CPU (oracle/_ref) on the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s & Mtri/s at 1080p/1M tris; p50/p99 latency, batched vs plain"
+W, H = 1920, 1080
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+# each kernel on this workload, from the ncu capture summarised in
+# profiles/ncu_kernels_1080p_1m.md; None until captured.
+NCU_TRAFFIC = {"k_raster_small": 34465536 + 512, "k_shadow_raster": 46918400 + 7424,
+               "k_shade": 29610752 + 670976}
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"axr_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        mhz, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                mhz.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not mhz:
+            return None
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ------------------------------------------------------------------ roofline bookkeeping
+
+def algorithmic_bytes(scene, stats, visible_tris):
+    """Lower-bound bytes each kernel must move per launch:
+    geometry it has to read once, framebuffer/map bytes it has to write once."""
+    T = scene.ntris
+    cull_T = sum(g.ntris for g in scene.groups if g.flags & 8)
+    alpha_T = sum(g.ntris for g in scene.groups if g.flags & 2)
+    npx = W * H
+    smap = [sc.dim * sc.dim for sc in scene.shadows]
+    return {
+        # xyz of every triangle (+ normals of culled groups), 4 B per list entry
+        "k_setup": 36 * T + 36 * cull_T + 4 * (stats["n_small"] + stats["n_large"]),
+        # xyz of every small triangle, visibility word written once per pixel
+        "k_raster_small": 36 * stats["n_small"] + 8 * npx,
+        "k_coarse": 36 * stats["n_large"] + 8 * stats["n_units"],
+        "k_raster_tiled": 36 * stats["n_large"] + 8 * stats["n_units"],
+        # visibility word read, colour + depth written, attributes of the visible triangles read once
+        "k_shade": 8 * npx + 10 * npx + 132 * visible_tris,
+        "k_init_keys": 4 * npx + 8 * npx,
+        "k_clear_depth": 4 * npx,
+        # per cascade: xyz (+ uv of alpha casters) read, map written once
+        "k_shadow_setup": 36 * T,
+        "k_shadow_raster": 36 * T + 24 * alpha_T + 4 * (sum(smap) // max(1, len(smap))),
+        "k_clear_shadow": 4 * (sum(smap) // max(1, len(smap))),
+    }
+
+
+def frame_bytes(scene):
+    """Per-frame algorithmic bytes B = 132 T + sum_c (36 T_cast + 24 T_alpha) + 10 W H + 4 sum S^2."""
+    T = scene.ntris
+    casts = sum(g.ntris for g in scene.groups if g.cast)
+    alpha = sum(g.ntris for g in scene.groups if g.cast and g.flags & 2)
+    return 132 * T + len(scene.shadows) * (36 * casts + 24 * alpha) + 10 * W * H + 4 * sum(
+        sc.dim * sc.dim for sc in scene.shadows)
+
+
+# ------------------------------------------------------------------ CPU legs
+
+def cpu_oracle_baseline(scene, view, budget_s=12.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build_oracle()
+    nthreads = os.cpu_count() or 1
+    n, t0 = 0, time.perf_counter()
+    while True:
+        O.render(scene, view, nthreads=nthreads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= 20:
+            break
+    return {"value": n / el, "unit": "frames/s", "cores": nthreads, "kind": "port",
+            "sample": f"{n} full frames (2 shadow cascades + 1920x1080 drawAll, 1,044,288 triangles) "
+                      f"on the C oracle with OpenMP, {el:.1f} s"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from axi_visualizer_b200 import scenes as S
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference checkout absent at build time)"}))
+        return 0
+    scene = S.reference_kernel_variant(S.scene_c2())
+    view = S.default_view(W, H)
+    nthreads = os.cpu_count() or 1
+    rd = O.RefDraw(scene, view)
+
+    def step():
+        for k in range(len(scene.shadows)):
+            rd.shadow_map(k, nthreads=nthreads)
+        rd.clear_zbuffer()
+        rc = rd.draw_all(nthreads=nthreads)
+        if rc != 0:
+            raise RuntimeError(f"reference drawAll failed: {rc}")
+        rd.get_frame()
+
+    for _ in range(args.warmup):
+        step()
+    lat = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        step()
+        lat.append(time.perf_counter() - t1)
+    el = time.perf_counter() - t0
+    fps = args.steps / el
+    line = {
+        "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "impl": "reference",
+        "config": {"workload": "c2_plain_1080p_1m_tris", "width": W, "height": H, "triangles": scene.ntris,
+                   "shadow_cascades": [sc.dim for sc in scene.shadows],
+                   "shader": "reference kernels drawtexcolsmp/drawtexcolsmpalpha (bilinear base level, no shadow "
+                             "lookup: the reference ships no trilinear+double-cascade kernel), drawmin/drawminalpha"},
+        "Mtri_per_s": scene.ntris * fps / 1e6, "Mpix_per_s": W * H * fps / 1e6,
+        "p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"{args.steps} frames of the scene through the reference's OpenCL kernels "
+                                   f"compiled for the CPU, one work-group per thread"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def _smi_index(torch, local):
+    """nvidia-smi id of the CUDA device `local` (PCI bus id when available)."""
+    try:
+        p = torch.cuda.get_device_properties(local)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x for x in vis.split(",") if x.strip()]
+        return ids[local] if local < len(ids) else str(local)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="axr", choices=["axr", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from axi_visualizer_b200 import scenes as S
+    from axi_visualizer_b200.ops import SceneRenderer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    scene = S.scene_c2()
+    view = S.default_view(W, H)
+    R = SceneRenderer(scene, W, H, device=local, pinned=True)
+    D = R.draw
+    stream = torch.cuda.ExternalStream(D.stream_ptr(), device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        R.frame(view)
+    D.sync()
+    stats = D.lastStats()
+
+    # ---- device-timed loop (value): scene resident in HBM
+    clocks = Clocks(_smi_index(torch, local))
+    barrier()
+    torch.cuda.synchronize()
+    D.sync()
+    launches0 = D.launchCount()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    clocks.start()
+    evs[0].record(stream)
+    for i in range(args.steps):
+        R.frame(view)
+        evs[i + 1].record(stream)
+    D.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    gpu_launches = D.launchCount() - launches0
+    frame_ms = np.array([evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)])
+    t_ms = max_over_ranks(float(evs[0].elapsed_time(evs[-1])))
+    barrier()
+    fps = world * args.steps / (t_ms / 1000.0)
+
+    # ---- per-kernel device times (roofline) on a second pass
+    D.setKernelTiming(True)
+    for _ in range(args.steps):
+        R.frame(view)
+    ktimes = D.kernelTimes()
+    D.setKernelTiming(False)
+    tid, cov = D.getIDs()
+    visible = int(np.unique(tid[tid >= 0]).size)
+    alg = algorithmic_bytes(scene, stats, visible)
+    hbm, peak_kind = peaks()
+    per_kernel = {k: {"avg_us": 1000 * ms / n, "launches_per_frame": n / args.steps,
+                      "share": 0.0} for k, (ms, n) in ktimes.items()}
+    tot = sum(ms for ms, n in ktimes.values())
+    for k, (ms, n) in ktimes.items():
+        per_kernel[k]["share"] = ms / tot if tot else 0.0
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0])[0]
+    dom_avg_s = ktimes[dom][0] / ktimes[dom][1] / 1000.0
+    achieved = alg.get(dom, 0) / dom_avg_s / 1e9
+    traffic = NCU_TRAFFIC.get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes": alg.get(dom, 0)}
+    fb = frame_bytes(scene)
+    frame_roof = {"bytes": fb, "achieved_gbs": fb / (t_ms / args.steps / 1000.0) / 1e9}
+    frame_roof["frac"] = frame_roof["achieved_gbs"] / hbm
+
+    # ---- end-to-end through the public API, host buffers, pinned memory
+    barrier()
+    pose = torch.empty(12, dtype=torch.float32, pin_memory=True).numpy()
+    pose[:3] = view.pos
+    pose[3:] = view.vv.reshape(-1)
+    D.sync()
+    t0 = time.perf_counter()
+    e2e_lat = []
+    for i in range(args.steps):
+        t1 = time.perf_counter()
+        R.shadow_pass()
+        D.setScaleCull(view.sscale, view.cax, view.cay)
+        D.setPos(pose[:3])
+        D.setVM(pose[3:].reshape(3, 3))
+        D.clearZBuffer()
+        D.drawAll(R.shaders, shadowIds=[0, 1])
+        D.getFrame()                      # D2H of colour planes + depth into pinned buffers (synchronises)
+        e2e_lat.append(time.perf_counter() - t1)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_fps = world * args.steps / e2e_s
+    d2h = W * H * (3 * 2 + 4)
+    h2d = 12 * 4 + 3 * 4 + 3 * len(scene.groups) * 96   # pose + scale/cull + 3 group tables per frame
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_oracle_baseline(scene, view)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+            "config": {"workload": "c2_plain_1080p_1m_tris", "width": W, "height": H, "triangles": scene.ntris,
+                       "materials": len(scene.groups), "shadow_cascades": [sc.dim for sc in scene.shadows],
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (geometry+textures "
+                       f"{(sum(g.xyz.nbytes * 4 // 3 + g.tex[0].nbytes * 3 for g in scene.groups)) / 1e6:.0f} MB)"},
+            "Mtri_per_s": scene.ntris * fps / 1e6, "Mpix_per_s": W * H * fps / 1e6,
+            "p50_ms": float(np.percentile(frame_ms, 50)), "p99_ms": float(np.percentile(frame_ms, 99)),
+            "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "p50_ms": 1000 * float(np.percentile(e2e_lat, 50)), "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
+            "gpu_launches": int(gpu_launches),
+            "roofline": roofline,
+            "frame_roofline": frame_roof,
+            "kernels": per_kernel,
+            "queues": stats,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -155,6 +155,17 @@ int axr_frame_device_ptrs(axr_ctx *ctx, void **r, void **g, void **b, void **dep
  * work-queue sizes (small triangles, large triangles, tile units). */
 int axr_last_stats(axr_ctx *ctx, int64_t *kernels, int64_t *n_small, int64_t *n_large, int64_t *n_units);
 
+/* Number of kernels the handle has launched since axr_create. */
+int axr_launch_count(axr_ctx *ctx, int64_t *total);
+
+/* Per-kernel timing (tracing): when enabled, every kernel launch is
+ * bracketed by CUDA events on the handle's stream; axr_kernel_times reports,
+ * per kernel name, the summed device time (ms) and the launch count since
+ * timing was enabled.  names receives up to `max` NUL-terminated names of
+ * name_len bytes each. Both calls synchronise the stream. */
+int axr_set_kernel_timing(axr_ctx *ctx, int enable);
+int axr_kernel_times(axr_ctx *ctx, int max, char *names, int name_len, double *total_ms, int64_t *launches, int *n);
+
 #ifdef __cplusplus
 }
 #endif
