@@ -19,6 +19,7 @@ EXPORTS = [
     "axr_set_frame", "axr_gamma", "axr_add_shadow_map", "axr_place_shadow_map", "axr_clear_shadow_map",
     "axr_shadow_map", "axr_get_shadow_map", "axr_sync", "axr_get_stream", "axr_frame_device_ptrs",
     "axr_last_stats", "axr_launch_count", "axr_set_kernel_timing", "axr_kernel_times",
+    "axr_shadow_map_noalloc",
 ]
 
 vp = C.c_void_p
@@ -58,6 +59,7 @@ _SIGS = {
     "axr_set_kernel_timing": (i32, [vp, i32]),
     "axr_kernel_times": (i32, [vp, i32, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                C.POINTER(i32)]),
+    "axr_shadow_map_noalloc": (i32, [vp, vp, vp, i32, i32, vp, vp, f32, f32, vp, i32, vp]),
 }
 
 _lib = None

@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -731,3 +732,150 @@ int axr_kernel_times(axr_ctx *c, int max, char *names, int name_len, double *tot
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Shadow depth pass without device allocation.
+//
+// Some callers cannot call cudaMalloc/cudaFree while they render: an engine
+// that hands all device memory to its own allocator, or a frame loop that
+// must not hit the implicit device synchronisation those calls can cause
+// while other streams are busy.  axr_shadow_map_noalloc serves them: the
+// caller passes device pointers for the triangles and the depth map, and the
+// only scratch (the list of accepted triangles and two work counters) lives
+// in the file-scope array below, which every GPU that loads this library
+// holds until the process exits.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr uint32_t NOALLOC_MAX_TRIS = 1u << 20;     // 4 MiB of triangle list per GPU
+constexpr uint32_t NOALLOC_WORDS = NOALLOC_MAX_TRIS + CTR_N;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_WORDS];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+uint32_t *g_noalloc_ptr[NOALLOC_MAX_DEVICES];       // device address of the array, per device
+std::mutex g_noalloc_mu;
+
+// One caster group, passed by value (no device-side table).
+__global__ void __launch_bounds__(256) k_shadow_setup_noalloc(GroupDev G, ShadowParams S) {
+  int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
+    int t = base + threadIdx.x;
+    bool ok = false;
+    if (t < S.total_tris) {
+      int ix[3], iy[3];
+      float z[3];
+      ok = project_ortho(G, t, S.sh, S.bias, ix, iy, z);
+    }
+    unsigned m = __ballot_sync(FULL, ok);
+    uint32_t b = 0;
+    if (lane == 0 && m) b = atomicAdd(&S.ctr[CTR_SH_LIST], __popc(m));
+    b = __shfl_sync(FULL, b, 0);
+    if (ok) S.list[b + __popc(m & ((1u << lane) - 1))] = (uint32_t)t;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_shadow_raster_noalloc(GroupDev G, ShadowParams S) {
+  __shared__ GroupDev sg[1];
+  __shared__ SpanS q[4][32];
+  __shared__ int pre[4][33];
+  if (threadIdx.x == 0) sg[0] = G;
+  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
+  __syncthreads();
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t n = S.ctr[CTR_SH_LIST];
+  int dim = S.sh.dim;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&S.ctr[CTR_SH_WORK], 32u);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= n) break;
+    ShadowLane L;
+    bool live = false;
+    if (base + lane < n) live = L.init(S, sg, S.list[base + lane]);
+    while (__any_sync(FULL, live)) {
+      SpanS s;
+      s.cnt = 0;
+      if (live) live = L.step(dim, s);
+      int c = s.cnt, incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int total = __shfl_sync(FULL, incl, 31);
+      if (total == 0) continue;
+      q[w][lane] = s;
+      pre[w][lane] = incl - c;
+      __syncwarp();
+      for (int p = lane; p < total; p += 32) {
+        int k = 0;
+#pragma unroll
+        for (int st = 16; st; st >>= 1)
+          if (pre[w][k + st] <= p) k += st;
+        shadow_fragment(S.map, dim, q[w][k], q[w][k].lo + (p - pre[w][k]));
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Resolves the device address of g_noalloc_scratch for the current device
+// (once per device; the host-side name is only a stand-in for it).
+int noalloc_scratch(uint32_t **out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(AXR_EINVAL, "device %d beyond %d", dev, NOALLOC_MAX_DEVICES);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return fail(AXR_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (uint32_t *)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int axr_shadow_map_noalloc(const float *xyz, const float *uv, const uint8_t *alpha_mask, int alpha_side,
+                                      int ntris, const float pos[3], const float vm[9], float scale, float bias,
+                                      float *map, int dim, void *stream) {
+  if (!xyz || !pos || !vm || !map) return fail(AXR_EINVAL, "null argument");
+  if (ntris < 0 || (uint32_t)ntris > NOALLOC_MAX_TRIS)
+    return fail(AXR_EINVAL, "axr_shadow_map_noalloc takes at most %u triangles per call, got %d", NOALLOC_MAX_TRIS,
+                ntris);
+  if (dim < 4 || dim > 16384) return fail(AXR_EINVAL, "shadow map size %d outside [4, 16384]", dim);
+  if (alpha_mask && (!uv || !is_pow2(alpha_side)))
+    return fail(AXR_EINVAL, "alpha casters need uv and a power-of-two mask side (got %d)", alpha_side);
+  uint32_t *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  if (ntris == 0) return 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  GroupDev G;
+  memset(&G, 0, sizeof G);
+  G.xyz = xyz; G.uv = uv; G.ntris = ntris; G.tri_base = 0; G.enabled = 1;
+  if (alpha_mask) { G.flags = F_ALPHA; G.amask = alpha_mask; G.alen = alpha_side; }
+  ShadowParams S;
+  memset(&S, 0, sizeof S);
+  S.groups = nullptr; S.ngroups = 1; S.total_tris = ntris;
+  S.sh.map = map; S.sh.dim = dim; S.sh.scale = scale;
+  memcpy(S.sh.pos, pos, sizeof S.sh.pos);
+  memcpy(S.sh.vv, vm, sizeof S.sh.vv);
+  S.map = map; S.bias = bias;
+  S.list = scratch;
+  S.ctr = scratch + NOALLOC_MAX_TRIS;
+  // the counters keep the previous call's values: start them at zero
+  CK(cudaMemsetAsync(S.ctr, 0, sizeof(uint32_t) * CTR_N, s));
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long g = ((long)ntris + 255) / 256;
+  if (g > (long)sms * 16) g = (long)sms * 16;
+  k_shadow_setup_noalloc<<<(int)std::max(g, 1L), 256, 0, s>>>(G, S);
+  k_shadow_raster_noalloc<<<sms * 8, 128, 0, s>>>(G, S);
+  CK(cudaGetLastError());
+  return 0;
+}

@@ -166,6 +166,32 @@ int axr_launch_count(axr_ctx *ctx, int64_t *total);
 int axr_set_kernel_timing(axr_ctx *ctx, int enable);
 int axr_kernel_times(axr_ctx *ctx, int max, char *names, int name_len, double *total_ms, int64_t *launches, int *n);
 
+/* Shadow-map depth pass that allocates no device memory.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc/cudaFree
+ * while rendering (an engine whose own allocator owns all device memory, or
+ * a frame loop that must not take the implicit device synchronisation those
+ * calls can cause).  Same arithmetic as axr_shadow_map for one group of
+ * casters: ortho setup (trisetupOrtho.c) and depth-min raster (drawmin.c,
+ * or drawminalpha.c when alpha_mask is given).
+ *
+ * All pointers except pos/vm are DEVICE pointers on the current device:
+ * xyz [3*ntris][3]; uv [3*ntris][2] and alpha_mask [alpha_side^2] only for
+ * alpha-tested casters (else NULL); map [dim][dim] is updated in place (the
+ * caller clears it, e.g. to 65535).  Work is queued on `stream` (NULL = the
+ * default stream); the call does not synchronise.
+ *
+ * Limits: at most 1,048,576 triangles per call (larger counts are rejected
+ * with AXR_EINVAL); dim in [4, 16384].  Scratch: a fixed 4 MiB array inside
+ * the library, held by every GPU that loads it until the process exits.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress); make the first call on each device before any
+ * stream capture.  Every call shares the array, so calls that overlap on the
+ * GPU (concurrent streams, or several host threads) race and give wrong
+ * maps: serialise them. */
+int axr_shadow_map_noalloc(const float *xyz, const float *uv, const uint8_t *alpha_mask, int alpha_side, int ntris,
+                           const float pos[3], const float vm[9], float scale, float bias, float *map, int dim,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif
