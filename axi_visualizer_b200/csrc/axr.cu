@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -286,7 +287,13 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
       cudaMallocHost(&c->h_ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess) {
     rc = fail(AXR_ENOMEM, "framebuffers for %dx%d", w, h);
   }
-  if (!rc) rc = grow_units(c, 1u << 22);
+  // initial tile-unit queue (grows after an overflow); AXR_UNIT_QUEUE overrides
+  uint32_t units0 = 1u << 22;
+  if (const char *e = getenv("AXR_UNIT_QUEUE")) {
+    long v = atol(e);
+    if (v >= 1 && v <= (1L << 30)) units0 = (uint32_t)v;
+  }
+  if (!rc) rc = grow_units(c, units0);
   if (rc) {
     axr_destroy(c);
     return rc;

@@ -152,9 +152,17 @@ class Scene:
 
 
 def terrain(rng, n, cell, origin, height_sd, uvspread=2.0):
-    """(n x n)-cell heightfield: VertTerrain.create triangulation, per-cell
-    UVs wrapped to [0,1), and -y facing normals from central differences."""
+    """(n x n)-cell heightfield of N(0,1)*height_sd heights."""
     h = (rng.standard_normal((n + 1, n + 1)) * height_sd).astype(np.float64)
+    return terrain_from_heights(h, cell, origin, uvspread)
+
+
+def terrain_from_heights(h, cell, origin, uvspread=2.0):
+    """VertTerrain.create triangulation of an (n+1)x(n+1) height field, per-cell
+    UVs wrapped to [0,1) (texMode "repeat"), -y facing normals from central
+    differences."""
+    h = np.asarray(h, np.float64)
+    n = h.shape[0] - 1
     i = np.arange(n + 1, dtype=np.float64)
     X = origin[0] + i[:, None] * cell + 0 * i[None, :]
     Z = origin[2] + i[None, :] * cell + 0 * i[:, None]

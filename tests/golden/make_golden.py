@@ -1,0 +1,104 @@
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Run in a checkout where the reference is present (it is read, never copied):
+
+    python oracle/build_ref.py                 # reference kernels -> oracle/_ref
+    python tests/golden/make_golden.py
+
+1. ref_frames.npz: frames and shadow maps rendered by the reference's own
+   OpenCL kernels compiled for the CPU (oracle/_ref, run work-item by
+   work-item) on small seeded scenes; colour planes and depth are stored
+   whole, plus SHA-256 digests of every array.
+2. ref_terrain.npz: vertex positions and UVs of the reference's own
+   VertTerrain.create (PyOpenCL27C/VertObjects.py:643-700) for a 4x4 height
+   field, and Utils.createMips (PyOpenCL27C/Utils.py:79-93) of an 8x8 RGB
+   texture, imported from the reference with a stub for its unused numexpr
+   import.
+"""
+import hashlib
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+REF = os.environ.get("AXR_REFERENCE", "/root/reference")
+
+CASES = [  # (seed, width, height, camera position)
+    (3, 160, 120, (0, 8, -30)),
+    (1, 160, 128, (3, 2, -8)),
+    (2, 128, 96, (-20, 3, 5)),
+]
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def frames():
+    import oracle as O
+    from axi_visualizer_b200 import scenes as S
+    out = {}
+    for i, (seed, w, h, pos) in enumerate(CASES):
+        sc = S.scene_small(seed=seed, flags=0, with_alpha=True)
+        view = S.default_view(w, h, pos=pos)
+        rd = O.RefDraw(sc, view)
+        for k in range(len(sc.shadows)):
+            rc, m = rd.shadow_map(k)
+            assert rc == 0
+            out[f"c{i}_shm{k}"] = m
+        rd.clear_zbuffer()
+        assert rd.draw_all() == 0
+        r, g, b, db = rd.get_frame()
+        out.update({f"c{i}_r": r, f"c{i}_g": g, f"c{i}_b": b, f"c{i}_db": db})
+    # the full-size 1080p scene (reference-kernel variant): digests only
+    sc = S.reference_kernel_variant(S.scene_c2())
+    view = S.default_view(1920, 1080)
+    rd = O.RefDraw(sc, view)
+    for k in range(len(sc.shadows)):
+        rc, m = rd.shadow_map(k, nthreads=1)
+        out[f"hd_shm{k}_sha256"] = np.array(digest(m))
+    rd.clear_zbuffer()
+    assert rd.draw_all() == 0
+    r, g, b, db = rd.get_frame()
+    for n, a in (("r", r), ("g", g), ("b", b), ("db", db)):
+        out[f"hd_{n}_sha256"] = np.array(digest(a))
+    for k in list(out):
+        if not k.endswith("sha256"):
+            out[k + "_sha256"] = np.array(digest(out[k]))
+    np.savez_compressed(os.path.join(HERE, "ref_frames.npz"), **out)
+
+
+def terrain():
+    sys.modules.setdefault("numexpr", types.ModuleType("numexpr"))
+    sys.path.insert(0, os.path.join(REF, "PyOpenCL27C"))
+    from Utils import createMips
+    from VertObjects import VertTerrain
+
+    class Viewer:
+        def __init__(self):
+            self.vtNames, self.vtextures, self.vertpoints, self.vertnorms = {}, [], [], []
+            self.vertu, self.vertv, self.vertBones, self.matShaders = [], [], [], {}
+            self.texAlphas, self.vaNames = [], {}
+
+    rng = np.random.default_rng(7)
+    hts = rng.standard_normal((5, 5)) * 2
+    v = Viewer()
+    t = VertTerrain(v, [-2, 0, -2], heights=hts.copy(), texture=os.path.join(REF, "Assets", "Grass1.png"), uvspread=2)
+    t.created()
+    pts = np.array(v.vertpoints[0]).reshape(-1, 3)
+    u = np.array(v.vertu[0]).reshape(-1)
+    vv = np.array(v.vertv[0]).reshape(-1)
+    tex = rng.integers(0, 8000, (8, 8, 3))
+    mips = createMips(tex)
+    np.savez_compressed(os.path.join(HERE, "ref_terrain.npz"), heights=hts, xyz=pts, u=u, v=vv, tex=tex, mips=mips)
+
+
+if __name__ == "__main__":
+    frames()
+    terrain()
+    print("golden fixtures written to", HERE)

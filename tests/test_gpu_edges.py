@@ -1,0 +1,105 @@
+"""Edge cases on the GPU: the CUDA path against the oracle on the
+known-answer scenes, the tile-unit queue overflow fallback, masked and empty
+groups, and the error behaviour of the API."""
+import os
+
+import numpy as np
+import pytest
+
+import kat
+import oracle as O
+from axi_visualizer_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+SCENES, VIEW = kat.case_scenes()
+
+
+def cuda_frame(sc, view, mask=None):
+    from axi_visualizer_b200.ops import SceneRenderer
+    R = SceneRenderer(sc, view.w, view.h)
+    R.shadow_pass()
+    R.set_view(view)
+    R.draw.clearZBuffer()
+    uses = any(g.flags & S.SHADOW for g in sc.groups)
+    R.draw.drawAll(R.shaders, mask=mask, shadowIds=list(range(min(2, len(sc.shadows)))) if uses else [])
+    r, g, b, db = [x.copy() for x in R.draw.getFrame()]
+    tid, cov = R.draw.getIDs()
+    return (r, g, b, db, tid, cov, [R.draw.getSHM(k) for k in range(len(sc.shadows))]), R
+
+
+def oracle_frame(sc, view, mask=None):
+    smaps = []
+    for k, s in enumerate(sc.shadows):
+        m = O.new_shadow_map(s.dim)
+        O.shadow_map(sc, k, m)
+        smaps.append(m)
+    fr = O.Frame(view.w, view.h)
+    O.clear_depth(fr.db)
+    O.draw_all(sc, view, fr, [], mask=mask)
+    return fr, smaps
+
+
+def assert_same(fr, smaps, got):
+    r, g, b, db, tid, cov, shm = got
+    for k, m in enumerate(smaps):
+        assert np.array_equal(shm[k].view(np.uint32), m.view(np.uint32))
+    assert np.array_equal(cov, fr.cov)
+    assert np.array_equal(tid, fr.tri_id)
+    assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32))
+    assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo)
+
+
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_kat_cuda_equals_oracle(name):
+    sc = SCENES[name]
+    mask = kat.masks(name, len(sc.groups))
+    fr, smaps = oracle_frame(sc, VIEW, mask)
+    got, _ = cuda_frame(sc, VIEW, mask)
+    assert_same(fr, smaps, got)
+
+
+def test_unit_queue_overflow_falls_back_then_grows(monkeypatch):
+    monkeypatch.setenv("AXR_UNIT_QUEUE", "16")
+    sc = S.scene_small(seed=1, flags=S.MIP | S.SHADOW)
+    view = S.default_view(320, 240, pos=(3, 2, -8))
+    fr, smaps = O.render(sc, view)
+    got, R = cuda_frame(sc, view)
+    st = R.draw.lastStats()
+    assert st["n_units"] > 16                        # the first frame overflowed ...
+    assert_same(fr, smaps, got)                      # ... and the fallback drew it exactly
+    R.frame(view)                                    # the queue has grown: the unit path again
+    r, g, b, db = R.draw.getFrame()
+    assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32))
+
+
+def test_repeated_frames_are_identical():
+    sc = S.scene_small(seed=2, flags=S.MIP | S.SHADOW)
+    view = S.default_view(256, 192, pos=(1, 3, -12))
+    got, R = cuda_frame(sc, view)
+    for _ in range(3):
+        R.frame(view)
+    r, g, b, db = R.draw.getFrame()
+    assert np.array_equal(db.view(np.uint32), got[3].view(np.uint32))
+    assert np.array_equal(r, got[0])
+
+
+def test_api_errors_raise():
+    from axi_visualizer_b200._lib import AxrError
+    from axi_visualizer_b200.ops import CLDraw, SceneRenderer
+    with pytest.raises(AxrError):
+        CLDraw(1, 64, 100, 64, 1)                    # width not a multiple of 16
+    sc = S.scene_small(seed=1, flags=S.MIP | S.SHADOW)
+    R = SceneRenderer(sc, 64, 48)
+    with pytest.raises(AxrError):
+        R.draw.drawAll(R.shaders[:-1])               # group count mismatch
+    with pytest.raises(AxrError):
+        R.draw.drawAll(R.shaders, shadowIds=[])      # shadow materials with no shadow map
+    bad = list(R.shaders)
+    bad[-1] = {"alpha": 5}
+    with pytest.raises(AxrError):
+        R.draw.drawAll(bad)                          # alpha mask index out of range
+    with pytest.raises(AxrError):
+        R.draw.addTextureGroup(np.zeros((4, 3)), np.zeros((4, 2)), np.zeros((4, 3)),
+                               np.zeros(16), np.zeros(16), np.zeros(16))   # not 3 vertices per triangle
+    R.draw.drawAll(R.shaders)                        # the handle still works
+    R.draw.sync()

@@ -1,0 +1,86 @@
+"""Host-side logic without a GPU: scenes, cameras, material parsing, mip
+layout, the correctly rounded log2 shared by oracle and kernels."""
+import math
+import struct
+
+import numpy as np
+import pytest
+
+import oracle as O
+from axi_visualizer_b200 import scenes as S
+
+
+def test_named_scene_sizes():
+    assert S.scene_c1().ntris == 24192
+    sc = S.scene_c2()
+    assert sc.ntris == 1044288
+    assert [g.ntris for g in sc.groups] == [262144, 262144, 240000, 240000, 40000]
+    assert [s.dim for s in sc.shadows] == [2048, 2048]
+    assert sc.alphas[0][1] == 1024 and 0.55 < sc.alphas[0][0].mean() < 0.65
+
+
+def test_camera_bases_orthonormal():
+    for a, b in ((0.3, 0.2), (1.7 * math.pi, 0.52), (-2.0, -0.7)):
+        for m in (S.camera_basis(a, b), S.view_mat(a, b)):
+            assert np.allclose(m @ m.T, np.eye(3), atol=1e-12)
+    v = S.default_view(1920, 1080)
+    assert abs(v.sscale - 960 / math.tan(35 * math.pi / 180)) < 1e-3
+
+
+def test_material_flags():
+    assert S.flags_from_string("mip shadow  cull") == S.MIP | S.SHADOW | S.CULL
+    assert S.flags_from_string("alpha ") == S.ALPHA
+    assert S.flags_from_string({"alpha": 1, "shadow": 1}) == S.ALPHA | S.SHADOW
+    assert S.flags_from_string("") == 0
+
+
+def test_cldraw_material_args_without_gpu():
+    from axi_visualizer_b200.ops import CLDraw
+
+    class Fake:
+        gSize = [3, 3, 3]
+    flags, aidx = CLDraw._material_args(Fake(), {0: "mip shadow", 1: {"alpha": 2}, 2: "cull"})
+    assert flags.tolist() == [S.MIP | S.SHADOW, S.ALPHA, S.CULL] and aidx.tolist() == [0, 2, 0]
+    with pytest.raises(Exception):
+        CLDraw._material_args(Fake(), ["mip"])
+
+
+def test_mip_chain_layout():
+    rgb = np.random.default_rng(0).integers(0, 8000, (16, 16, 3))
+    planes, num = S.texture_planes(rgb.astype(np.uint16), True)
+    assert num == 4 and planes[0].size == (4 * 16 * 16 - 1) // 3
+    assert np.array_equal(planes[0][-256:], rgb[..., 0].reshape(-1))        # largest level last
+    lvl1 = (rgb[0::2, 0::2] + rgb[1::2, 0::2] + rgb[0::2, 1::2] + rgb[1::2, 1::2]) >> 2
+    start = (8 * 8 - 1) // 3                                              # levels 1x1, 2x2, 4x4 come first
+    assert np.array_equal(planes[0][start:start + 64], lvl1[..., 0].reshape(-1))
+
+
+def f32(x):
+    return struct.unpack("f", struct.pack("f", x))[0]
+
+
+def test_log2_correctly_rounded():
+    L = O.lib()
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([rng.random(20000) * 10.0 ** rng.integers(-30, 30, 20000),
+                         np.array([1.0, 2.0, 0.5, 1e-40, 3.4e38, 1.5, 1.4142135])]).astype(np.float32)
+    bad = 0
+    for x in xs:
+        got = L.orc_log2f(float(x))
+        want = f32(math.log2(float(x)))
+        if got != want:
+            bad += 1
+            # differs only where the exact value sits on a float rounding boundary
+            assert abs(got - want) <= abs(want) * 2 ** -23 + 1e-45
+    assert bad <= 2
+    assert L.orc_log2f(0.0) == -math.inf and L.orc_log2f(math.inf) == math.inf
+    assert math.isnan(L.orc_log2f(-1.0))
+
+
+def test_vert_light_matches_formula():
+    vn = np.array([[0, -1, 0], [0.6, -0.8, 0]], np.float32)
+    li = S.vert_light(vn, S.LIGHT_DIRS, S.LIGHT_INTS, 0.2)
+    d1 = S.LIGHT_DIRS[1].astype(np.float32)
+    s = max(0.0, float(np.float32(vn[0] @ d1)) + 0.5) * 0.66
+    assert abs(li[0, 0] - max(0.2, s * 0.5 + max(0.0, float(vn[0] @ S.LIGHT_DIRS[2]) + 0.5) * 0.66 * 0.1)) < 1e-5
+    assert (li >= 0.2).all()
