@@ -44,22 +44,32 @@ int fail(int code, const char *fmt, ...) {
 
 struct Group {
   float *xyz = nullptr, *vn = nullptr, *uv = nullptr, *li = nullptr;
-  uint16_t *tr = nullptr, *tg = nullptr, *tb = nullptr;
+  ushort4 *tex = nullptr;     // interleaved (R, G, B, 0) texels
   int ntris = 0, tri_base = 0, tex_size = 0, mip_side = 0;
   long ntexels = 0;
 };
 
 struct Alpha {
   uint8_t *mask = nullptr;
+  uint8_t *quad = nullptr;    // 2x2 bilinear footprint of each texel as 4 bits
   int side = 0;
 };
 
+// A shadow map has its own stream, scratch (caster list, counters) and group
+// table, so cascades render concurrently with each other and with the main
+// view's visibility pass; ev_write orders the shade pass after the map's last
+// writer, ev_read orders the next writer after the map's last reader.
 struct Shadow {
   float *map = nullptr;
   int dim = 0;
   float scale = 1;
   float pos[3] = {0, 0, 0};
   float vv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_write = nullptr, ev_read = nullptr;
+  uint32_t *list = nullptr, *ctr = nullptr;
+  uint32_t cap = 0;
+  GroupDev *tab = nullptr;
 };
 
 constexpr int MAX_GROUPS = 64;
@@ -70,6 +80,8 @@ constexpr int MAX_SHADOWS = 16;
 struct axr_ctx {
   int device = 0, w = 0, h = 0, sms = 148;
   cudaStream_t stream = nullptr;
+  cudaStream_t s_alpha = nullptr;            // alpha-tested rasterizers of a drawAll
+  cudaEvent_t ev_setup = nullptr, ev_coarse = nullptr, ev_alpha = nullptr;
   std::vector<Group> groups;
   std::vector<Alpha> alphas;
   int total_tris = 0;
@@ -81,7 +93,7 @@ struct axr_ctx {
   uint16_t *ro = nullptr, *go = nullptr, *bo = nullptr;
   float *db = nullptr;
   uint64_t *keys = nullptr;
-  uint32_t *small_list = nullptr, *large_list = nullptr, *sh_list = nullptr;
+  uint32_t *small_list = nullptr, *large_list = nullptr, *items = nullptr;
   uint32_t cap_list = 0;
   uint2 *units = nullptr;
   uint32_t cap_units = 0;
@@ -107,11 +119,13 @@ int ensure_lists(axr_ctx *c) {
   uint32_t need = (uint32_t)std::max(c->total_tris, 1);
   if (need <= c->cap_list) return 0;
   uint32_t cap = std::max(need, c->cap_list * 2);
-  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->sh_list);
-  c->small_list = c->large_list = c->sh_list = nullptr;
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items);
+  c->small_list = c->large_list = c->items = nullptr;
+  if (cap > 0x3fffffffu / MAX_CHUNKS) return fail(AXR_EINVAL, "too many triangles");
   if (cudaMalloc(&c->small_list, sizeof(uint32_t) * cap) != cudaSuccess ||
       cudaMalloc(&c->large_list, sizeof(uint32_t) * cap) != cudaSuccess ||
-      cudaMalloc(&c->sh_list, sizeof(uint32_t) * cap) != cudaSuccess)
+      cudaMalloc(&c->items, sizeof(uint32_t) * cap * MAX_CHUNKS) != cudaSuccess)
     return fail(AXR_ENOMEM, "triangle lists of %u entries", cap);
   c->cap_list = cap;
   return 0;
@@ -133,15 +147,22 @@ void collect_times(axr_ctx *c);
 
 // Reads the counters of the last drawAll; grows the unit queue after an
 // overflow (that frame was completed by the fallback kernel).
+int sync_all(axr_ctx *c);
+
 int settle(axr_ctx *c) {
   if (!c->tpend.empty()) {
-    CK(cudaStreamSynchronize(c->stream));
+    int rc = sync_all(c);
+    if (rc) return rc;
     collect_times(c);
   }
   if (!c->pending) return 0;
   CK(cudaStreamSynchronize(c->stream));
   c->pending = false;
-  if (c->h_ctr[CTR_OVERFLOW]) return grow_units(c, c->h_ctr[CTR_UNITS]);
+  if (c->h_ctr[CTR_LIMIT]) {
+    c->h_ctr[CTR_LIMIT] = 0;
+    return fail(AXR_ECUDA, "a raster loop reached its safety limit; the frame is incomplete");
+  }
+  if (c->h_ctr[CTR_OVERFLOW]) return grow_units(c, c->h_ctr[CTR_UNITS_RESERVED]);
   return 0;
 }
 
@@ -165,19 +186,28 @@ cudaEvent_t ev_get(axr_ctx *c) {
 // Launches one kernel through `f`, counting it and, when timing is on,
 // bracketing it with events on the handle's stream.
 template <class F>
-void launch(axr_ctx *c, const char *name, F f) {
+void launch(axr_ctx *c, cudaStream_t st, const char *name, F f) {
   cudaEvent_t a = nullptr;
   if (c->timing) {
     a = ev_get(c);
-    cudaEventRecord(a, c->stream);
+    cudaEventRecord(a, st);
   }
   f();
   c->launches++;
   if (c->timing) {
     cudaEvent_t b = ev_get(c);
-    cudaEventRecord(b, c->stream);
+    cudaEventRecord(b, st);
     c->tpend.push_back({name, a, b});
   }
+}
+
+// Waits for every stream of the handle.
+int sync_all(axr_ctx *c) {
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->s_alpha) CK(cudaStreamSynchronize(c->s_alpha));
+  for (auto &sm : c->shadows)
+    if (sm.st) CK(cudaStreamSynchronize(sm.st));
+  return 0;
 }
 
 // Folds the finished event pairs into the per-kernel totals.
@@ -232,7 +262,7 @@ int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, 
     const Group &G = c->groups[g];
     GroupDev &d = tab[g];
     d.xyz = G.xyz; d.vn = G.vn; d.uv = G.uv; d.li = G.li;
-    d.tr = G.tr; d.tg = G.tg; d.tb = G.tb;
+    d.tex = G.tex;
     d.ntris = G.ntris; d.tri_base = G.tri_base; d.tex_size = G.tex_size;
     d.flags = flags ? flags[g] : 0;
     d.mip_bias = 0.f;
@@ -252,6 +282,7 @@ int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, 
         return fail(AXR_EINVAL, "group %d: alpha mask side %d differs from texture side %d", g, c->alphas[ai].side,
                     base_len);
       d.amask = c->alphas[ai].mask;
+      d.aquad = c->alphas[ai].quad;
       d.alen = c->alphas[ai].side;
     }
   }
@@ -280,6 +311,10 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
   size_t n = (size_t)w * h;
   int rc = 0;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->s_alpha, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_setup, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_coarse, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_alpha, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc(&c->ro, n * 2) != cudaSuccess || cudaMalloc(&c->go, n * 2) != cudaSuccess ||
       cudaMalloc(&c->bo, n * 2) != cudaSuccess || cudaMalloc(&c->db, n * 4) != cudaSuccess ||
       cudaMalloc(&c->keys, n * 8) != cudaSuccess || cudaMalloc(&c->ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
@@ -321,12 +356,21 @@ int axr_destroy(axr_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto &g : c->groups) {
     cudaFree(g.xyz); cudaFree(g.vn); cudaFree(g.uv); cudaFree(g.li);
-    cudaFree(g.tr); cudaFree(g.tg); cudaFree(g.tb);
+    cudaFree(g.tex);
   }
-  for (auto &a : c->alphas) cudaFree(a.mask);
-  for (auto &s : c->shadows) cudaFree(s.map);
+  for (auto &a : c->alphas) { cudaFree(a.mask); cudaFree(a.quad); }
+  for (auto &sm : c->shadows) {
+    if (sm.st) { cudaStreamSynchronize(sm.st); cudaStreamDestroy(sm.st); }
+    if (sm.ev_write) cudaEventDestroy(sm.ev_write);
+    if (sm.ev_read) cudaEventDestroy(sm.ev_read);
+    cudaFree(sm.map); cudaFree(sm.list); cudaFree(sm.ctr); cudaFree(sm.tab);
+  }
+  if (c->s_alpha) { cudaStreamSynchronize(c->s_alpha); cudaStreamDestroy(c->s_alpha); }
+  if (c->ev_setup) cudaEventDestroy(c->ev_setup);
+  if (c->ev_coarse) cudaEventDestroy(c->ev_coarse);
+  if (c->ev_alpha) cudaEventDestroy(c->ev_alpha);
   cudaFree(c->ro); cudaFree(c->go); cudaFree(c->bo); cudaFree(c->db); cudaFree(c->keys);
-  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->sh_list); cudaFree(c->units);
+  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items); cudaFree(c->units);
   cudaFree(c->ctr); cudaFree(c->d_groups);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
   for (auto &p : c->tpend) { c->ev_pool.push_back(p.a); c->ev_pool.push_back(p.b); }
@@ -370,9 +414,10 @@ int axr_add_texture_group(axr_ctx *c, const float *xyz, const float *uv, const f
     G.tex_size = (int)side;
   }
   size_t nv = (size_t)ntris * 3;
+  std::vector<ushort4> texels((size_t)ntexels);
+  for (long k = 0; k < ntexels; k++) texels[k] = make_ushort4(r[k], g[k], b[k], 0);
   if ((rc = upload(c, &G.xyz, xyz, nv * 3)) || (rc = upload(c, &G.vn, vn, nv * 3)) || (rc = upload(c, &G.uv, uv, nv * 2)) ||
-      (rc = upload(c, &G.tr, r, (size_t)ntexels)) || (rc = upload(c, &G.tg, g, (size_t)ntexels)) ||
-      (rc = upload(c, &G.tb, b, (size_t)ntexels)))
+      (rc = upload(c, &G.tex, texels.data(), (size_t)ntexels)))
     return rc;
   if (cudaMalloc(&G.li, sizeof(float) * std::max<size_t>(nv * 3, 1)) != cudaSuccess) return fail(AXR_ENOMEM, "LI buffer");
   CK(cudaMemsetAsync(G.li, 0, sizeof(float) * nv * 3, c->stream));
@@ -437,9 +482,15 @@ int axr_add_tex_alpha(axr_ctx *c, const uint8_t *mask, int side, int *out_id) {
   if (!mask || !is_pow2(side)) return fail(AXR_EINVAL, "alpha mask side %d is not a power of two", side);
   Alpha a;
   a.side = side;
-  std::vector<uint8_t> b((size_t)side * side);
+  std::vector<uint8_t> b((size_t)side * side), q((size_t)side * side);
   for (size_t i = 0; i < b.size(); i++) b[i] = mask[i] ? 1 : 0;
-  if ((rc = upload(c, &a.mask, b.data(), b.size()))) return rc;
+  for (int t2 = 0; t2 < side; t2++)
+    for (int t1 = 0; t1 < side; t1++) {
+      int t1n = std::min(t1 + 1, side - 1), t2n = std::min(t2 + 1, side - 1);
+      q[(size_t)side * t2 + t1] = (uint8_t)(b[(size_t)side * t2 + t1] | b[(size_t)side * t2 + t1n] << 1 |
+                                            b[(size_t)side * t2n + t1] << 2 | b[(size_t)side * t2n + t1n] << 3);
+    }
+  if ((rc = upload(c, &a.mask, b.data(), b.size())) || (rc = upload(c, &a.quad, q.data(), q.size()))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   c->alphas.push_back(a);
   if (out_id) *out_id = (int)c->alphas.size() - 1;
@@ -468,7 +519,7 @@ int axr_set_vm(axr_ctx *c, const float vm[9]) {
 int axr_clear_zbuffer(axr_ctx *c) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  launch(c, "k_clear_depth", [&] { k_clear_depth<<<grid_for(c, (long)c->w * c->h, 256, 8), 256, 0, c->stream>>>(c->db, c->w, c->h, 4); });
+  launch(c, c->stream, "k_clear_depth", [&] { k_clear_depth<<<grid_for(c, (long)c->w * c->h, 256, 8), 256, 0, c->stream>>>(c->db, c->w, c->h, 4); });
   CK(cudaGetLastError());
   return 0;
 }
@@ -482,9 +533,11 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   if ((rc = settle(c))) return rc;
   DrawParams P;
   memset(&P, 0, sizeof P);
-  bool any_shadow = false;
-  for (int g = 0; g < ngroups; g++)
+  bool any_shadow = false, any_alpha = false;
+  for (int g = 0; g < ngroups; g++) {
     if ((!mask || !mask[g]) && flags && (flags[g] & F_SHADOW)) any_shadow = true;
+    if ((!mask || !mask[g]) && flags && (flags[g] & F_ALPHA)) any_alpha = true;
+  }
   P.nsh = nshadow;
   for (int k = 0; k < nshadow; k++) {
     int id = shadow_ids[k];
@@ -504,22 +557,42 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   memcpy(P.light.ldir, c->ldir, sizeof c->ldir);
   P.light.amb = c->amb;
   P.keys = c->keys; P.ro = c->ro; P.go = c->go; P.bo = c->bo; P.db = c->db;
-  P.small_list = c->small_list; P.large_list = c->large_list;
+  P.small_list = c->small_list; P.large_list = c->large_list; P.items = c->items;
   P.units = c->units; P.ctr = c->ctr;
   P.cap_list = c->cap_list; P.cap_units = c->cap_units;
   long npix = (long)c->w * c->h;
   cudaStream_t s = c->stream;
   int64_t nk = 0;
-  launch(c, "k_init_keys", [&] { k_init_keys<<<grid_for(c, npix, 256, 16), 256, 0, s>>>(c->db, c->keys, (int)npix, c->ctr); }); nk++;
+  cudaStream_t sa = c->s_alpha;
+  launch(c, s, "k_init_keys", [&] { k_init_keys<<<grid_for(c, npix, 256, 16), 256, 0, s>>>(c->db, c->keys, (int)npix, c->ctr); }); nk++;
   if (c->total_tris > 0) {
-    launch(c, "k_setup", [&] { k_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, s>>>(P); }); nk++;
-    launch(c, "k_raster_small", [&] { k_raster_small<<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
-    launch(c, "k_coarse", [&] { k_coarse<<<c->sms * 4, 128, 0, s>>>(P); }); nk++;
-    launch(c, "k_raster_tiled", [&] { k_raster_tiled<<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
-    launch(c, "k_raster_tiled_fallback", [&] { k_raster_tiled_fallback<<<c->sms * 2, 128, 0, s>>>(P); }); nk++;
+    // visibility: opaque rasterizers on the main stream, alpha-tested ones
+    // concurrently on a side stream (all of them atomicMin the same buffer)
+    launch(c, s, "k_setup", [&] { k_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, s>>>(P); }); nk++;
+    if (any_alpha) {
+      CK(cudaEventRecord(c->ev_setup, s));
+      CK(cudaStreamWaitEvent(sa, c->ev_setup, 0));
+      launch(c, sa, "k_raster_small_alpha", [&] { k_raster_small<true><<<c->sms * 6, 128, 0, sa>>>(P); }); nk++;
+    }
+    launch(c, s, "k_raster_small", [&] { k_raster_small<false><<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
+    launch(c, s, "k_coarse", [&] { k_coarse<<<c->sms * 4, 128, 0, s>>>(P); }); nk++;
+    if (any_alpha) {
+      CK(cudaEventRecord(c->ev_coarse, s));
+      CK(cudaStreamWaitEvent(sa, c->ev_coarse, 0));
+      launch(c, sa, "k_raster_tiled_alpha", [&] { k_raster_tiled<true><<<c->sms * 6, 128, 0, sa>>>(P); }); nk++;
+    }
+    launch(c, s, "k_raster_tiled", [&] { k_raster_tiled<false><<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
+    launch(c, s, "k_raster_tiled_fallback", [&] { k_raster_tiled_fallback<<<c->sms * 2, 128, 0, s>>>(P); }); nk++;
+    if (any_alpha) {
+      CK(cudaEventRecord(c->ev_alpha, sa));
+      CK(cudaStreamWaitEvent(s, c->ev_alpha, 0));
+    }
   }
+  // shading samples the cascades: wait for their last writers
+  for (int k = 0; k < nshadow; k++) CK(cudaStreamWaitEvent(s, c->shadows[shadow_ids[k]].ev_write, 0));
   dim3 sb(16, 16), sgd((c->w + 15) / 16, (c->h + 15) / 16);
-  launch(c, "k_shade", [&] { k_shade<<<sgd, sb, 0, s>>>(P); }); nk++;
+  launch(c, s, "k_shade", [&] { k_shade<<<sgd, sb, 0, s>>>(P); }); nk++;
+  for (int k = 0; k < nshadow; k++) CK(cudaEventRecord(c->shadows[shadow_ids[k]].ev_read, s));
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_ctr, c->ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
   c->pending = true;
@@ -576,7 +649,7 @@ int axr_gamma(axr_ctx *c, float ex) {
   int rc = check_ctx(c);
   if (rc) return rc;
   long n = (long)c->w * c->h;
-  launch(c, "k_gamma", [&] { k_gamma<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, ex); });
+  launch(c, c->stream, "k_gamma", [&] { k_gamma<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, ex); });
   CK(cudaGetLastError());
   return 0;
 }
@@ -586,14 +659,25 @@ int axr_add_shadow_map(axr_ctx *c, int i, int size, float scale, float amb) {
   if (rc) return rc;
   if (i < 0 || i >= MAX_SHADOWS || size < 4 || size > 16384) return fail(AXR_EINVAL, "shadow map %d of size %d", i, size);
   Shadow &s = c->shadows[i];
-  if (s.map && s.dim != size) { CK(cudaStreamSynchronize(c->stream)); cudaFree(s.map); s.map = nullptr; }
+  if (!s.st) {
+    if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s.ev_write, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s.ev_read, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&s.ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
+        cudaMalloc(&s.tab, sizeof(GroupDev) * MAX_GROUPS) != cudaSuccess)
+      return fail(AXR_ENOMEM, "shadow map %d state", i);
+  }
+  if (s.map && s.dim != size) { CK(cudaStreamSynchronize(s.st)); cudaFree(s.map); s.map = nullptr; }
+  CK(cudaStreamWaitEvent(s.st, s.ev_read, 0));
   if (!s.map && cudaMalloc(&s.map, sizeof(float) * (size_t)size * size) != cudaSuccess)
     return fail(AXR_ENOMEM, "shadow map %dx%d", size, size);
   s.dim = size;
   s.scale = scale;
   // a fresh map holds 65535 (Ops.py:1049)
-  k_clear_depth<<<grid_for(c, (long)size * size, 256, 8), 256, 0, c->stream>>>(s.map, size, size, 1);
+  k_clear_depth<<<grid_for(c, (long)size * size, 256, 8), 256, 0, s.st>>>(s.map, size, size, 1);
+  c->launches++;
   CK(cudaGetLastError());
+  CK(cudaEventRecord(s.ev_write, s.st));
   c->amb = amb;
   return 0;
 }
@@ -612,8 +696,10 @@ int axr_clear_shadow_map(axr_ctx *c, int i) {
   if (rc) return rc;
   if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
   Shadow &s = c->shadows[i];
-  launch(c, "k_clear_shadow", [&] { k_clear_depth<<<grid_for(c, (long)s.dim * s.dim, 256, 8), 256, 0, c->stream>>>(s.map, s.dim, s.dim, 16); });
+  CK(cudaStreamWaitEvent(s.st, s.ev_read, 0));
+  launch(c, s.st, "k_clear_shadow", [&] { k_clear_depth<<<grid_for(c, (long)s.dim * s.dim, 256, 8), 256, 0, s.st>>>(s.map, s.dim, s.dim, 16); });
   CK(cudaGetLastError());
+  CK(cudaEventRecord(s.ev_write, s.st));
   return 0;
 }
 
@@ -642,20 +728,38 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
       d.alen = c->alphas[ai].side;
     }
   }
-  CK(cudaMemcpyAsync(c->d_groups, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, c->stream));
   Shadow &sm = c->shadows[i];
+  if (sm.cap < c->cap_list) {
+    CK(cudaStreamSynchronize(sm.st));
+    cudaFree(sm.list);
+    sm.list = nullptr;
+    if (cudaMalloc(&sm.list, sizeof(uint32_t) * c->cap_list) != cudaSuccess)
+      return fail(AXR_ENOMEM, "caster list of shadow map %d", i);
+    sm.cap = c->cap_list;
+  }
+  CK(cudaStreamWaitEvent(sm.st, sm.ev_read, 0));
+  CK(cudaMemcpyAsync(sm.tab, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, sm.st));
   ShadowParams S;
   memset(&S, 0, sizeof S);
-  S.groups = c->d_groups; S.ngroups = ngroups; S.total_tris = c->total_tris;
+  S.groups = sm.tab; S.ngroups = ngroups; S.total_tris = c->total_tris;
   S.sh.map = sm.map; S.sh.dim = sm.dim; S.sh.scale = sm.scale;
   memcpy(S.sh.pos, sm.pos, sizeof sm.pos);
   memcpy(S.sh.vv, sm.vv, sizeof sm.vv);
-  S.map = sm.map; S.bias = bias; S.list = c->sh_list; S.ctr = c->ctr;
+  S.map = sm.map; S.bias = bias; S.list = sm.list; S.cap_list = sm.cap; S.ctr = sm.ctr;
   if (c->total_tris == 0) return 0;
-  CK(cudaMemsetAsync(c->ctr + CTR_SH_LIST, 0, sizeof(uint32_t) * 2, c->stream));
-  launch(c, "k_shadow_setup", [&] { k_shadow_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, c->stream>>>(S); });
-  launch(c, "k_shadow_raster", [&] { k_shadow_raster<<<c->sms * 8, 128, 0, c->stream>>>(S); });
+  bool any_alpha = false;
+  for (int g = 0; g < ngroups; g++)
+    if (cast[g] && (tab[g].flags & F_ALPHA)) any_alpha = true;
+  static_assert(CTR_SH_LIST_A == CTR_SH_LIST + 1 && CTR_SH_WORK == CTR_SH_LIST + 2 && CTR_SH_WORK_A == CTR_SH_LIST + 3,
+                "shadow counters are contiguous");
+  CK(cudaMemsetAsync(sm.ctr, 0, sizeof(uint32_t) * CTR_N, sm.st));
+  cudaStream_t st = sm.st;
+  launch(c, st, "k_shadow_setup", [&] { k_shadow_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, st>>>(S); });
+  launch(c, st, "k_shadow_raster", [&] { k_shadow_raster<false><<<c->sms * 8, 128, 0, st>>>(S); });
+  if (any_alpha)
+    launch(c, st, "k_shadow_raster_alpha", [&] { k_shadow_raster<true><<<c->sms * 6, 128, 0, st>>>(S); });
   CK(cudaGetLastError());
+  CK(cudaEventRecord(sm.ev_write, st));
   return 0;
 }
 
@@ -665,15 +769,15 @@ int axr_get_shadow_map(axr_ctx *c, int i, float *out) {
   if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
   if (!out) return fail(AXR_EINVAL, "null output");
   Shadow &s = c->shadows[i];
-  CK(cudaMemcpyAsync(out, s.map, sizeof(float) * (size_t)s.dim * s.dim, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpyAsync(out, s.map, sizeof(float) * (size_t)s.dim * s.dim, cudaMemcpyDeviceToHost, s.st));
+  CK(cudaStreamSynchronize(s.st));
   return settle(c);
 }
 
 int axr_sync(axr_ctx *c) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  CK(cudaStreamSynchronize(c->stream));
+  if ((rc = sync_all(c))) return rc;
   return settle(c);
 }
 
@@ -698,9 +802,9 @@ int axr_last_stats(axr_ctx *c, int64_t *kernels, int64_t *n_small, int64_t *n_la
   if (rc) return rc;
   if ((rc = axr_sync(c))) return rc;
   if (kernels) *kernels = c->last_kernels;
-  if (n_small) *n_small = c->h_ctr[CTR_SMALL];
+  if (n_small) *n_small = (int64_t)c->h_ctr[CTR_SMALL] + c->h_ctr[CTR_SMALL_A];
   if (n_large) *n_large = c->h_ctr[CTR_LARGE];
-  if (n_units) *n_units = c->h_ctr[CTR_UNITS];
+  if (n_units) *n_units = c->h_ctr[CTR_UNITS_RESERVED];   // units the frame needed (queued or not)
   return 0;
 }
 
@@ -765,66 +869,26 @@ std::mutex g_noalloc_mu;
 
 // One caster group, passed by value (no device-side table).
 __global__ void __launch_bounds__(256) k_shadow_setup_noalloc(GroupDev G, ShadowParams S) {
+  __shared__ GroupDev sg[1];
+  if (threadIdx.x == 0) sg[0] = G;
+  __syncthreads();
   int lane = threadIdx.x & 31;
   for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
     int t = base + threadIdx.x;
-    bool ok = false;
-    if (t < S.total_tris) {
-      int ix[3], iy[3];
-      float z[3];
-      ok = project_ortho(G, t, S.sh, S.bias, ix, iy, z);
-    }
-    unsigned m = __ballot_sync(FULL, ok);
-    uint32_t b = 0;
-    if (lane == 0 && m) b = atomicAdd(&S.ctr[CTR_SH_LIST], __popc(m));
-    b = __shfl_sync(FULL, b, 0);
-    if (ok) S.list[b + __popc(m & ((1u << lane) - 1))] = (uint32_t)t;
+    bool ok, alpha;
+    shadow_classify(sg, S, t, ok, alpha);
+    shadow_append(S, t, ok, alpha, lane);
   }
 }
 
-__global__ void __launch_bounds__(128) k_shadow_raster_noalloc(GroupDev G, ShadowParams S) {
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_shadow_raster_noalloc(GroupDev G, ShadowParams S) {
   __shared__ GroupDev sg[1];
-  __shared__ SpanS q[4][32];
-  __shared__ int pre[4][33];
+  __shared__ ShadowQ<ALPHA> qs[4];
   if (threadIdx.x == 0) sg[0] = G;
-  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
   __syncthreads();
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t n = S.ctr[CTR_SH_LIST];
-  int dim = S.sh.dim;
-  while (true) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&S.ctr[CTR_SH_WORK], 32u);
-    base = __shfl_sync(FULL, base, 0);
-    if (base >= n) break;
-    ShadowLane L;
-    bool live = false;
-    if (base + lane < n) live = L.init(S, sg, S.list[base + lane]);
-    while (__any_sync(FULL, live)) {
-      SpanS s;
-      s.cnt = 0;
-      if (live) live = L.step(dim, s);
-      int c = s.cnt, incl = c;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int v = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += v;
-      }
-      int total = __shfl_sync(FULL, incl, 31);
-      if (total == 0) continue;
-      q[w][lane] = s;
-      pre[w][lane] = incl - c;
-      __syncwarp();
-      for (int p = lane; p < total; p += 32) {
-        int k = 0;
-#pragma unroll
-        for (int st = 16; st; st >>= 1)
-          if (pre[w][k + st] <= p) k += st;
-        shadow_fragment(S.map, dim, q[w][k], q[w][k].lo + (p - pre[w][k]));
-      }
-      __syncwarp();
-    }
-  }
+  shadow_warp_loop<ALPHA>(S, sg, qs[w], lane, ALPHA ? CTR_SH_LIST_A : CTR_SH_LIST, ALPHA ? CTR_SH_WORK_A : CTR_SH_WORK);
 }
 
 // Resolves the device address of g_noalloc_scratch for the current device
@@ -873,6 +937,7 @@ extern "C" int axr_shadow_map_noalloc(const float *xyz, const float *uv, const u
   memcpy(S.sh.vv, vm, sizeof S.sh.vv);
   S.map = map; S.bias = bias;
   S.list = scratch;
+  S.cap_list = NOALLOC_MAX_TRIS;
   S.ctr = scratch + NOALLOC_MAX_TRIS;
   // the counters keep the previous call's values: start them at zero
   CK(cudaMemsetAsync(S.ctr, 0, sizeof(uint32_t) * CTR_N, s));
@@ -882,7 +947,8 @@ extern "C" int axr_shadow_map_noalloc(const float *xyz, const float *uv, const u
   long g = ((long)ntris + 255) / 256;
   if (g > (long)sms * 16) g = (long)sms * 16;
   k_shadow_setup_noalloc<<<(int)std::max(g, 1L), 256, 0, s>>>(G, S);
-  k_shadow_raster_noalloc<<<sms * 8, 128, 0, s>>>(G, S);
+  if (alpha_mask) k_shadow_raster_noalloc<true><<<sms * 6, 128, 0, s>>>(G, S);
+  else k_shadow_raster_noalloc<false><<<sms * 8, 128, 0, s>>>(G, S);
   CK(cudaGetLastError());
   return 0;
 }

@@ -7,7 +7,9 @@
 //   k_raster_small persistent; warps take 32 small triangles, each lane walks
 //                  its rows (drawSmall, Templates.py:250-323) and the warp
 //                  fills the queued spans pixel-parallel; fragment = 64-bit
-//                  atomicMin(depth key | ~order) in the L2-resident buffer
+//                  atomicMin(depth key | ~order) in the L2-resident buffer.
+//                  Opaque and alpha-tested materials run as separate
+//                  specialisations (the opaque one needs far fewer registers)
 //   k_coarse       per large triangle: tile binning of coarse.c, written as
 //                  (triangle, tile) units with warp-scan offsets
 //   k_raster_tiled persistent over units: per-tile restart of the tiled
@@ -33,14 +35,26 @@ struct DrawParams {
   uint64_t *keys;
   uint16_t *ro, *go, *bo;
   float *db;
-  uint32_t *small_list, *large_list;
-  uint2 *units;
-  uint32_t *ctr;       // see CTR_*
+  uint32_t *small_list;  // opaque small triangles from the front, alpha-tested from the back
+  uint32_t *items;       // row chunks of small triangles: (list position << 2 | chunk), same two ends
+  uint32_t *large_list;
+  uint2 *units;          // opaque (triangle, tile) units from the front, alpha-tested from the back
+  uint32_t *ctr;         // see CTR_*
   uint32_t cap_list, cap_units;
 };
 
-enum { CTR_SMALL = 0, CTR_LARGE = 1, CTR_UNITS = 2, CTR_WORK_SMALL = 3, CTR_WORK_UNITS = 4, CTR_OVERFLOW = 5,
-       CTR_WORK_LARGE = 6, CTR_SH_LIST = 7, CTR_SH_WORK = 8, CTR_N = 16 };
+enum {
+  CTR_SMALL = 0, CTR_SMALL_A, CTR_LARGE, CTR_UNITS, CTR_UNITS_A, CTR_WORK_SMALL, CTR_WORK_SMALL_A, CTR_WORK_LARGE,
+  CTR_WORK_UNITS, CTR_WORK_UNITS_A, CTR_OVERFLOW, CTR_SH_LIST, CTR_SH_LIST_A, CTR_SH_WORK, CTR_SH_WORK_A,
+  CTR_UNITS_RESERVED, CTR_LIMIT, CTR_ITEMS, CTR_ITEMS_A, CTR_N = 32
+};
+
+// Every data-dependent loop is bounded by construction (rows of a small
+// triangle < 2*96, of a tile unit <= 2*16, of a shadow triangle <= 2*(dim+240)
+// because of the setup rejections).  As a second line of defence each one
+// also stops after LOOP_LIMIT rounds and records that in ctr[CTR_LIMIT],
+// which the host reports as an error.
+constexpr int LOOP_LIMIT = 1 << 16;
 
 // ------------------------------------------------------------ helpers
 
@@ -60,6 +74,19 @@ __device__ __forceinline__ void span_clip(int ax0, float bound, int w, int &lo, 
   float fb = floorf(bound);
   int hi = fb >= (float)(w - 1) ? w - 1 : f2i(fb);
   cnt = hi >= lo ? hi - lo + 1 : 0;
+}
+
+// A small triangle's rows (bottom half y1..y2, then top half y3..y2, both
+// inclusive) are cut into at most MAX_CHUNKS chunks of at least MIN_CHUNK
+// rows, so that large "small" triangles spread over several lanes; a lane
+// replays the row accumulation up to its chunk, which keeps every
+// interpolant bit-identical to the serial walk.
+constexpr int MIN_CHUNK = 16;
+constexpr int MAX_CHUNKS = 3;
+__device__ __forceinline__ int small_rows(int y1, int y3) { return y3 - y1 + 2; }
+__device__ __forceinline__ int chunk_len(int rows) {
+  int c = (rows + MAX_CHUNKS - 1) / MAX_CHUNKS;
+  return c < MIN_CHUNK ? MIN_CHUNK : c;
 }
 
 // ------------------------------------------------------------ keys / clear
@@ -128,85 +155,137 @@ __global__ void __launch_bounds__(256) k_setup(DrawParams P) {
   for (int base = blockIdx.x * blockDim.x; base < P.total_tris; base += gridDim.x * blockDim.x) {
     int t = base + threadIdx.x;
     int cls = 0;
+    bool alpha = false;
+    int iy0 = 0, iy1 = 0, iy2 = 0;
     if (t < P.total_tris) {
       int g = find_group(sg, P.ngroups, (uint32_t)t);
       const GroupDev &G = sg[g];
       if (G.enabled) {
         float sx[3], sy[3], sz[3];
         cls = project_persp(G, t - G.tri_base, P.view, sx, sy, sz);
+        alpha = (G.flags & F_ALPHA) != 0;
+        iy0 = f2i(sy[0]); iy1 = f2i(sy[1]); iy2 = f2i(sy[2]);
       }
     }
-    unsigned ms = __ballot_sync(FULL, cls == 1), ml = __ballot_sync(FULL, cls == 2);
-    uint32_t bs = 0, bl = 0;
+    unsigned ms = __ballot_sync(FULL, cls == 1 && !alpha), ma = __ballot_sync(FULL, cls == 1 && alpha);
+    unsigned ml = __ballot_sync(FULL, cls == 2);
+    uint32_t bs = 0, ba = 0, bl = 0;
     if (lane == 0) {
       if (ms) bs = atomicAdd(&P.ctr[CTR_SMALL], __popc(ms));
+      if (ma) ba = atomicAdd(&P.ctr[CTR_SMALL_A], __popc(ma));
       if (ml) bl = atomicAdd(&P.ctr[CTR_LARGE], __popc(ml));
     }
     bs = __shfl_sync(FULL, bs, 0);
+    ba = __shfl_sync(FULL, ba, 0);
     bl = __shfl_sync(FULL, bl, 0);
     unsigned lt = (1u << lane) - 1;
-    if (cls == 1) P.small_list[bs + __popc(ms & lt)] = (uint32_t)t;
+    uint32_t pos = 0;
+    if (cls == 1 && !alpha) { pos = bs + __popc(ms & lt); P.small_list[pos] = (uint32_t)t; }
+    if (cls == 1 && alpha) { pos = ba + __popc(ma & lt); P.small_list[P.cap_list - 1 - pos] = (uint32_t)t; }
     if (cls == 2) P.large_list[bl + __popc(ml & lt)] = (uint32_t)t;
+    // row chunks of the small triangles
+    int nch = 0;
+    if (cls == 1) {
+      int y0 = min(iy0, min(iy1, iy2)), y3 = max(iy0, max(iy1, iy2));
+      int rows = small_rows(y0, y3);
+      nch = (rows + chunk_len(rows) - 1) / chunk_len(rows);
+    }
+    int co = (cls == 1 && !alpha) ? nch : 0, ca = (cls == 1 && alpha) ? nch : 0;
+    int io = co, ia = ca;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(FULL, io, o), va = __shfl_up_sync(FULL, ia, o);
+      if (lane >= o) { io += v; ia += va; }
+    }
+    uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
+    uint32_t oo = 0, oa = 0;
+    if (lane == 31) {
+      if (to) oo = atomicAdd(&P.ctr[CTR_ITEMS], to);
+      if (ta) oa = atomicAdd(&P.ctr[CTR_ITEMS_A], ta);
+    }
+    oo = __shfl_sync(FULL, oo, 31) + (uint32_t)(io - co);
+    oa = __shfl_sync(FULL, oa, 31) + (uint32_t)(ia - ca);
+    uint32_t cap_items = P.cap_list * MAX_CHUNKS;
+    for (int c = 0; c < nch; c++) {
+      uint32_t item = (pos << 2) | (uint32_t)c;
+      if (!alpha) P.items[oo + c] = item;
+      else P.items[cap_items - 1 - (oa + c)] = item;
+    }
   }
 }
 
 // ------------------------------------------------------------ span queue
 
-struct SpanV {
-  int cy, lo, cnt;
-  uint32_t ord;
-  float cx1, cx2, cz1, cz2;
-  float u1x, u1y, u2x, u2y;
-  int g, alen;
-  int pad0, pad1;
+// One round of spans, one per lane, in structure-of-arrays form in shared
+// memory; the warp then fills their pixels cooperatively.  d = cx1 - cx2 and
+// rd = its reciprocal (or 0) are per span, so a pixel's t costs one multiply
+// and two fused multiply-adds instead of a division.
+template <bool ALPHA>
+struct VisQ {
+  int cyw[32], lo[32];
+  uint32_t ord[32];
+  float cx2[32], d[32], rd[32], cz1[32], cz2[32];
+  float u1x[ALPHA ? 32 : 1], u1y[ALPHA ? 32 : 1], u2x[ALPHA ? 32 : 1], u2y[ALPHA ? 32 : 1];
+  int g[ALPHA ? 32 : 1];
+  int pre[32];
 };
 
-// Per-fragment visibility: alpha test (av_draw_alpha.c:80-97) then the
-// packed depth/order atomicMin.
-__device__ __forceinline__ void vis_fragment(const DrawParams &P, const GroupDev *sg, const SpanV &s, int ax) {
-  float t = ((float)ax - s.cx2) / (s.cx1 - s.cx2);
-  t = clamp_t(t);
-  float tz = 1.0f / ((1 - t) * s.cz2 + t * s.cz1);
-  if (tz != tz) return;
-  if (s.g >= 0) {
-    float omt = 1 - t;
-    V2 uvi{omt * s.u2x + t * s.u1x, omt * s.u2y + t * s.u1y};
-    Taps q = make_taps(uvi, tz, s.alen, 0);
-    float ca = bilerp_bool(q, sg[s.g].amask);
-    if (!(ca > 0.5f)) return;
-  }
-  atomicMin((unsigned long long *)&P.keys[(size_t)P.view.w * s.cy + ax], (unsigned long long)frag_key(tz, s.ord));
-}
-
-// Drain one round of spans (one per lane) cooperatively across the warp.
-__device__ __forceinline__ void warp_fill(const DrawParams &P, const GroupDev *sg, SpanV *q, int *pre, int lane,
-                                          const SpanV &mine) {
-  int c = mine.cnt;
-  int incl = c;
+// Exclusive offsets of the lanes' pixel counts; returns the round's total.
+__device__ __forceinline__ int warp_offsets(int cnt, int lane, int *pre) {
+  int incl = cnt;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     int v = __shfl_up_sync(FULL, incl, o);
     if (lane >= o) incl += v;
   }
-  int total = __shfl_sync(FULL, incl, 31);
+  pre[lane] = incl - cnt;
+  return __shfl_sync(FULL, incl, 31);
+}
+
+// index of the span holding pixel p: the largest s with pre[s] <= p
+__device__ __forceinline__ int span_of(const int *pre, int p) {
+  int s = 0;
+#pragma unroll
+  for (int step = 16; step; step >>= 1)
+    if (pre[s + step] <= p) s += step;     // s + step <= 31
+  return s;
+}
+
+// Per-fragment visibility: alpha test (av_draw_alpha.c:80-97) then the
+// packed depth/order atomicMin.
+template <bool ALPHA>
+__device__ __forceinline__ void vis_pixel(const DrawParams &P, const GroupDev *sg, const VisQ<ALPHA> &q, int s, int ax) {
+  float t = quot_by_recip((float)ax - q.cx2[s], q.d[s], q.rd[s]);
+  t = clamp_t(t);
+  float tz = 1.0f / ((1 - t) * q.cz2[s] + t * q.cz1[s]);
+  if (tz != tz) return;
+  if (ALPHA) {
+    const GroupDev &G = sg[q.g[s]];
+    float omt = 1 - t;
+    V2 uvi{omt * q.u2x[s] + t * q.u1x[s], omt * q.u2y[s] + t * q.u1y[s]};
+    Taps tp = make_taps(uvi, tz, G.alen, 0);
+    if (!(bilerp_quad(tp, G.aquad) > 0.5f)) return;
+  }
+  atomicMin((unsigned long long *)&P.keys[(size_t)q.cyw[s] + ax], (unsigned long long)frag_key(tz, q.ord[s]));
+}
+
+template <bool ALPHA>
+__device__ __forceinline__ void vis_fill(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, int cnt) {
+  int total = warp_offsets(cnt, lane, q.pre);
   if (total == 0) return;
-  q[lane] = mine;
-  pre[lane] = incl - c;
   __syncwarp();
   for (int p = lane; p < total; p += 32) {
-    int s = 0;
-#pragma unroll
-    for (int step = 16; step; step >>= 1)
-      if (pre[s + step] <= p) s += step;
-    vis_fragment(P, sg, q[s], q[s].lo + (p - pre[s]));
+    int s = span_of(q.pre, p);
+    vis_pixel<ALPHA>(P, sg, q, s, q.lo[s] + (p - q.pre[s]));
   }
   __syncwarp();
 }
 
 // ------------------------------------------------------------ small triangles
 
+template <bool ALPHA>
 struct SmallLane {
-  int g, alen;
+  int g;
   uint32_t gtri;
   int x1, x2, x3, y1, y2, y3;
   float z1, z2, z3, x4, z4;
@@ -214,7 +293,6 @@ struct SmallLane {
   int half, cy;
   float s1, s2, sz1, sz2, cx1, cx2, cz1, cz2;
   V2 su1, su2, cu1, cu2;
-  bool alpha;
 
   __device__ __forceinline__ void start_half0() {
     half = 0;
@@ -225,7 +303,7 @@ struct SmallLane {
     sz2 = (z4 - z1) * yd;
     cx1 = cx2 = (float)x1;
     cz1 = cz2 = z1;
-    if (alpha) {
+    if (ALPHA) {
       su1 = mul2(sub2(uv2, uv1), yd);
       su2 = mul2(sub2(uv4, uv1), yd);
       cu1 = cu2 = uv1;
@@ -233,7 +311,7 @@ struct SmallLane {
     if (s1 < s2) {
       float t = s1; s1 = s2; s2 = t;
       t = sz1; sz1 = sz2; sz2 = t;
-      V2 tv = su1; su1 = su2; su2 = tv;
+      if (ALPHA) { V2 tv = su1; su1 = su2; su2 = tv; }
     }
     cy = y1;
   }
@@ -246,7 +324,7 @@ struct SmallLane {
     sz2 = (z3 - z4) * yd;
     cx1 = cx2 = (float)x3;
     cz1 = cz2 = z3;
-    if (alpha) {
+    if (ALPHA) {
       su1 = mul2(neg2(sub2(uv2, uv3)), yd);
       su2 = mul2(neg2(sub2(uv4, uv3)), yd);
       cu1 = cu2 = uv3;
@@ -254,9 +332,34 @@ struct SmallLane {
     if (s1 < s2) {
       float t = s1; s1 = s2; s2 = t;
       t = sz1; sz1 = sz2; sz2 = t;
-      V2 tv = su1; su1 = su2; su2 = tv;
+      if (ALPHA) { V2 tv = su1; su1 = su2; su2 = tv; }
     }
     cy = y3;
+  }
+
+  int left;   // rows left in this lane's chunk
+
+  // advances one row without drawing (the replay up to a chunk's first row)
+  __device__ __forceinline__ void skip_row() {
+    if (half == 0) {
+      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
+      if (ALPHA) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
+      cy++;
+      if (cy > y2) start_half1();
+    } else {
+      cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
+      if (ALPHA) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
+      cy--;
+    }
+  }
+
+  __device__ __forceinline__ void init_chunk(const DrawParams &P, const GroupDev *sg, uint32_t t, int chunk) {
+    init(P, sg, t);
+    int rows = small_rows(y1, y3);
+    int cl = chunk_len(rows);
+    int first = chunk * cl;
+    left = min(cl, rows - first);
+    for (int r = 0; r < first; r++) skip_row();
   }
 
   __device__ __forceinline__ void init(const DrawParams &P, const GroupDev *sg, uint32_t t) {
@@ -269,14 +372,13 @@ struct SmallLane {
     int ix[3], iy[3];
     float z[3];
     Attr<false> a[3];
-    alpha = (G.flags & F_ALPHA) != 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       ix[k] = f2i(sx[k]); iy[k] = f2i(sy[k]); z[k] = sz[k];
-      if (alpha) a[k] = a_load<false>(G, tri, k, sz[k]);
+      if (ALPHA) a[k] = a_load<false>(G, tri, k, sz[k]);
     }
 #define SW(i, j) { int ti = iy[i]; iy[i] = iy[j]; iy[j] = ti; ti = ix[i]; ix[i] = ix[j]; ix[j] = ti; \
-                   float tf = z[i]; z[i] = z[j]; z[j] = tf; Attr<false> ta = a[i]; a[i] = a[j]; a[j] = ta; }
+                   float tf = z[i]; z[i] = z[j]; z[j] = tf; if (ALPHA) { Attr<false> ta = a[i]; a[i] = a[j]; a[j] = ta; } }
     if (iy[0] > iy[1]) SW(0, 1);
     if (iy[1] > iy[2]) SW(1, 2);
     if (iy[0] > iy[1]) SW(0, 1);
@@ -286,65 +388,68 @@ struct SmallLane {
     float yd = (float)(y2 - y1) / (float)(y3 - y1);
     x4 = (float)x1 + yd * (float)(x3 - x1);
     z4 = z1 + yd * (z3 - z1);
-    if (alpha) {
+    if (ALPHA) {
       uv4 = add2(a[0].uv, smul2(yd, sub2(a[2].uv, a[0].uv)));
-      int num_mip = (G.flags & F_MIP) ? G.tex_size : 0;
-      if (G.flags & F_MIP) mip_setup<false>(a, z, true, ix, iy, nullptr, nullptr, num_mip, G.mip_bias);
+      if (G.flags & F_MIP) mip_setup<false>(a, z, true, ix, iy, nullptr, nullptr, G.tex_size, G.mip_bias);
       uv1 = a[0].uv; uv2 = a[1].uv; uv3 = a[2].uv;
-      alen = G.alen;
     }
     start_half0();
   }
 
-  // emits the span of the current row and advances; returns false when done
-  __device__ __forceinline__ bool step(const DrawParams &P, SpanV &s) {
-    s.cnt = 0;
-    s.cy = cy;
-    s.ord = make_order(0, gtri, half);
-    s.cx1 = cx1; s.cx2 = cx2; s.cz1 = cz1; s.cz2 = cz2;
-    s.g = alpha ? g : -1;
-    s.alen = alen;
-    if (alpha) { s.u1x = cu1.x; s.u1y = cu1.y; s.u2x = cu2.x; s.u2y = cu2.y; }
+  // writes the current row's span into q[lane], advances; returns the span's
+  // pixel count and sets `live` false after the last row
+  __device__ __forceinline__ int emit(const DrawParams &P, VisQ<ALPHA> &q, int lane, bool &live) {
+    int lo = 0, cnt = 0;
     if (cy >= 0 && cy < P.view.h) {
-      if (half == 0) span_clip(f2i(cx2), cx1, P.view.w, s.lo, s.cnt);
-      else span_clip(f2i(cx1), cx2, P.view.w, s.lo, s.cnt);
+      if (half == 0) span_clip(f2i(cx2), cx1, P.view.w, lo, cnt);
+      else span_clip(f2i(cx1), cx2, P.view.w, lo, cnt);
     }
-    if (half == 0) {
-      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
-      if (alpha) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
-      cy++;
-      if (cy > y2) start_half1();
-      return true;
+    if (cnt) {
+      float d = cx1 - cx2;
+      q.cyw[lane] = cy * P.view.w;
+      q.lo[lane] = lo;
+      q.ord[lane] = make_order(0, gtri, half);
+      q.cx2[lane] = cx2; q.d[lane] = d; q.rd[lane] = span_recip(d);
+      q.cz1[lane] = cz1; q.cz2[lane] = cz2;
+      if (ALPHA) { q.u1x[lane] = cu1.x; q.u1y[lane] = cu1.y; q.u2x[lane] = cu2.x; q.u2y[lane] = cu2.y; q.g[lane] = g; }
     }
-    cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
-    if (alpha) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
-    cy--;
-    return cy >= y2;
+    skip_row();
+    live = --left > 0;
+    return cnt;
   }
 };
 
-__global__ void __launch_bounds__(128) k_raster_small(DrawParams P) {
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_small(DrawParams P) {
   __shared__ GroupDev sg[64];
-  __shared__ SpanV q[4][32];
-  __shared__ int pre[4][33];
+  __shared__ VisQ<ALPHA> qs[4];
   for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
   __syncthreads();
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t n = P.ctr[CTR_SMALL];
+  VisQ<ALPHA> &q = qs[w];
+  uint32_t n = P.ctr[ALPHA ? CTR_ITEMS_A : CTR_ITEMS];
+  uint32_t cap_items = P.cap_list * MAX_CHUNKS;
   while (true) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&P.ctr[CTR_WORK_SMALL], 32u);
+    if (lane == 0) base = atomicAdd(&P.ctr[ALPHA ? CTR_WORK_SMALL_A : CTR_WORK_SMALL], 32u);
     base = __shfl_sync(FULL, base, 0);
     if (base >= n) break;
-    SmallLane L;
+    SmallLane<ALPHA> L;
     bool live = base + lane < n;
-    if (live) L.init(P, sg, P.small_list[base + lane]);
-    while (__any_sync(FULL, live)) {
-      SpanV s;
-      s.cnt = 0;
-      if (live) live = L.step(P, s);
-      warp_fill(P, sg, q[w], pre[w], lane, s);
+    if (live) {
+      uint32_t idx = base + lane;
+      uint32_t item = P.items[ALPHA ? cap_items - 1 - idx : idx];
+      uint32_t pos = item >> 2;
+      L.init_chunk(P, sg, P.small_list[ALPHA ? P.cap_list - 1 - pos : pos], (int)(item & 3));
+    }
+    for (int round = 0; __any_sync(FULL, live); round++) {
+      if (round == LOOP_LIMIT) {
+        if (lane == 0) atomicOr(&P.ctr[CTR_LIMIT], 1u);
+        break;
+      }
+      int cnt = 0;
+      if (live) cnt = L.emit(P, q, lane, live);
+      vis_fill<ALPHA>(P, sg, q, lane, cnt);
     }
   }
 }
@@ -368,8 +473,9 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
   if (s1 < s2) { t = s1; s1 = s2; s2 = t; }
   float sbias = 1.f + floorf(y1) - y1;
   float wcm1 = (float)wc - 1;
+  int guard = 0;
   if (y1 != y2) {
-    for (int cy = f2i(floorf(y1)); (float)cy <= ceilf(y2); cy++) {
+    for (int cy = f2i(floorf(y1)); (float)cy <= ceilf(y2) && guard < LOOP_LIMIT; cy++, guard++) {
       float mx1 = cx1 + sbias * s1;
       if (s1 < 0) mx1 -= s1;
       float mx2 = cx2 + sbias * s2;
@@ -379,7 +485,7 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
       if (cy >= 0 && cy < hc) {
         int a1 = f2i(floorf(mx2));
         float hb = ceilf(mx1);
-        for (int ax = a1; (float)ax <= hb; ax++) emit(wc * cy + ax);
+        for (int ax = a1; (float)ax <= hb && ax < wc; ax++) emit(wc * cy + ax);
       }
       cx1 += s1;
       cx2 += s2;
@@ -391,7 +497,7 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
   if (s1 < s2) { t = s1; s1 = s2; s2 = t; }
   sbias = y3 - floorf(y3);
   if (y2 != y3) {
-    for (int cy = f2i(ceilf(y3)); (float)cy >= floorf(y2); cy--) {
+    for (int cy = f2i(ceilf(y3)); (float)cy >= floorf(y2) && guard < 2 * LOOP_LIMIT; cy--, guard++) {
       float mx1 = cx1 - sbias * s1;
       if (s1 < 0) mx1 += s1;
       float mx2 = cx2 - sbias * s2;
@@ -401,7 +507,7 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
       if (cy >= 0 && cy < hc) {
         int a1 = f2i(floorf(mx1));
         float hb = ceilf(mx2);
-        for (int ax = a1; (float)ax <= hb; ax++) emit(wc * cy + ax);
+        for (int ax = a1; (float)ax <= hb && ax < wc; ax++) emit(wc * cy + ax);
       }
       cx1 -= s1;
       cx2 -= s2;
@@ -409,6 +515,7 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
   }
 }
 
+// Opaque units fill the queue from the front, alpha-tested ones from the back.
 __global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
   __shared__ GroupDev sg[64];
   for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
@@ -425,29 +532,50 @@ __global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
     float sx[3], sy[3], sz[3];
     uint32_t gt = 0;
     int cnt = 0;
+    bool alpha = false;
     if (live) {
       gt = P.large_list[base + lane];
       const GroupDev &G = sg[find_group(sg, P.ngroups, gt)];
+      alpha = (G.flags & F_ALPHA) != 0;
       project_persp(G, (int)(gt - G.tri_base), P.view, sx, sy, sz);
       coarse_walk(sx, sy, wc, hc, [&](int) { cnt++; });
     }
-    int incl = cnt;
+    int co = alpha ? 0 : cnt, ca = alpha ? cnt : 0;
+    int io = co, ia = ca;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(FULL, incl, o);
-      if (lane >= o) incl += v;
+      int v = __shfl_up_sync(FULL, io, o);
+      int va = __shfl_up_sync(FULL, ia, o);
+      if (lane >= o) { io += v; ia += va; }
     }
-    uint32_t total = (uint32_t)__shfl_sync(FULL, incl, 31);
-    uint32_t off = 0;
-    if (lane == 31 && total) off = atomicAdd(&P.ctr[CTR_UNITS], total);
-    off = __shfl_sync(FULL, off, 31) + (uint32_t)(incl - cnt);
-    if (live && cnt) {
-      if ((uint64_t)off + (uint64_t)cnt > (uint64_t)P.cap_units) {
+    uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
+    // Capacity is reserved for both kinds together, so the opaque units
+    // (growing from the front) and the alpha units (from the back) never
+    // meet; after an overflow the fallback kernel draws every large triangle.
+    uint32_t oo = 0, oa = 0, fits = 1;
+    if (lane == 31 && to + ta) {
+      uint32_t r = atomicAdd(&P.ctr[CTR_UNITS_RESERVED], to + ta);
+      if ((uint64_t)r + to + ta > (uint64_t)P.cap_units) {
+        fits = 0;
         atomicOr(&P.ctr[CTR_OVERFLOW], 1u);
       } else {
-        uint2 *u = P.units + off;
+        if (to) oo = atomicAdd(&P.ctr[CTR_UNITS], to);
+        if (ta) oa = atomicAdd(&P.ctr[CTR_UNITS_A], ta);
+      }
+    }
+    fits = __shfl_sync(FULL, fits, 31);
+    oo = __shfl_sync(FULL, oo, 31) + (uint32_t)(io - co);
+    oa = __shfl_sync(FULL, oa, 31) + (uint32_t)(ia - ca);
+    if (live && cnt && fits) {
+      {
         int k = 0;
-        coarse_walk(sx, sy, wc, hc, [&](int tile) { u[k++] = make_uint2(gt, (uint32_t)tile); });
+        if (!alpha) {
+          uint2 *u = P.units + oo;
+          coarse_walk(sx, sy, wc, hc, [&](int tile) { u[k++] = make_uint2(gt, (uint32_t)tile); });
+        } else {
+          uint2 *u = P.units + (P.cap_units - 1 - oa);
+          coarse_walk(sx, sy, wc, hc, [&](int tile) { *(u - k) = make_uint2(gt, (uint32_t)tile); k++; });
+        }
       }
     }
   }
@@ -455,8 +583,9 @@ __global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
 
 // ------------------------------------------------------------ tiled (large) raster
 
+template <bool ALPHA>
 struct TileLane {
-  int g, alen;
+  int g;
   uint32_t gtri;
   float x1, x2, x3, y1, y2, y3, z1, z2, z3, x4, z4;
   V2 uv1, uv2, uv3, uv4;
@@ -466,7 +595,6 @@ struct TileLane {
   float ybound;
   float s1, s2, sz1, sz2, cx1, cx2, cz1, cz2;
   V2 su1, su2, cu1, cu2;
-  bool alpha;
 
   __device__ __forceinline__ void start_half0() {
     half = 0;
@@ -475,17 +603,17 @@ struct TileLane {
     s2 = (x4 - x1) * yd;
     sz1 = (z2 - z1) * yd;
     sz2 = (z4 - z1) * yd;
-    if (alpha) { su1 = mul2(sub2(uv2, uv1), yd); su2 = mul2(sub2(uv4, uv1), yd); }
+    if (ALPHA) { su1 = mul2(sub2(uv2, uv1), yd); su2 = mul2(sub2(uv4, uv1), yd); }
     if (s1 < s2) {
       float t = s1; s1 = s2; s2 = t;
       t = sz1; sz1 = sz2; sz2 = t;
-      V2 tv = su1; su1 = su2; su2 = tv;
+      if (ALPHA) { V2 tv = su1; su1 = su2; su2 = tv; }
     }
     cy = f2i(clampf_(y1, yMin, yMax));
     float dy = (float)cy - y1;
     cx1 = x1 + dy * s1; cx2 = x1 + dy * s2;
     cz1 = z1 + dy * sz1; cz2 = z1 + dy * sz2;
-    if (alpha) { cu1 = add2(uv1, smul2(dy, su1)); cu2 = add2(uv1, smul2(dy, su2)); }
+    if (ALPHA) { cu1 = add2(uv1, smul2(dy, su1)); cu2 = add2(uv1, smul2(dy, su2)); }
     ybound = clampf_(y2, yMin, yMax);
     live_half = (y2 > yMin) && ((float)cy <= ybound);
   }
@@ -496,17 +624,17 @@ struct TileLane {
     s2 = (x3 - x4) * yd;
     sz1 = (z3 - z2) * yd;
     sz2 = (z3 - z4) * yd;
-    if (alpha) { su1 = mul2(neg2(sub2(uv2, uv3)), yd); su2 = mul2(neg2(sub2(uv4, uv3)), yd); }
+    if (ALPHA) { su1 = mul2(neg2(sub2(uv2, uv3)), yd); su2 = mul2(neg2(sub2(uv4, uv3)), yd); }
     if (s1 < s2) {
       float t = s1; s1 = s2; s2 = t;
       t = sz1; sz1 = sz2; sz2 = t;
-      V2 tv = su1; su1 = su2; su2 = tv;
+      if (ALPHA) { V2 tv = su1; su1 = su2; su2 = tv; }
     }
     cy = f2i(clampf_(y3, yMin, yMax));
     float dy = (float)cy - y3;
     cx1 = x3 + dy * s1; cx2 = x3 + dy * s2;
     cz1 = z3 + dy * sz1; cz2 = z3 + dy * sz2;
-    if (alpha) { cu1 = add2(uv3, smul2(dy, su1)); cu2 = add2(uv3, smul2(dy, su2)); }
+    if (ALPHA) { cu1 = add2(uv3, smul2(dy, su1)); cu2 = add2(uv3, smul2(dy, su2)); }
     ybound = clampf_(y2, yMin, yMax);
     live_half = (y2 < yMax) && ((float)cy >= ybound);
   }
@@ -520,16 +648,15 @@ struct TileLane {
     int tri = (int)(gtri - G.tri_base);
     float sx[3], sy[3], sz[3];
     project_persp(G, tri, P.view, sx, sy, sz);
-    alpha = (G.flags & F_ALPHA) != 0;
     Attr<false> a[3];
     float x[3], y[3], z[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       x[k] = sx[k]; y[k] = sy[k]; z[k] = sz[k];
-      if (alpha) a[k] = a_load<false>(G, tri, k, sz[k]);
+      if (ALPHA) a[k] = a_load<false>(G, tri, k, sz[k]);
     }
 #define SW(i, j) { float tf = y[i]; y[i] = y[j]; y[j] = tf; tf = x[i]; x[i] = x[j]; x[j] = tf; \
-                   tf = z[i]; z[i] = z[j]; z[j] = tf; Attr<false> ta = a[i]; a[i] = a[j]; a[j] = ta; }
+                   tf = z[i]; z[i] = z[j]; z[j] = tf; if (ALPHA) { Attr<false> ta = a[i]; a[i] = a[j]; a[j] = ta; } }
     if (y[0] > y[1]) SW(0, 1);
     if (y[1] > y[2]) SW(1, 2);
     if (y[0] > y[1]) SW(0, 1);
@@ -539,11 +666,10 @@ struct TileLane {
     float yd = (y2 - y1) / (y3 - y1);
     x4 = x1 + yd * (x3 - x1);
     z4 = z1 + yd * (z3 - z1);
-    if (alpha) {
+    if (ALPHA) {
       uv4 = add2(a[0].uv, smul2(yd, sub2(a[2].uv, a[0].uv)));
       if (G.flags & F_MIP) mip_setup<false>(a, z, false, nullptr, nullptr, x, y, G.tex_size, G.mip_bias);
       uv1 = a[0].uv; uv2 = a[1].uv; uv3 = a[2].uv;
-      alen = G.alen;
     }
     int wc = P.view.w / TILE;
     int tileX = bx % wc;
@@ -557,63 +683,118 @@ struct TileLane {
     return live_half;
   }
 
-  __device__ __forceinline__ bool step(SpanV &s) {
-    s.cnt = 0;
-    s.cy = cy;
-    s.ord = make_order(1, gtri, half);
-    s.cx1 = cx1; s.cx2 = cx2; s.cz1 = cz1; s.cz2 = cz2;
-    s.g = alpha ? g : -1;
-    s.alen = alen;
-    if (alpha) { s.u1x = cu1.x; s.u1y = cu1.y; s.u2x = cu2.x; s.u2y = cu2.y; }
+  __device__ __forceinline__ void put(const DrawParams &P, VisQ<ALPHA> &q, int lane, int lo) {
+    float d = cx1 - cx2;
+    q.cyw[lane] = cy * P.view.w;
+    q.lo[lane] = lo;
+    q.ord[lane] = make_order(1, gtri, half);
+    q.cx2[lane] = cx2; q.d[lane] = d; q.rd[lane] = span_recip(d);
+    q.cz1[lane] = cz1; q.cz2[lane] = cz2;
+    if (ALPHA) { q.u1x[lane] = cu1.x; q.u1y[lane] = cu1.y; q.u2x[lane] = cu2.x; q.u2y[lane] = cu2.y; q.g[lane] = g; }
+  }
+
+  __device__ __forceinline__ int emit(const DrawParams &P, VisQ<ALPHA> &q, int lane, bool &live) {
+    int cnt = 0;
     if (half == 0) {
       if (cx2 < xMax && cx1 > xMin) {
-        s.lo = f2i(clampf_(cx2, xMin, xMax));
+        int lo = f2i(clampf_(cx2, xMin, xMax));
         int hi = f2i(floorf(clampf_(cx1, xMin, xMax)));
-        s.cnt = hi >= s.lo ? hi - s.lo + 1 : 0;
+        cnt = hi >= lo ? hi - lo + 1 : 0;
+        if (cnt) put(P, q, lane, lo);
       }
       cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
-      if (alpha) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
+      if (ALPHA) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
       cy++;
-      if ((float)cy <= ybound) return true;
-      start_half1();
-      return live_half;
+      if ((float)cy > ybound) {
+        start_half1();
+        live = live_half;
+      }
+      return cnt;
     }
     if (cx1 < xMax && cx2 > xMin) {
-      s.lo = f2i(clampf_(cx1, xMin, xMax));
+      int lo = f2i(clampf_(cx1, xMin, xMax));
       int hi = f2i(floorf(clampf_(cx2, xMin, xMax)));
-      s.cnt = hi >= s.lo ? hi - s.lo + 1 : 0;
+      cnt = hi >= lo ? hi - lo + 1 : 0;
+      if (cnt) put(P, q, lane, lo);
     }
     cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
-    if (alpha) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
+    if (ALPHA) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
     cy--;
-    return (float)cy >= ybound;
+    live = (float)cy >= ybound;
+    return cnt;
   }
 };
 
-__global__ void __launch_bounds__(128) k_raster_tiled(DrawParams P) {
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_tiled(DrawParams P) {
   __shared__ GroupDev sg[64];
-  __shared__ SpanV q[4][32];
-  __shared__ int pre[4][33];
+  __shared__ VisQ<ALPHA> qs[4];
   for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
   __syncthreads();
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t n = min(P.ctr[CTR_UNITS], P.cap_units);
   if (P.ctr[CTR_OVERFLOW]) return;
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  VisQ<ALPHA> &q = qs[w];
+  uint32_t n = P.ctr[ALPHA ? CTR_UNITS_A : CTR_UNITS];
   while (true) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&P.ctr[CTR_WORK_UNITS], 32u);
+    if (lane == 0) base = atomicAdd(&P.ctr[ALPHA ? CTR_WORK_UNITS_A : CTR_WORK_UNITS], 32u);
     base = __shfl_sync(FULL, base, 0);
     if (base >= n) break;
-    TileLane L;
+    TileLane<ALPHA> L;
     bool live = false;
-    if (base + lane < n) live = L.init(P, sg, P.units[base + lane]);
-    while (__any_sync(FULL, live)) {
-      SpanV s;
-      s.cnt = 0;
-      if (live) live = L.step(s);
-      warp_fill(P, sg, q[w], pre[w], lane, s);
+    if (base + lane < n) {
+      uint32_t idx = base + lane;
+      live = L.init(P, sg, P.units[ALPHA ? P.cap_units - 1 - idx : idx]);
     }
+    for (int round = 0; __any_sync(FULL, live); round++) {
+      if (round == LOOP_LIMIT) {
+        if (lane == 0) atomicOr(&P.ctr[CTR_LIMIT], 1u);
+        break;
+      }
+      int cnt = 0;
+      if (live) cnt = L.emit(P, q, lane, live);
+      vis_fill<ALPHA>(P, sg, q, lane, cnt);
+    }
+  }
+}
+
+// Tile-unit queue overflow: every large triangle is rasterized here instead,
+// one triangle per warp, its coarse tiles dealt round-robin to the lanes and
+// each lane filling its tiles on its own (slow, same fragments).
+template <bool ALPHA>
+__device__ __forceinline__ void fallback_unit(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane,
+                                              uint32_t gt, int tile) {
+  TileLane<ALPHA> L;
+  bool live = L.init(P, sg, make_uint2(gt, (uint32_t)tile));
+  for (int round = 0; live && round < LOOP_LIMIT; round++) {
+    int cnt = L.emit(P, q, lane, live);
+    for (int j = 0; j < cnt; j++) vis_pixel<ALPHA>(P, sg, q, lane, q.lo[lane] + j);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_raster_tiled_fallback(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  __shared__ VisQ<false> qo[4];
+  __shared__ VisQ<true> qa[4];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  if (!P.ctr[CTR_OVERFLOW]) return;
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  uint32_t n = P.ctr[CTR_LARGE];
+  int wc = P.view.w / TILE, hc = P.view.h / TILE;
+  for (uint32_t i = gw; i < n; i += nw) {
+    uint32_t gt = P.large_list[i];
+    const GroupDev &G = sg[find_group(sg, P.ngroups, gt)];
+    bool alpha = (G.flags & F_ALPHA) != 0;
+    float sx[3], sy[3], sz[3];
+    project_persp(G, (int)(gt - G.tri_base), P.view, sx, sy, sz);
+    int k = 0;
+    coarse_walk(sx, sy, wc, hc, [&](int tile) {
+      if ((k++ & 31) != lane) return;
+      if (alpha) fallback_unit<true>(P, sg, qa[w], lane, gt, tile);
+      else fallback_unit<false>(P, sg, qo[w], lane, gt, tile);
+    });
   }
 }
 
@@ -768,15 +949,18 @@ __device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev 
   if (mip) {
     // av_draw_normmap_mip.c:73-123
     Taps q1 = make_taps(uvi, tz, ms.len_mip, ms.start_mip);
-    outR = bilerp_u16(q1, G.tr); outG = bilerp_u16(q1, G.tg); outB = bilerp_u16(q1, G.tb);
+    V3 c1v = bilerp_rgb(q1, G.tex);
+    outR = c1v.x; outG = c1v.y; outB = c1v.z;
     Taps q2 = make_taps(uvi, tz, ms.len_mip2, ms.start_mip2);
     float ofm = 1 - ms.fmip;
-    outR = ofm * outR + ms.fmip * bilerp_u16(q2, G.tr);
-    outG = ofm * outG + ms.fmip * bilerp_u16(q2, G.tg);
-    outB = ofm * outB + ms.fmip * bilerp_u16(q2, G.tb);
+    V3 c2v = bilerp_rgb(q2, G.tex);
+    outR = ofm * outR + ms.fmip * c2v.x;
+    outG = ofm * outG + ms.fmip * c2v.y;
+    outB = ofm * outB + ms.fmip * c2v.z;
   } else {
     Taps q = make_taps(uvi, tz, G.tex_size, 0);
-    outR = bilerp_u16(q, G.tr); outG = bilerp_u16(q, G.tg); outB = bilerp_u16(q, G.tb);
+    V3 cv = bilerp_rgb(q, G.tex);
+    outR = cv.x; outG = cv.y; outB = cv.z;
   }
   float light = 1;
   if (G.flags & F_SHADOW) {
@@ -808,38 +992,6 @@ __global__ void __launch_bounds__(256) k_shade(DrawParams P) {
   shade_pixel(P, sg, ax, cy, key);
 }
 
-// Tile-unit queue overflow: every large triangle is rasterized here instead,
-// one triangle per warp, its coarse tiles dealt round-robin to the lanes and
-// each lane filling its tiles on its own (slow, same fragments).
-__global__ void __launch_bounds__(128) k_raster_tiled_fallback(DrawParams P) {
-  __shared__ GroupDev sg[64];
-  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  __syncthreads();
-  if (!P.ctr[CTR_OVERFLOW]) return;
-  int lane = threadIdx.x & 31;
-  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  uint32_t n = P.ctr[CTR_LARGE];
-  int wc = P.view.w / TILE, hc = P.view.h / TILE;
-  for (uint32_t i = gw; i < n; i += nw) {
-    uint32_t gt = P.large_list[i];
-    const GroupDev &G = sg[find_group(sg, P.ngroups, gt)];
-    float sx[3], sy[3], sz[3];
-    project_persp(G, (int)(gt - G.tri_base), P.view, sx, sy, sz);
-    int k = 0;
-    coarse_walk(sx, sy, wc, hc, [&](int tile) {
-      if ((k++ & 31) != lane) return;
-      TileLane L;
-      if (!L.init(P, sg, make_uint2(gt, (uint32_t)tile))) return;
-      bool more = true;
-      while (more) {
-        SpanV s;
-        more = L.step(s);
-        for (int j = 0; j < s.cnt; j++) vis_fragment(P, sg, s, s.lo + j);
-      }
-    });
-  }
-}
-
 __global__ void k_ids(const uint64_t *__restrict__ keys, int n, int32_t *tri_id, uint8_t *cov) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t ord = 0xffffffffu - (uint32_t)keys[i];
@@ -858,9 +1010,38 @@ struct ShadowParams {
   ShadowDev sh;
   float *map;
   float bias;
-  uint32_t *list;
+  uint32_t *list;      // opaque casters from the front, alpha-tested from the back
+  uint32_t cap_list;
   uint32_t *ctr;
 };
+
+__device__ __forceinline__ void shadow_classify(const GroupDev *sg, const ShadowParams &S, int t, bool &ok, bool &alpha) {
+  ok = false;
+  alpha = false;
+  if (t < S.total_tris) {
+    const GroupDev &G = sg[find_group(sg, S.ngroups, (uint32_t)t)];
+    if (G.enabled) {
+      int ix[3], iy[3];
+      float z[3];
+      ok = project_ortho(G, t - G.tri_base, S.sh, S.bias, ix, iy, z);
+      alpha = (G.flags & F_ALPHA) != 0;
+    }
+  }
+}
+
+__device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int lane) {
+  unsigned mo = __ballot_sync(FULL, ok && !alpha), ma = __ballot_sync(FULL, ok && alpha);
+  uint32_t bo = 0, ba = 0;
+  if (lane == 0) {
+    if (mo) bo = atomicAdd(&S.ctr[CTR_SH_LIST], __popc(mo));
+    if (ma) ba = atomicAdd(&S.ctr[CTR_SH_LIST_A], __popc(ma));
+  }
+  bo = __shfl_sync(FULL, bo, 0);
+  ba = __shfl_sync(FULL, ba, 0);
+  unsigned lt = (1u << lane) - 1;
+  if (ok && !alpha) S.list[bo + __popc(mo & lt)] = (uint32_t)t;
+  if (ok && alpha) S.list[S.cap_list - 1 - (ba + __popc(ma & lt))] = (uint32_t)t;
+}
 
 __global__ void __launch_bounds__(256) k_shadow_setup(ShadowParams S) {
   __shared__ GroupDev sg[64];
@@ -869,20 +1050,9 @@ __global__ void __launch_bounds__(256) k_shadow_setup(ShadowParams S) {
   int lane = threadIdx.x & 31;
   for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
     int t = base + threadIdx.x;
-    bool ok = false;
-    if (t < S.total_tris) {
-      const GroupDev &G = sg[find_group(sg, S.ngroups, (uint32_t)t)];
-      if (G.enabled) {
-        int ix[3], iy[3];
-        float z[3];
-        ok = project_ortho(G, t - G.tri_base, S.sh, S.bias, ix, iy, z);
-      }
-    }
-    unsigned m = __ballot_sync(FULL, ok);
-    uint32_t b = 0;
-    if (lane == 0 && m) b = atomicAdd(&S.ctr[CTR_SH_LIST], __popc(m));
-    b = __shfl_sync(FULL, b, 0);
-    if (ok) S.list[b + __popc(m & ((1u << lane) - 1))] = (uint32_t)t;
+    bool ok, alpha;
+    shadow_classify(sg, S, t, ok, alpha);
+    shadow_append(S, t, ok, alpha, lane);
   }
 }
 
@@ -891,33 +1061,36 @@ __device__ __forceinline__ void atomic_min_depth(float *addr, float v) {
   else atomicMax((unsigned int *)addr, __float_as_uint(v));
 }
 
-struct SpanS {
-  int cy, lo, cnt, alen;
-  float cx1, cx2, cz1, cz2;
-  float cu1, cv1, cu2, cv2;
-  const uint8_t *amask;
+template <bool ALPHA>
+struct ShadowQ {
+  int cyw[32], lo[32];
+  float cx2[32], d[32], rd[32], cz1[32], cz2[32];
+  float cu1[ALPHA ? 32 : 1], cv1[ALPHA ? 32 : 1], cu2[ALPHA ? 32 : 1], cv2[ALPHA ? 32 : 1];
+  int g[ALPHA ? 32 : 1];
+  int pre[32];
 };
 
+template <bool ALPHA>
 struct ShadowLane {
   int x1, x2, x3, y1, y2, y3, x4;
   float z1, z2, z3, z4, u1, u2, u3, u4, v1, v2, v3, v4;
-  int half, cy;
+  int half, cy, g;
   float s1, s2, sz1, sz2, su1, su2, sv1, sv2;
   float cx1, cx2, cz1, cz2, cu1, cu2, cv1, cv2;
-  const uint8_t *amask;
-  int alen;
 
   __device__ __forceinline__ void start_half0() {
     half = 0;
     float d = (float)(y2 - y1);
     s1 = (float)(x2 - x1) / d;
     s2 = (float)(x4 - x1) / d;
-    su1 = (u2 - u1) / d; sv1 = (v2 - v1) / d;
-    su2 = (u4 - u1) / d; sv2 = (v4 - v1) / d;
+    if (ALPHA) { su1 = (u2 - u1) / d; sv1 = (v2 - v1) / d; su2 = (u4 - u1) / d; sv2 = (v4 - v1) / d; }
     sz1 = (z2 - z1) / d; sz2 = (z4 - z1) / d;
     cx1 = cx2 = (float)x1; cz1 = cz2 = z1;
-    cu1 = cu2 = u1; cv1 = cv2 = v1;
-    if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(su1, su2); swap_(sv1, sv2); }
+    if (ALPHA) { cu1 = cu2 = u1; cv1 = cv2 = v1; }
+    if (s1 < s2) {
+      swap_(s1, s2); swap_(sz1, sz2);
+      if (ALPHA) { swap_(su1, su2); swap_(sv1, sv2); }
+    }
     cy = y1;
   }
   __device__ __forceinline__ void start_half1() {
@@ -925,137 +1098,144 @@ struct ShadowLane {
     float d = (float)(y3 - y2);
     s1 = (float)(x3 - x2) / d;
     s2 = (float)(x3 - x4) / d;
-    su1 = (u3 - u2) / d; sv1 = (v3 - v2) / d;
-    su2 = (u3 - u4) / d; sv2 = (v3 - v4) / d;
+    if (ALPHA) { su1 = (u3 - u2) / d; sv1 = (v3 - v2) / d; su2 = (u3 - u4) / d; sv2 = (v3 - v4) / d; }
     sz1 = (z3 - z2) / d; sz2 = (z3 - z4) / d;
     cx1 = cx2 = (float)x3; cz1 = cz2 = z3;
-    cu1 = cu2 = u3; cv1 = cv2 = v3;
-    if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(su1, su2); swap_(sv1, sv2); }
+    if (ALPHA) { cu1 = cu2 = u3; cv1 = cv2 = v3; }
+    if (s1 < s2) {
+      swap_(s1, s2); swap_(sz1, sz2);
+      if (ALPHA) { swap_(su1, su2); swap_(sv1, sv2); }
+    }
     cy = y3;
   }
 
   __device__ __forceinline__ bool init(const ShadowParams &S, const GroupDev *sg, uint32_t t) {
-    const GroupDev &G = sg[find_group(sg, S.ngroups, t)];
+    g = find_group(sg, S.ngroups, t);
+    const GroupDev &G = sg[g];
     int tri = (int)(t - G.tri_base);
     int ix[3], iy[3];
     float z[3];
     project_ortho(G, tri, S.sh, S.bias, ix, iy, z);
     V2 uv[3] = {V2{0, 0}, V2{0, 0}, V2{0, 0}};
-    amask = (G.flags & F_ALPHA) ? G.amask : nullptr;
-    alen = G.alen;
-    if (amask) {
+    if (ALPHA) {
 #pragma unroll
       for (int k = 0; k < 3; k++) uv[k] = mul2(ld2(G.uv + ((size_t)tri * 3 + k) * 2), z[k]);
     }
-    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(uv[0], uv[1]); }
-    if (iy[1] > iy[2]) { swap_(iy[1], iy[2]); swap_(ix[1], ix[2]); swap_(z[1], z[2]); swap_(uv[1], uv[2]); }
-    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(uv[0], uv[1]); }
+    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); if (ALPHA) swap_(uv[0], uv[1]); }
+    if (iy[1] > iy[2]) { swap_(iy[1], iy[2]); swap_(ix[1], ix[2]); swap_(z[1], z[2]); if (ALPHA) swap_(uv[1], uv[2]); }
+    if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); if (ALPHA) swap_(uv[0], uv[1]); }
     x1 = ix[0]; x2 = ix[1]; x3 = ix[2]; y1 = iy[0]; y2 = iy[1]; y3 = iy[2];
     z1 = z[0]; z2 = z[1]; z3 = z[2];
     if (!((y1 < S.sh.dim) && (y3 >= 0))) return false;
-    u1 = uv[0].x; u2 = uv[1].x; u3 = uv[2].x; v1 = uv[0].y; v2 = uv[1].y; v3 = uv[2].y;
     float q = (float)(y2 - y1) / (float)(y3 - y1);
     x4 = f2i((float)x1 + q * (float)(x3 - x1));
     z4 = z1 + q * (z3 - z1);
-    u4 = u1 + q * (u3 - u1);
-    v4 = v1 + q * (v3 - v1);
-    start_half0();
-    if (cy > y2) {               // no bottom rows
-      start_half1();
-      return cy > y2;
+    if (ALPHA) {
+      u1 = uv[0].x; u2 = uv[1].x; u3 = uv[2].x; v1 = uv[0].y; v2 = uv[1].y; v3 = uv[2].y;
+      u4 = u1 + q * (u3 - u1);
+      v4 = v1 + q * (v3 - v1);
     }
+    start_half0();
     return true;
   }
 
-  __device__ __forceinline__ bool step(int dim, SpanS &s) {
-    s.cnt = 0;
-    s.cy = cy;
-    s.cx1 = cx1; s.cx2 = cx2; s.cz1 = cz1; s.cz2 = cz2;
-    s.cu1 = cu1; s.cv1 = cv1; s.cu2 = cu2; s.cv2 = cv2;
-    s.amask = amask;
-    s.alen = alen;
+  __device__ __forceinline__ int emit(int dim, ShadowQ<ALPHA> &q, int lane, bool &live) {
+    int cnt = 0;
     if (cy >= 0 && cy < dim) {
       int a0 = half == 0 ? f2i(cx2) : f2i(cx1);
       int a1 = half == 0 ? f2i(cx1) : f2i(cx2);
       int lo = a0 < 0 ? 0 : a0, hi = a1 > dim - 1 ? dim - 1 : a1;
-      s.lo = lo;
-      s.cnt = hi >= lo ? hi - lo + 1 : 0;
+      cnt = hi >= lo ? hi - lo + 1 : 0;
+      if (cnt) {
+        float d = cx1 - cx2;
+        q.cyw[lane] = cy * dim;
+        q.lo[lane] = lo;
+        q.cx2[lane] = cx2; q.d[lane] = d; q.rd[lane] = span_recip(d);
+        q.cz1[lane] = cz1; q.cz2[lane] = cz2;
+        if (ALPHA) { q.cu1[lane] = cu1; q.cv1[lane] = cv1; q.cu2[lane] = cu2; q.cv2[lane] = cv2; q.g[lane] = g; }
+      }
     }
     if (half == 0) {
       cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
-      cu1 += su1; cv1 += sv1; cu2 += su2; cv2 += sv2;
+      if (ALPHA) { cu1 += su1; cv1 += sv1; cu2 += su2; cv2 += sv2; }
       cy++;
-      if (cy <= y2) return true;
-      start_half1();
-      return cy > y2;
+      if (cy > y2) {
+        start_half1();
+        live = cy > y2;
+      }
+      return cnt;
     }
     cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
-    cu1 -= su1; cv1 -= sv1; cu2 -= su2; cv2 -= sv2;
+    if (ALPHA) { cu1 -= su1; cv1 -= sv1; cu2 -= su2; cv2 -= sv2; }
     cy--;
-    return cy > y2;
+    live = cy > y2;
+    return cnt;
   }
 };
 
-__device__ __forceinline__ void shadow_fragment(float *map, int dim, const SpanS &s, int ax) {
-  float t = ((float)ax - s.cx2) / (s.cx1 - s.cx2);
+// drawmin.c:71-76 / drawminalpha.c:83-97 for one pixel of span s
+template <bool ALPHA>
+__device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int ax) {
+  float t = quot_by_recip((float)ax - q.cx2[s], q.d[s], q.rd[s]);
   t = clamp_t(t);
-  float tz = 1.0f / ((1 - t) * s.cz2 + t * s.cz1);
+  float tz = 1.0f / ((1 - t) * q.cz2[s] + t * q.cz1[s]);
   if (tz != tz) return;
-  if (s.amask) {
-    int len = s.alen;
+  if (ALPHA) {
+    const GroupDev &G = sg[q.g[s]];
+    int len = G.alen;
     float lm1 = (float)(len - 1);
-    int t1 = f2i((((1 - t) * s.cu2 + t * s.cu1) * tz) * lm1);
+    int t1 = f2i((((1 - t) * q.cu2[s] + t * q.cu1[s]) * tz) * lm1);
     t1 = iabs_(t1) & (len - 1);
-    int t2 = f2i((lm1 * ((1 - t) * s.cv2 + t * s.cv1)) * tz);
+    int t2 = f2i((lm1 * ((1 - t) * q.cv2[s] + t * q.cv1[s])) * tz);
     t2 = iabs_(t2) & (len - 1);
-    if (!__ldg(s.amask + t1 + t2 * len)) return;
+    if (!__ldg(G.amask + t1 + t2 * len)) return;
   }
-  atomic_min_depth(map + (size_t)dim * s.cy + ax, tz);
+  atomic_min_depth(map + (size_t)q.cyw[s] + ax, tz);
 }
 
-__global__ void __launch_bounds__(128) k_shadow_raster(ShadowParams S) {
-  __shared__ GroupDev sg[64];
-  __shared__ SpanS q[4][32];
-  __shared__ int pre[4][33];
-  for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
-  if (threadIdx.x < 4) pre[threadIdx.x][32] = 0x7fffffff;
-  __syncthreads();
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t n = S.ctr[CTR_SH_LIST];
+template <bool ALPHA>
+__device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const GroupDev *sg, ShadowQ<ALPHA> &q, int lane,
+                                                 int ctr_list, int ctr_work) {
+  uint32_t n = S.ctr[ctr_list];
   int dim = S.sh.dim;
   while (true) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&S.ctr[CTR_SH_WORK], 32u);
+    if (lane == 0) base = atomicAdd(&S.ctr[ctr_work], 32u);
     base = __shfl_sync(FULL, base, 0);
     if (base >= n) break;
-    ShadowLane L;
+    ShadowLane<ALPHA> L;
     bool live = false;
-    if (base + lane < n) live = L.init(S, sg, S.list[base + lane]);
-    while (__any_sync(FULL, live)) {
-      SpanS s;
-      s.cnt = 0;
-      if (live) live = L.step(dim, s);
-      int c = s.cnt, incl = c;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int v = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += v;
+    if (base + lane < n) {
+      uint32_t idx = base + lane;
+      live = L.init(S, sg, S.list[ALPHA ? S.cap_list - 1 - idx : idx]);
+    }
+    for (int round = 0; __any_sync(FULL, live); round++) {
+      if (round == LOOP_LIMIT) {
+        if (lane == 0) atomicOr(&S.ctr[CTR_LIMIT], 1u);
+        break;
       }
-      int total = __shfl_sync(FULL, incl, 31);
+      int cnt = 0;
+      if (live) cnt = L.emit(dim, q, lane, live);
+      int total = warp_offsets(cnt, lane, q.pre);
       if (total == 0) continue;
-      q[w][lane] = s;
-      pre[w][lane] = incl - c;
       __syncwarp();
       for (int p = lane; p < total; p += 32) {
-        int k = 0;
-#pragma unroll
-        for (int st = 16; st; st >>= 1)
-          if (pre[w][k + st] <= p) k += st;
-        shadow_fragment(S.map, dim, q[w][k], q[w][k].lo + (p - pre[w][k]));
+        int s = span_of(q.pre, p);
+        shadow_pixel<ALPHA>(S.map, sg, q, s, q.lo[s] + (p - q.pre[s]));
       }
       __syncwarp();
     }
   }
+}
+
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_shadow_raster(ShadowParams S) {
+  __shared__ GroupDev sg[64];
+  __shared__ ShadowQ<ALPHA> qs[4];
+  for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
+  __syncthreads();
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  shadow_warp_loop<ALPHA>(S, sg, qs[w], lane, ALPHA ? CTR_SH_LIST_A : CTR_SH_LIST, ALPHA ? CTR_SH_WORK_A : CTR_SH_WORK);
 }
 
 }  // namespace axr

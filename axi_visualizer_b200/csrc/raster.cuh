@@ -21,8 +21,9 @@ constexpr unsigned FULL = 0xffffffffu;
 
 struct GroupDev {
   const float *xyz, *vn, *uv, *li;
-  const uint16_t *tr, *tg, *tb;
-  const uint8_t *amask;
+  const ushort4 *tex;     // texels as (R, G, B, 0): one 8-byte load per bilinear tap
+  const uint8_t *amask;   // alpha mask, one byte per texel (nearest-texel tests)
+  const uint8_t *aquad;   // per texel the 4 taps of its bilinear footprint as bits
   int alen;
   int ntris, tri_base, tex_size, flags;
   float mip_bias;
@@ -91,6 +92,27 @@ __device__ __forceinline__ float axr_log2f(float x) {
   }
   double r = (double)e + sum * 2.8853900817779268;
   return (float)r;
+}
+
+// Correctly rounded n/d from y = RN(1/d) (Markstein's theorem, "Computation
+// of elementary functions on the IBM RISC System/6000", IBM J. R&D 1990):
+// q = RN(n*y), r = n - d*q (exact with a fused multiply-add), RN(q + r*y) is
+// RN(n/d) when nothing overflows or underflows.  span_recip returns y, or 0
+// when d is outside [2^-60, 2^60] (zero, denormal, huge, inf, NaN) and the
+// caller must divide; quot_by_recip also divides when |n| is outside that
+// range, so every quotient equals the IEEE division bit for bit.
+__device__ __forceinline__ float span_recip(float d) {
+  float a = fabsf(d);
+  return (a >= 8.6736174e-19f && a <= 1.1529215e18f) ? __frcp_rn(d) : 0.f;
+}
+__device__ __forceinline__ float quot_by_recip(float n, float d, float y) {
+  float an = fabsf(n);
+  if (y != 0.f && an <= 1.1529215e18f && (an >= 8.6736174e-19f || n == 0.f)) {
+    float q = __fmul_rn(n, y);
+    float r = __fmaf_rn(-d, q, n);
+    return __fmaf_rn(r, y, q);
+  }
+  return n / d;
 }
 
 // ------------------------------------------------------------ order keys
@@ -320,6 +342,23 @@ __device__ __forceinline__ Taps make_taps(V2 uvi, float tz, int len, int start) 
   q.texr1 = rx; q.texr2 = ry;
   q.texi1 = 1 - rx; q.texi2 = 1 - ry;
   return q;
+}
+// bilinear R, G, B of av_draw_base.c:50-55 (same products and sums per channel)
+__device__ __forceinline__ V3 bilerp_rgb(const Taps &q, const ushort4 *__restrict__ T) {
+  ushort4 a = __ldg(T + q.tex), b = __ldg(T + q.tex10), c = __ldg(T + q.tex01), d = __ldg(T + q.tex11);
+  float w00 = q.texi1 * q.texi2, w10 = q.texr1 * q.texi2, w01 = q.texi1 * q.texr2, w11 = q.texr1 * q.texr2;
+  V3 r;
+  r.x = w00 * (float)a.x + w10 * (float)b.x + w01 * (float)c.x + w11 * (float)d.x;
+  r.y = w00 * (float)a.y + w10 * (float)b.y + w01 * (float)c.y + w11 * (float)d.y;
+  r.z = w00 * (float)a.z + w10 * (float)b.z + w01 * (float)c.z + w11 * (float)d.z;
+  return r;
+}
+// bilinear boolean alpha of av_draw_alpha.c:95-96 from the packed footprint:
+// bit 0 = tap (t1,t2), bit 1 = (t1+1,t2), bit 2 = (t1,t2+1), bit 3 = (t1+1,t2+1)
+__device__ __forceinline__ float bilerp_quad(const Taps &q, const uint8_t *__restrict__ Q) {
+  unsigned m = __ldg(Q + q.tex);
+  return q.texi1 * q.texi2 * (float)(m & 1) + q.texr1 * q.texi2 * (float)((m >> 1) & 1) +
+         q.texi1 * q.texr2 * (float)((m >> 2) & 1) + q.texr1 * q.texr2 * (float)((m >> 3) & 1);
 }
 __device__ __forceinline__ float bilerp_u16(const Taps &q, const uint16_t *__restrict__ T) {
   return q.texi1 * q.texi2 * (float)__ldg(T + q.tex) + q.texr1 * q.texi2 * (float)__ldg(T + q.tex10) +

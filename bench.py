@@ -42,6 +42,11 @@ NCU_TRAFFIC = {"k_raster_small": 34465536 + 512, "k_shadow_raster": 46918400 + 7
                "k_shade": 29610752 + 670976}
 
 
+def progress(msg):
+    """Stage marker on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def peaks():
     try:
         with open(PEAKS_FILE) as f:
@@ -258,17 +263,20 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    progress("scene")
     scene = S.scene_c2()
     view = S.default_view(W, H)
     R = SceneRenderer(scene, W, H, device=local, pinned=True)
     D = R.draw
     stream = torch.cuda.ExternalStream(D.stream_ptr(), device=f"cuda:{local}")
 
+    progress("warmup")
     for _ in range(args.warmup):
         R.frame(view)
     D.sync()
     stats = D.lastStats()
 
+    progress("timed loop")
     # ---- device-timed loop (value): scene resident in HBM
     clocks = Clocks(_smi_index(torch, local))
     barrier()
@@ -290,6 +298,7 @@ def main():
     barrier()
     fps = world * args.steps / (t_ms / 1000.0)
 
+    progress("kernel timing")
     # ---- per-kernel device times (roofline) on a second pass
     D.setKernelTiming(True)
     for _ in range(args.steps):
@@ -316,6 +325,7 @@ def main():
     frame_roof = {"bytes": fb, "achieved_gbs": fb / (t_ms / args.steps / 1000.0) / 1e9}
     frame_roof["frac"] = frame_roof["achieved_gbs"] / hbm
 
+    progress("e2e")
     # ---- end-to-end through the public API, host buffers, pinned memory
     barrier()
     pose = torch.empty(12, dtype=torch.float32, pin_memory=True).numpy()
@@ -339,6 +349,7 @@ def main():
     d2h = W * H * (3 * 2 + 4)
     h2d = 12 * 4 + 3 * 4 + 3 * len(scene.groups) * 96   # pose + scale/cull + 3 group tables per frame
 
+    progress("cpu baseline")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_oracle_baseline(scene, view)
