@@ -19,8 +19,17 @@ EXPORTS = [
     "axr_set_frame", "axr_gamma", "axr_add_shadow_map", "axr_place_shadow_map", "axr_clear_shadow_map",
     "axr_shadow_map", "axr_get_shadow_map", "axr_sync", "axr_get_stream", "axr_frame_device_ptrs",
     "axr_last_stats", "axr_launch_count", "axr_set_kernel_timing", "axr_kernel_times",
-    "axr_shadow_map_noalloc",
+    "axr_shadow_map_noalloc", "axr_batch_create", "axr_batch_set_views", "axr_batch_render",
+    "axr_batch_get_frame", "axr_batch_get_ids", "axr_batch_stats", "axr_batch_destroy",
+    "axr_batch_set_tuning", "axr_set_tuning",
 ]
+
+
+class ViewDesc(C.Structure):
+    """axr_view_desc of include/axr.h"""
+    _fields_ = [("kind", C.c_int), ("w", C.c_int), ("h", C.c_int), ("pos", C.c_float * 3), ("vm", C.c_float * 9),
+                ("scale", C.c_float), ("cax", C.c_float), ("cay", C.c_float), ("bias", C.c_float),
+                ("cascades", C.c_int * 2), ("ncascades", C.c_int)]
 
 vp = C.c_void_p
 i32 = C.c_int
@@ -60,6 +69,15 @@ _SIGS = {
     "axr_kernel_times": (i32, [vp, i32, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                C.POINTER(i32)]),
     "axr_shadow_map_noalloc": (i32, [vp, vp, vp, i32, i32, vp, vp, f32, f32, vp, i32, vp]),
+    "axr_batch_create": (i32, [vp, vp, i32, C.POINTER(vp)]),
+    "axr_batch_set_views": (i32, [vp, vp, i32]),
+    "axr_batch_render": (i32, [vp, vp, vp, vp, i32]),
+    "axr_batch_get_frame": (i32, [vp, i32, vp, vp, vp, vp]),
+    "axr_batch_get_ids": (i32, [vp, i32, vp, vp]),
+    "axr_batch_stats": (i32, [vp, C.POINTER(C.c_int64), C.POINTER(i32), C.POINTER(i32)]),
+    "axr_batch_destroy": (i32, [vp]),
+    "axr_batch_set_tuning": (i32, [vp, i32, i32]),
+    "axr_set_tuning": (i32, [vp, i32]),
 }
 
 _lib = None

@@ -18,7 +18,7 @@
 #include <vector>
 
 #include "../../include/axr.h"
-#include "kernels.cuh"
+#include "batch.cuh"
 
 using namespace axr;
 
@@ -105,6 +105,7 @@ struct axr_ctx {
   bool pending = false;
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
+  int min_chunk = MIN_CHUNK;
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
   struct Pending { const char *name; cudaEvent_t a, b; };
@@ -560,6 +561,7 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   P.small_list = c->small_list; P.large_list = c->large_list; P.items = c->items;
   P.units = c->units; P.ctr = c->ctr;
   P.cap_list = c->cap_list; P.cap_units = c->cap_units;
+  P.min_chunk = c->min_chunk;
   long npix = (long)c->w * c->h;
   cudaStream_t s = c->stream;
   int64_t nk = 0;
@@ -839,6 +841,413 @@ int axr_kernel_times(axr_ctx *c, int max, char *names, int name_len, double *tot
     k++;
   }
   if (n) *n = k;
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched multi-view rendering: one cooperative persistent launch per batch,
+// captured once in a CUDA graph together with the uploads of the camera and
+// material tables (from pinned host buffers) and the read-back of the work
+// counters; every render replays the graph.
+// ---------------------------------------------------------------------------
+
+struct axr_batch {
+  axr_ctx *c = nullptr;
+  std::vector<axr_view_desc> desc;
+  struct Buf {
+    uint16_t *ro = nullptr, *go = nullptr, *bo = nullptr;
+    float *db = nullptr, *map = nullptr;
+    uint64_t *keys = nullptr;
+    uint32_t *small = nullptr, *large = nullptr, *items = nullptr, *list = nullptr, *ctr = nullptr;
+    uint2 *units = nullptr;
+    uint32_t cap_units = 0;
+  };
+  std::vector<Buf> buf;
+  uint32_t cap_list = 0;
+  BatchView *d_views = nullptr, *h_views = nullptr;
+  GroupDev *d_gdraw = nullptr, *d_gshadow = nullptr, *h_gdraw = nullptr, *h_gshadow = nullptr;
+  uint32_t *d_bar = nullptr, *h_bar = nullptr, *h_ctrs = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;
+  bool graph = false, pending = false;
+  int grid = 0, per_sm_max = 0, min_chunk = MIN_CHUNK;
+  int64_t launches = 0;
+};
+
+namespace {
+
+void batch_free_buffers(axr_batch *b) {
+  for (auto &x : b->buf) {
+    cudaFree(x.ro); cudaFree(x.go); cudaFree(x.bo); cudaFree(x.db); cudaFree(x.map); cudaFree(x.keys);
+    cudaFree(x.small); cudaFree(x.large); cudaFree(x.items); cudaFree(x.list); cudaFree(x.ctr); cudaFree(x.units);
+  }
+  b->buf.clear();
+}
+
+int batch_check_views(axr_ctx *c, const axr_view_desc *v, int n) {
+  if (!v || n < 1 || n > 64) return fail(AXR_EINVAL, "a batch holds 1..64 views");
+  for (int k = 0; k < n; k++) {
+    if (v[k].kind == AXR_VIEW_SHADED) {
+      if (v[k].w <= 0 || v[k].h <= 0 || v[k].w % TILE || (long)v[k].w * v[k].h > (1L << 27))
+        return fail(AXR_EINVAL, "view %d: shaded views need w a positive multiple of 16", k);
+      if (v[k].ncascades < 0 || v[k].ncascades > 2) return fail(AXR_EINVAL, "view %d: at most two cascades", k);
+      for (int j = 0; j < v[k].ncascades; j++) {
+        int cv = v[k].cascades[j];
+        if (cv < 0 || cv >= n || v[cv].kind != AXR_VIEW_DEPTH)
+          return fail(AXR_EINVAL, "view %d: cascade %d is not a depth view of the batch", k, cv);
+      }
+    } else if (v[k].kind == AXR_VIEW_DEPTH) {
+      if (v[k].w < 4 || v[k].w > 16384) return fail(AXR_EINVAL, "view %d: depth map side %d", k, v[k].w);
+    } else {
+      return fail(AXR_EINVAL, "view %d: unknown kind %d", k, v[k].kind);
+    }
+  }
+  (void)c;
+  return 0;
+}
+
+int batch_alloc(axr_batch *b, uint32_t units_per_view) {
+  axr_ctx *c = b->c;
+  uint32_t cap = (uint32_t)std::max(c->total_tris, 1);
+  b->cap_list = cap;
+  b->buf.assign(b->desc.size(), axr_batch::Buf());
+  for (size_t k = 0; k < b->desc.size(); k++) {
+    const axr_view_desc &v = b->desc[k];
+    axr_batch::Buf &x = b->buf[k];
+    bool ok = cudaMalloc(&x.ctr, sizeof(uint32_t) * CTR_N) == cudaSuccess;
+    if (v.kind == AXR_VIEW_SHADED) {
+      size_t n = (size_t)v.w * v.h;
+      ok = ok && cudaMalloc(&x.ro, n * 2) == cudaSuccess && cudaMalloc(&x.go, n * 2) == cudaSuccess &&
+           cudaMalloc(&x.bo, n * 2) == cudaSuccess && cudaMalloc(&x.db, n * 4) == cudaSuccess &&
+           cudaMalloc(&x.keys, n * 8) == cudaSuccess && cudaMalloc(&x.small, 4ull * cap) == cudaSuccess &&
+           cudaMalloc(&x.large, 4ull * cap) == cudaSuccess && cudaMalloc(&x.items, 4ull * cap * MAX_CHUNKS) == cudaSuccess &&
+           cudaMalloc(&x.units, sizeof(uint2) * (size_t)units_per_view) == cudaSuccess;
+      x.cap_units = units_per_view;
+      if (ok) {
+        std::vector<uint16_t> ones(n, 1);
+        ok = cudaMemcpy(x.ro, ones.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(x.go, ones.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(x.bo, ones.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemset(x.db, 0, n * 4) == cudaSuccess;
+      }
+    } else {
+      size_t n = (size_t)v.w * v.w;
+      ok = ok && cudaMalloc(&x.map, n * 4) == cudaSuccess && cudaMalloc(&x.list, 4ull * cap) == cudaSuccess;
+      if (ok) {
+        std::vector<float> f(n, 65535.f);
+        ok = cudaMemcpy(x.map, f.data(), n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
+      }
+    }
+    if (!ok) return fail(AXR_ENOMEM, "batch view %zu buffers", k);
+  }
+  return 0;
+}
+
+// Host-side view table of the current cameras and buffers.
+void batch_fill_views(axr_batch *b) {
+  axr_ctx *c = b->c;
+  for (size_t k = 0; k < b->desc.size(); k++) {
+    const axr_view_desc &v = b->desc[k];
+    axr_batch::Buf &x = b->buf[k];
+    BatchView &V = b->h_views[k];
+    memset(&V, 0, sizeof V);
+    V.kind = v.kind;
+    V.w = v.w;
+    V.h = v.kind == AXR_VIEW_SHADED ? v.h : v.w;
+    if (v.kind == AXR_VIEW_SHADED) {
+      DrawParams &P = V.dp;
+      P.groups = b->d_gdraw; P.ngroups = (int)c->groups.size(); P.total_tris = c->total_tris;
+      P.view.w = v.w; P.view.h = v.h;
+      memcpy(P.view.pos, v.pos, sizeof v.pos); memcpy(P.view.vv, v.vm, sizeof v.vm);
+      P.view.sscale = v.scale; P.view.cax = v.cax; P.view.cay = v.cay;
+      memcpy(P.light.lint, c->lint, sizeof c->lint); memcpy(P.light.ldir, c->ldir, sizeof c->ldir);
+      P.light.amb = c->amb;
+      P.nsh = v.ncascades;
+      for (int j = 0; j < v.ncascades; j++) {
+        const axr_view_desc &sv = b->desc[v.cascades[j]];
+        P.sh[j].map = b->buf[v.cascades[j]].map; P.sh[j].dim = sv.w; P.sh[j].scale = sv.scale;
+        memcpy(P.sh[j].pos, sv.pos, sizeof sv.pos); memcpy(P.sh[j].vv, sv.vm, sizeof sv.vm);
+      }
+      P.keys = x.keys; P.ro = x.ro; P.go = x.go; P.bo = x.bo; P.db = x.db;
+      P.small_list = x.small; P.items = x.items; P.large_list = x.large; P.units = x.units; P.ctr = x.ctr;
+      P.cap_list = b->cap_list; P.cap_units = x.cap_units;
+      P.min_chunk = b->min_chunk;
+    } else {
+      ShadowParams &S = V.sp;
+      S.groups = b->d_gshadow; S.ngroups = (int)c->groups.size(); S.total_tris = c->total_tris;
+      S.sh.map = x.map; S.sh.dim = v.w; S.sh.scale = v.scale;
+      memcpy(S.sh.pos, v.pos, sizeof v.pos); memcpy(S.sh.vv, v.vm, sizeof v.vm);
+      S.map = x.map; S.bias = v.bias; S.list = x.list; S.cap_list = b->cap_list; S.ctr = x.ctr;
+    }
+  }
+}
+
+// Enqueues one batch render on the handle's stream (captured or direct).
+int batch_enqueue(axr_batch *b) {
+  axr_ctx *c = b->c;
+  cudaStream_t s = c->stream;
+  size_t nv = b->desc.size(), ng = std::max<size_t>(c->groups.size(), 1);
+  CK(cudaMemcpyAsync(b->d_views, b->h_views, sizeof(BatchView) * nv, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(b->d_gdraw, b->h_gdraw, sizeof(GroupDev) * ng, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(b->d_gshadow, b->h_gshadow, sizeof(GroupDev) * ng, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(b->d_bar, 0, sizeof(uint32_t) * 4, s));
+  BatchParams B;
+  B.views = b->d_views; B.nviews = (int)nv;
+  B.groups_draw = b->d_gdraw; B.groups_shadow = b->d_gshadow; B.ngroups = (int)c->groups.size();
+  B.bar = b->d_bar; B.nblocks = (uint32_t)b->grid;
+  void *args[] = {&B};
+  CK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(b->grid), dim3(128), args, 0, s));
+  for (size_t k = 0; k < nv; k++)
+    CK(cudaMemcpyAsync(b->h_ctrs + k * CTR_N, b->buf[k].ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(b->h_bar, b->d_bar, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, s));
+  return 0;
+}
+
+int batch_build_graph(axr_batch *b) {
+  axr_ctx *c = b->c;
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  b->graph = false;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int rc = batch_enqueue(b);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc || e != cudaSuccess || !g) {
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    return 0;   // not capturable here: render with direct launches
+  }
+  if (cudaGraphInstantiate(&b->exec, g, 0) == cudaSuccess) b->graph = true;
+  else cudaGetLastError();
+  cudaGraphDestroy(g);
+  return 0;
+}
+
+// Checks the last render's counters; grows a view's unit queue after an
+// overflow (that render was completed by the fallback path).
+int batch_settle(axr_batch *b) {
+  if (!b->pending) return 0;
+  CK(cudaEventSynchronize(b->done));
+  b->pending = false;
+  if (b->h_bar[2]) return fail(AXR_ECUDA, "batch grid barrier timed out");
+  bool rebuild = false;
+  for (size_t k = 0; k < b->desc.size(); k++) {
+    uint32_t *h = b->h_ctrs + k * CTR_N;
+    if (h[CTR_LIMIT]) return fail(AXR_ECUDA, "a raster loop of batch view %zu reached its safety limit", k);
+    if (b->desc[k].kind == AXR_VIEW_SHADED && h[CTR_OVERFLOW]) {
+      axr_batch::Buf &x = b->buf[k];
+      uint64_t need = (uint64_t)h[CTR_UNITS_RESERVED] + h[CTR_UNITS_RESERVED] / 4 + 1024;
+      if (need > 0x7fffffffull) need = 0x7fffffffull;
+      cudaFree(x.units);
+      x.units = nullptr;
+      if (cudaMalloc(&x.units, sizeof(uint2) * need) != cudaSuccess) return fail(AXR_ENOMEM, "batch unit queue");
+      x.cap_units = (uint32_t)need;
+      rebuild = true;
+    }
+  }
+  if (rebuild && b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->graph = false; }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int axr_batch_create(axr_ctx *c, const axr_view_desc *views, int nviews, axr_batch **out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return fail(AXR_EINVAL, "out is null");
+  *out = nullptr;
+  if ((rc = batch_check_views(c, views, nviews))) return rc;
+  if (c->groups.empty()) return fail(AXR_ESTATE, "add texture groups before creating a batch");
+  if ((rc = sync_all(c))) return rc;
+  axr_batch *b = new axr_batch();
+  b->c = c;
+  b->desc.assign(views, views + nviews);
+  uint32_t units0 = 1u << 20;
+  if (const char *e = getenv("AXR_UNIT_QUEUE")) {
+    long v = atol(e);
+    if (v >= 1 && v <= (1L << 30)) units0 = (uint32_t)v;
+  }
+  size_t ng = std::max<size_t>(c->groups.size(), 1);
+  bool ok = cudaMalloc(&b->d_views, sizeof(BatchView) * nviews) == cudaSuccess &&
+            cudaMallocHost(&b->h_views, sizeof(BatchView) * nviews) == cudaSuccess &&
+            cudaMalloc(&b->d_gdraw, sizeof(GroupDev) * ng) == cudaSuccess &&
+            cudaMalloc(&b->d_gshadow, sizeof(GroupDev) * ng) == cudaSuccess &&
+            cudaMallocHost(&b->h_gdraw, sizeof(GroupDev) * ng) == cudaSuccess &&
+            cudaMallocHost(&b->h_gshadow, sizeof(GroupDev) * ng) == cudaSuccess &&
+            cudaMalloc(&b->d_bar, sizeof(uint32_t) * 4) == cudaSuccess &&
+            cudaMallocHost(&b->h_bar, sizeof(uint32_t) * 4) == cudaSuccess &&
+            cudaMallocHost(&b->h_ctrs, sizeof(uint32_t) * CTR_N * nviews) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) rc = fail(AXR_ENOMEM, "batch tables");
+  if (!rc) rc = batch_alloc(b, units0);
+  if (!rc) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, 128, 0) != cudaSuccess || per_sm < 1)
+      rc = fail(AXR_ECUDA, "batch kernel occupancy");
+    b->per_sm_max = per_sm;
+    b->grid = per_sm * c->sms;
+  }
+  if (rc) {
+    axr_batch_destroy(b);
+    return rc;
+  }
+  memset(b->h_bar, 0, sizeof(uint32_t) * 4);
+  memset(b->h_ctrs, 0, sizeof(uint32_t) * CTR_N * nviews);
+  *out = b;
+  return 0;
+}
+
+int axr_batch_set_views(axr_batch *b, const axr_view_desc *views, int nviews) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  int rc = batch_check_views(b->c, views, nviews);
+  if (rc) return rc;
+  if (nviews != (int)b->desc.size()) return fail(AXR_EINVAL, "batch has %zu views", b->desc.size());
+  for (int k = 0; k < nviews; k++)
+    if (views[k].kind != b->desc[k].kind || views[k].w != b->desc[k].w ||
+        (views[k].kind == AXR_VIEW_SHADED && views[k].h != b->desc[k].h))
+      return fail(AXR_EINVAL, "view %d changes kind or size; create a new batch", k);
+  b->desc.assign(views, views + nviews);
+  return 0;
+}
+
+int axr_batch_render(axr_batch *b, const int32_t *flags, const int32_t *alpha_index, const uint8_t *cast, int ngroups) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  axr_ctx *c = b->c;
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (ngroups != (int)c->groups.size()) return fail(AXR_EINVAL, "render with %d groups, handle has %zu", ngroups,
+                                                    c->groups.size());
+  if ((uint32_t)std::max(c->total_tris, 1) > b->cap_list) return fail(AXR_ESTATE, "groups were added after the batch was created");
+  if ((rc = batch_settle(b))) return rc;       // the previous render has left the pinned tables
+  for (int g = 0; g < ngroups; g++)
+    if (flags && (flags[g] & F_SHADOW)) {
+      for (auto &v : b->desc)
+        if (v.kind == AXR_VIEW_SHADED && v.ncascades == 0)
+          return fail(AXR_ESTATE, "shadow materials in a shaded view without cascades");
+    }
+  // material tables: shaded views use every group, depth views the casters
+  if ((rc = upload_groups(c, flags, alpha_index, nullptr, false, ngroups))) return rc;
+  GroupDev tab[MAX_GROUPS];
+  CK(cudaMemcpyAsync(tab, c->d_groups, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  memcpy(b->h_gdraw, tab, sizeof(GroupDev) * ngroups);
+  for (int g = 0; g < ngroups; g++) {
+    GroupDev d = tab[g];
+    d.flags &= F_ALPHA;
+    d.enabled = cast ? (cast[g] ? 1 : 0) : 1;
+    b->h_gshadow[g] = d;
+  }
+  batch_fill_views(b);
+  if (!b->exec) {
+    if ((rc = batch_build_graph(b))) return rc;
+  }
+  if (b->exec) {
+    CK(cudaGraphLaunch(b->exec, c->stream));
+  } else {
+    if ((rc = batch_enqueue(b))) return rc;
+  }
+  b->launches++;
+  c->launches++;
+  CK(cudaEventRecord(b->done, c->stream));
+  b->pending = true;
+  return 0;
+}
+
+int axr_batch_get_frame(axr_batch *b, int view, uint16_t *r, uint16_t *g, uint16_t *bb, float *depth) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  axr_ctx *c = b->c;
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (view < 0 || view >= (int)b->desc.size()) return fail(AXR_EINVAL, "view %d", view);
+  const axr_view_desc &v = b->desc[view];
+  axr_batch::Buf &x = b->buf[view];
+  if (v.kind == AXR_VIEW_SHADED) {
+    size_t n = (size_t)v.w * v.h;
+    if (r) CK(cudaMemcpyAsync(r, x.ro, n * 2, cudaMemcpyDeviceToHost, c->stream));
+    if (g) CK(cudaMemcpyAsync(g, x.go, n * 2, cudaMemcpyDeviceToHost, c->stream));
+    if (bb) CK(cudaMemcpyAsync(bb, x.bo, n * 2, cudaMemcpyDeviceToHost, c->stream));
+    if (depth) CK(cudaMemcpyAsync(depth, x.db, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  } else if (depth) {
+    CK(cudaMemcpyAsync(depth, x.map, sizeof(float) * (size_t)v.w * v.w, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return batch_settle(b);
+}
+
+int axr_batch_get_ids(axr_batch *b, int view, int32_t *tri_id, uint8_t *cov) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  axr_ctx *c = b->c;
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (view < 0 || view >= (int)b->desc.size() || b->desc[view].kind != AXR_VIEW_SHADED)
+    return fail(AXR_EINVAL, "view %d is not a shaded view", view);
+  if ((rc = batch_settle(b))) return rc;
+  size_t n = (size_t)b->desc[view].w * b->desc[view].h;
+  int32_t *dt = nullptr;
+  uint8_t *dc = nullptr;
+  if (cudaMalloc(&dt, n * 4) != cudaSuccess || cudaMalloc(&dc, n) != cudaSuccess) {
+    cudaFree(dt);
+    return fail(AXR_ENOMEM, "id buffers");
+  }
+  k_ids<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(b->buf[view].keys, (int)n, dt, dc);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && tri_id) e = cudaMemcpyAsync(tri_id, dt, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && cov) e = cudaMemcpyAsync(cov, dc, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(dt);
+  cudaFree(dc);
+  if (e != cudaSuccess) return fail(AXR_ECUDA, "batch ids: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+int axr_batch_stats(axr_batch *b, int64_t *renders, int *graph, int *grid) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  if (renders) *renders = b->launches;
+  if (graph) *graph = b->graph ? 1 : 0;
+  if (grid) *grid = b->grid;
+  return 0;
+}
+
+int axr_batch_set_tuning(axr_batch *b, int blocks_per_sm, int min_chunk) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  if (blocks_per_sm < 1 || blocks_per_sm > b->per_sm_max)
+    return fail(AXR_EINVAL, "blocks per SM %d outside [1, %d]", blocks_per_sm, b->per_sm_max);
+  if (min_chunk < 1 || min_chunk > 256) return fail(AXR_EINVAL, "chunk rows %d outside [1, 256]", min_chunk);
+  int rc = batch_settle(b);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(b->c->stream));
+  b->grid = blocks_per_sm * b->c->sms;
+  b->min_chunk = min_chunk;
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->graph = false; }
+  return 0;
+}
+
+int axr_set_tuning(axr_ctx *c, int min_chunk) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  if (min_chunk < 1 || min_chunk > 256) return fail(AXR_EINVAL, "chunk rows %d outside [1, 256]", min_chunk);
+  c->min_chunk = min_chunk;
+  return 0;
+}
+
+int axr_batch_destroy(axr_batch *b) {
+  if (!b) return 0;
+  if (b->c) cudaStreamSynchronize(b->c->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  batch_free_buffers(b);
+  cudaFree(b->d_views); cudaFree(b->d_gdraw); cudaFree(b->d_gshadow); cudaFree(b->d_bar);
+  if (b->h_views) cudaFreeHost(b->h_views);
+  if (b->h_gdraw) cudaFreeHost(b->h_gdraw);
+  if (b->h_gshadow) cudaFreeHost(b->h_gshadow);
+  if (b->h_bar) cudaFreeHost(b->h_bar);
+  if (b->h_ctrs) cudaFreeHost(b->h_ctrs);
+  if (b->done) cudaEventDestroy(b->done);
+  delete b;
   return 0;
 }
 

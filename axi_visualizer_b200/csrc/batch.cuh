@@ -1,0 +1,165 @@
+// batch.cuh -- many views in one persistent launch (sm_100a).
+//
+// One cooperative kernel renders a batch of views of uneven size -- shaded
+// perspective views (main view, cubemap faces) and depth-only orthographic
+// views (shadow cascades) -- through five phases separated by grid barriers:
+//   0 clear depth / visibility words / counters of every view
+//   1 triangle setup of every view (perspective and orthographic)
+//   2 coarse binning, small-triangle raster and shadow-map raster
+//   3 tiled raster of the large triangles' (triangle, tile) units
+//   4 shading of every shaded view's pixels (sampling the batch's cascades)
+// Work of all views shares each phase: warps move from one view's queue to
+// the next, so small views fill the machine together with large ones.  The
+// per-phase device functions are the ones the single-view kernels use, so a
+// view rendered in a batch is bit-identical to the same view rendered alone.
+#pragma once
+#include "kernels.cuh"
+
+namespace axr {
+
+enum { VIEW_SHADED = 0, VIEW_DEPTH = 1 };
+
+struct BatchView {
+  int kind;
+  int w, h;          // framebuffer, or map side
+  DrawParams dp;     // shaded views
+  ShadowParams sp;   // depth views
+};
+
+struct BatchParams {
+  const BatchView *views;
+  int nviews;
+  const GroupDev *groups_draw, *groups_shadow;
+  int ngroups;
+  uint32_t *bar;     // [0] arrivals, [1] generation, [2] barrier error
+  uint32_t nblocks;
+};
+
+constexpr long BARRIER_SPIN_LIMIT = 1L << 26;   // ~6 s of polling, then give up
+
+// Grid-wide barrier of a cooperative launch (all blocks are co-resident).  A
+// block that polls longer than BARRIER_SPIN_LIMIT records an error and the
+// kernel ends; returns false when the batch must stop.
+__device__ __forceinline__ bool grid_sync(uint32_t *bar, uint32_t nblocks) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t *vgen = bar + 1;
+    uint32_t gen = *vgen;
+    __threadfence();
+    uint32_t arrived = atomicAdd(bar, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long it = 0;
+      while (*vgen == gen) {
+        if (++it > BARRIER_SPIN_LIMIT) {
+          atomicOr(bar + 2, 1u);
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+    ok = *(volatile uint32_t *)(bar + 2) == 0;
+  }
+  __syncthreads();
+  return ok;
+}
+
+union WarpQueue {
+  VisQ<false> vo;
+  VisQ<true> va;
+  ShadowQ<false> so;
+  ShadowQ<true> sa;
+};
+
+__global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
+  __shared__ GroupDev sgd[64], sgs[64];
+  __shared__ WarpQueue wq[4];
+  for (int i = threadIdx.x; i < B.ngroups; i += blockDim.x) {
+    sgd[i] = B.groups_draw[i];
+    sgs[i] = B.groups_shadow[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int first = blockIdx.x * blockDim.x, step = gridDim.x * blockDim.x;
+  const int tid = first + threadIdx.x;
+  const int gw = tid >> 5, nw = step >> 5;
+  WarpQueue &q = wq[w];
+
+  // phase 0: clears (clearzb.c regions) and visibility words, counters
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (tid < CTR_N) (V.kind == VIEW_SHADED ? V.dp.ctr : V.sp.ctr)[tid] = 0;
+    if (V.kind == VIEW_SHADED) {
+      int W = V.w, H = V.h, bw = (W / 4) * 4, bh = (H / 4) * 4;
+      for (int i = tid; i < W * H; i += step) {
+        int y = i / W, x = i - y * W;
+        float d = V.dp.db[i];
+        if (y < bh && x < bw) {
+          d = 65535.f;
+          V.dp.db[i] = d;
+        }
+        V.dp.keys[i] = ((uint64_t)depth_key(d) << 32) | 0xffffffffull;
+      }
+    } else {
+      int D = V.w, bd = (D / 16) * 16;
+      for (int i = tid; i < bd * bd; i += step) {
+        int y = i / bd, x = i - y * bd;
+        V.sp.map[(size_t)D * y + x] = 65535.f;
+      }
+    }
+  }
+  if (!grid_sync(B.bar, B.nblocks)) return;
+
+  // phase 1: setup of every view
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind == VIEW_SHADED) setup_phase(V.dp, sgd, first, step);
+    else shadow_setup_phase(V.sp, sgs, first, step);
+  }
+  if (!grid_sync(B.bar, B.nblocks)) return;
+
+  // phase 2: coarse units, small triangles, shadow maps
+  for (int v = 0; v < B.nviews; v++)
+    if (B.views[v].kind == VIEW_SHADED) coarse_loop(B.views[v].dp, sgd, lane);
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind != VIEW_DEPTH) continue;
+    shadow_warp_loop<false>(V.sp, sgs, q.so, lane, CTR_SH_LIST, CTR_SH_WORK);
+    shadow_warp_loop<true>(V.sp, sgs, q.sa, lane, CTR_SH_LIST_A, CTR_SH_WORK_A);
+  }
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind != VIEW_SHADED) continue;
+    raster_small_loop<true>(V.dp, sgd, q.va, lane);
+    raster_small_loop<false>(V.dp, sgd, q.vo, lane);
+  }
+  if (!grid_sync(B.bar, B.nblocks)) return;
+
+  // phase 3: large triangles, tile by tile
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind != VIEW_SHADED) continue;
+    raster_tiled_loop<true>(V.dp, sgd, q.va, lane);
+    raster_tiled_loop<false>(V.dp, sgd, q.vo, lane);
+    fallback_loop(V.dp, sgd, q.vo, q.va, lane, gw, nw);
+  }
+  if (!grid_sync(B.bar, B.nblocks)) return;
+
+  // phase 4: shading
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind != VIEW_SHADED) continue;
+    int W = V.w, n = V.w * V.h;
+    for (int i = tid; i < n; i += step) {
+      int y = i / W, x = i - y * W;
+      shade_pixel(V.dp, sgd, x, y, V.dp.keys[i]);
+    }
+  }
+}
+
+}  // namespace axr

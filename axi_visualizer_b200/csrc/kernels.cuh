@@ -41,6 +41,7 @@ struct DrawParams {
   uint2 *units;          // opaque (triangle, tile) units from the front, alpha-tested from the back
   uint32_t *ctr;         // see CTR_*
   uint32_t cap_list, cap_units;
+  int min_chunk;         // rows per small-triangle work item (at least; tuning knob)
 };
 
 enum {
@@ -81,12 +82,12 @@ __device__ __forceinline__ void span_clip(int ax0, float bound, int w, int &lo, 
 // rows, so that large "small" triangles spread over several lanes; a lane
 // replays the row accumulation up to its chunk, which keeps every
 // interpolant bit-identical to the serial walk.
-constexpr int MIN_CHUNK = 16;
+constexpr int MIN_CHUNK = 16;   // default of DrawParams::min_chunk
 constexpr int MAX_CHUNKS = 3;
 __device__ __forceinline__ int small_rows(int y1, int y3) { return y3 - y1 + 2; }
-__device__ __forceinline__ int chunk_len(int rows) {
+__device__ __forceinline__ int chunk_len(int rows, int min_chunk) {
   int c = (rows + MAX_CHUNKS - 1) / MAX_CHUNKS;
-  return c < MIN_CHUNK ? MIN_CHUNK : c;
+  return c < min_chunk ? min_chunk : c;
 }
 
 // ------------------------------------------------------------ keys / clear
@@ -146,13 +147,11 @@ __global__ void k_vert_light(const float *__restrict__ vn, float *__restrict__ l
 
 // ------------------------------------------------------------ setup
 
-// one thread per triangle of every enabled group; lists hold global ids
-__global__ void __launch_bounds__(256) k_setup(DrawParams P) {
-  __shared__ GroupDev sg[64];
-  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  __syncthreads();
+// one thread per triangle of every enabled group; lists hold global ids.
+// `first`/`step` give the block's grid-stride over the triangles.
+__device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev *sg, int first, int step) {
   int lane = threadIdx.x & 31;
-  for (int base = blockIdx.x * blockDim.x; base < P.total_tris; base += gridDim.x * blockDim.x) {
+  for (int base = first; base < P.total_tris; base += step) {
     int t = base + threadIdx.x;
     int cls = 0;
     bool alpha = false;
@@ -188,7 +187,8 @@ __global__ void __launch_bounds__(256) k_setup(DrawParams P) {
     if (cls == 1) {
       int y0 = min(iy0, min(iy1, iy2)), y3 = max(iy0, max(iy1, iy2));
       int rows = small_rows(y0, y3);
-      nch = (rows + chunk_len(rows) - 1) / chunk_len(rows);
+      int cl = chunk_len(rows, P.min_chunk);
+      nch = (rows + cl - 1) / cl;
     }
     int co = (cls == 1 && !alpha) ? nch : 0, ca = (cls == 1 && alpha) ? nch : 0;
     int io = co, ia = ca;
@@ -212,6 +212,13 @@ __global__ void __launch_bounds__(256) k_setup(DrawParams P) {
       else P.items[cap_items - 1 - (oa + c)] = item;
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_setup(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  setup_phase(P, sg, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------ span queue
@@ -356,7 +363,7 @@ struct SmallLane {
   __device__ __forceinline__ void init_chunk(const DrawParams &P, const GroupDev *sg, uint32_t t, int chunk) {
     init(P, sg, t);
     int rows = small_rows(y1, y3);
-    int cl = chunk_len(rows);
+    int cl = chunk_len(rows, P.min_chunk);
     int first = chunk * cl;
     left = min(cl, rows - first);
     for (int r = 0; r < first; r++) skip_row();
@@ -420,13 +427,7 @@ struct SmallLane {
 };
 
 template <bool ALPHA>
-__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_small(DrawParams P) {
-  __shared__ GroupDev sg[64];
-  __shared__ VisQ<ALPHA> qs[4];
-  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  __syncthreads();
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  VisQ<ALPHA> &q = qs[w];
+__device__ __forceinline__ void raster_small_loop(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane) {
   uint32_t n = P.ctr[ALPHA ? CTR_ITEMS_A : CTR_ITEMS];
   uint32_t cap_items = P.cap_list * MAX_CHUNKS;
   while (true) {
@@ -452,6 +453,15 @@ __global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_small(DrawParams 
       vis_fill<ALPHA>(P, sg, q, lane, cnt);
     }
   }
+}
+
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_small(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  __shared__ VisQ<ALPHA> qs[4];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  raster_small_loop<ALPHA>(P, sg, qs[threadIdx.x >> 5], threadIdx.x & 31);
 }
 
 // ------------------------------------------------------------ coarse binning
@@ -516,11 +526,7 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
 }
 
 // Opaque units fill the queue from the front, alpha-tested ones from the back.
-__global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
-  __shared__ GroupDev sg[64];
-  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  __syncthreads();
-  int lane = threadIdx.x & 31;
+__device__ __forceinline__ void coarse_loop(const DrawParams &P, const GroupDev *sg, int lane) {
   uint32_t n = P.ctr[CTR_LARGE];
   int wc = P.view.w / TILE, hc = P.view.h / TILE;
   while (true) {
@@ -579,6 +585,13 @@ __global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(128) k_coarse(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  coarse_loop(P, sg, threadIdx.x & 31);
 }
 
 // ------------------------------------------------------------ tiled (large) raster
@@ -726,14 +739,8 @@ struct TileLane {
 };
 
 template <bool ALPHA>
-__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_tiled(DrawParams P) {
-  __shared__ GroupDev sg[64];
-  __shared__ VisQ<ALPHA> qs[4];
-  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  __syncthreads();
+__device__ __forceinline__ void raster_tiled_loop(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane) {
   if (P.ctr[CTR_OVERFLOW]) return;
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  VisQ<ALPHA> &q = qs[w];
   uint32_t n = P.ctr[ALPHA ? CTR_UNITS_A : CTR_UNITS];
   while (true) {
     uint32_t base = 0;
@@ -758,6 +765,15 @@ __global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_tiled(DrawParams 
   }
 }
 
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_raster_tiled(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  __shared__ VisQ<ALPHA> qs[4];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  raster_tiled_loop<ALPHA>(P, sg, qs[threadIdx.x >> 5], threadIdx.x & 31);
+}
+
 // Tile-unit queue overflow: every large triangle is rasterized here instead,
 // one triangle per warp, its coarse tiles dealt round-robin to the lanes and
 // each lane filling its tiles on its own (slow, same fragments).
@@ -772,15 +788,9 @@ __device__ __forceinline__ void fallback_unit(const DrawParams &P, const GroupDe
   }
 }
 
-__global__ void __launch_bounds__(128) k_raster_tiled_fallback(DrawParams P) {
-  __shared__ GroupDev sg[64];
-  __shared__ VisQ<false> qo[4];
-  __shared__ VisQ<true> qa[4];
-  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
-  __syncthreads();
+__device__ __forceinline__ void fallback_loop(const DrawParams &P, const GroupDev *sg, VisQ<false> &qo, VisQ<true> &qa,
+                                              int lane, int gw, int nw) {
   if (!P.ctr[CTR_OVERFLOW]) return;
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   uint32_t n = P.ctr[CTR_LARGE];
   int wc = P.view.w / TILE, hc = P.view.h / TILE;
   for (uint32_t i = gw; i < n; i += nw) {
@@ -792,10 +802,21 @@ __global__ void __launch_bounds__(128) k_raster_tiled_fallback(DrawParams P) {
     int k = 0;
     coarse_walk(sx, sy, wc, hc, [&](int tile) {
       if ((k++ & 31) != lane) return;
-      if (alpha) fallback_unit<true>(P, sg, qa[w], lane, gt, tile);
-      else fallback_unit<false>(P, sg, qo[w], lane, gt, tile);
+      if (alpha) fallback_unit<true>(P, sg, qa, lane, gt, tile);
+      else fallback_unit<false>(P, sg, qo, lane, gt, tile);
     });
   }
+}
+
+__global__ void __launch_bounds__(128) k_raster_tiled_fallback(DrawParams P) {
+  __shared__ GroupDev sg[64];
+  __shared__ VisQ<false> qo[4];
+  __shared__ VisQ<true> qa[4];
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
+  __syncthreads();
+  int w = threadIdx.x >> 5;
+  fallback_loop(P, sg, qo[w], qa[w], threadIdx.x & 31, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                (gridDim.x * blockDim.x) >> 5);
 }
 
 // ------------------------------------------------------------ shade
@@ -1043,17 +1064,21 @@ __device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool
   if (ok && alpha) S.list[S.cap_list - 1 - (ba + __popc(ma & lt))] = (uint32_t)t;
 }
 
-__global__ void __launch_bounds__(256) k_shadow_setup(ShadowParams S) {
-  __shared__ GroupDev sg[64];
-  for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
-  __syncthreads();
+__device__ __forceinline__ void shadow_setup_phase(const ShadowParams &S, const GroupDev *sg, int first, int step) {
   int lane = threadIdx.x & 31;
-  for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
+  for (int base = first; base < S.total_tris; base += step) {
     int t = base + threadIdx.x;
     bool ok, alpha;
     shadow_classify(sg, S, t, ok, alpha);
     shadow_append(S, t, ok, alpha, lane);
   }
+}
+
+__global__ void __launch_bounds__(256) k_shadow_setup(ShadowParams S) {
+  __shared__ GroupDev sg[64];
+  for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
+  __syncthreads();
+  shadow_setup_phase(S, sg, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
 }
 
 __device__ __forceinline__ void atomic_min_depth(float *addr, float v) {

@@ -335,6 +335,15 @@ def scene_c1(seed=1, tex=512, terrain_n=64, spheres=200, shadow_dim=1024, flags_
     return _finish(groups, [], shadows)
 
 
+def scene_c3(seed=1):
+    """The 24,192-triangle scene of scene_c1 with two cascades (2048^2 and
+    1024^2) for the batched multi-view workload."""
+    sc = scene_c1(seed=seed)
+    sc.shadows = [ShadowCam.facing(2048, 2048 / 2 / 45.0, (0, 0, 0), SUN),
+                  ShadowCam.facing(1024, 1024 / 2 / 15.0, (0, 0, 0), SUN)]
+    return sc
+
+
 def scene_c2(seed=2, terrain_n=512, spheres=6000, nquads=20000, tex=2048, alpha_tex=1024, cascades=(2048, 2048)):
     """1080p stress scene: 512x512 terrain (524,288 tris) + 6,000 icospheres
     (480,000) + 20,000 alpha quads (40,000) = 1,044,288 triangles over 5

@@ -214,6 +214,78 @@ def reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ batched multi-view
+
+def batched_section(steps, device, log=progress):
+    """Batched multi-view frame of the 24,192-triangle scene: 6 cube faces at
+    512^2, cascades at 2048^2 and 1024^2 and the 1920x1080 main view, as one
+    graph-replayed persistent launch, against the same nine views issued as
+    plain per-view calls (two handles: 1920x1080 and 512x512, each with its
+    own cascades because the plain API keeps shadow maps per handle)."""
+    import torch
+    from axi_visualizer_b200 import autotune
+    from axi_visualizer_b200 import scenes as S
+    from axi_visualizer_b200.batch import Batch, scene_batch_views
+    from axi_visualizer_b200.ops import SceneRenderer
+
+    sc = S.scene_c3()
+    main = S.default_view(W, H)
+    eye = (0.0, 5.0, -25.0)
+    R = SceneRenderer(sc, W, H, device=device)
+    descs = scene_batch_views(sc, main, faces_at=eye, face_side=512)
+    B = Batch(R.draw, descs)
+    flags = [g.flags for g in sc.groups]
+    aidx = [g.alpha_index for g in sc.groups]
+    tuned = autotune.tune(B, flags, aidx, ntris=sc.ntris, gpu=torch.cuda.get_device_name(device), log=log)
+    stream = torch.cuda.ExternalStream(R.draw.stream_ptr(), device=f"cuda:{device}")
+    for _ in range(3):
+        B.render(flags, aidx)
+    R.draw.sync()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    ev[0].record(stream)
+    for i in range(steps):
+        B.render(flags, aidx)
+        ev[i + 1].record(stream)
+    R.draw.sync()
+    per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(steps)])
+    batch_ms = ev[0].elapsed_time(ev[-1]) / steps
+
+    # plain per-view calls
+    from axi_visualizer_b200.batch import cube_faces
+    F = SceneRenderer(sc, 512, 512, device=device)
+    faces = cube_faces(eye, 512)
+    casc = [0, 1]
+
+    def plain_frame():
+        R.frame(main)
+        F.shadow_pass()
+        for fv in faces:
+            F.set_view(fv)
+            F.draw.clearZBuffer()
+            F.draw.drawAll(F.shaders, shadowIds=casc)
+
+    for _ in range(3):
+        plain_frame()
+    R.draw.sync()
+    F.draw.sync()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        plain_frame()
+    R.draw.sync()
+    F.draw.sync()
+    plain_ms = 1000 * (time.perf_counter() - t0) / steps
+    pix = sum(d.w * (d.h if d.kind == 0 else d.w) for d in descs)
+    st = B.stats()
+    return {"workload": "c3_batched_9_views", "triangles": sc.ntris,
+            "views": [f"{'shaded' if d.kind == 0 else 'depth'} {d.w}x{d.h if d.kind == 0 else d.w}" for d in descs],
+            "frames_per_s": 1000.0 / batch_ms, "ms_per_frame": batch_ms,
+            "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+            "Mpix_per_s": pix * 1000.0 / batch_ms / 1e6,
+            "plain_frames_per_s": 1000.0 / plain_ms, "plain_ms_per_frame": plain_ms,
+            "speedup_vs_plain": plain_ms / batch_ms, "graph": st["graph"], "grid_blocks": st["grid"],
+            "tuning": {k: tuned[k] for k in ("blocks_per_sm", "min_chunk", "ms", "cached")}}
+
+
 # ------------------------------------------------------------------ GPU arm
 
 def _smi_index(torch, local):
@@ -234,6 +306,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="axr", choices=["axr", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -350,6 +423,11 @@ def main():
     h2d = 12 * 4 + 3 * 4 + 3 * len(scene.groups) * 96   # pose + scale/cull + 3 group tables per frame
 
     progress("cpu baseline")
+    batched = None
+    if not args.no_batched:
+        progress("batched multi-view")
+        batched = batched_section(min(args.steps, 100), local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_oracle_baseline(scene, view)
@@ -374,6 +452,7 @@ def main():
             "queues": stats,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(line))
     if world > 1:

@@ -166,6 +166,64 @@ int axr_launch_count(axr_ctx *ctx, int64_t *total);
 int axr_set_kernel_timing(axr_ctx *ctx, int enable);
 int axr_kernel_times(axr_ctx *ctx, int max, char *names, int name_len, double *total_ms, int64_t *launches, int *n);
 
+/* ------------------------------------------------------------------------
+ * Batched multi-view rendering (no counterpart in the reference, which draws
+ * one view per drawAll).  A batch holds views of uneven size over the
+ * handle's scene: shaded perspective views (main view, cubemap faces) and
+ * depth-only orthographic views (shadow cascades, which the shaded views of
+ * the same batch sample).  One render runs every view in one cooperative
+ * persistent kernel, replayed from a captured CUDA graph; each view's result
+ * is bit-identical to rendering it alone with drawAll/shadowMap.
+ * ------------------------------------------------------------------------ */
+#define AXR_VIEW_SHADED 0
+#define AXR_VIEW_DEPTH 1
+
+typedef struct axr_view_desc {
+  int kind;          /* AXR_VIEW_SHADED or AXR_VIEW_DEPTH */
+  int w, h;          /* shaded: framebuffer (w a multiple of 16); depth: map side w (h unused) */
+  float pos[3];      /* camera position */
+  float vm[9];       /* basis rows (view, horizontal, vertical) / Utils.viewMat rows */
+  float scale;       /* shaded: sScale; depth: orthographic scale */
+  float cax, cay;    /* shaded: cull bounds (setScaleCull) */
+  float bias;        /* depth: shBias of shadowMap */
+  int cascades[2];   /* shaded: batch indices of the depth views it samples */
+  int ncascades;
+} axr_view_desc;
+
+typedef struct axr_batch axr_batch;
+
+/* Creates a batch of views over the handle's current groups (add groups
+ * first).  Allocates the views' framebuffers, maps and work queues. */
+int axr_batch_create(axr_ctx *ctx, const axr_view_desc *views, int nviews, axr_batch **out);
+
+/* New cameras (same kinds and sizes) for the next render. */
+int axr_batch_set_views(axr_batch *b, const axr_view_desc *views, int nviews);
+
+/* Renders every view: depth views clear and draw the casters (cast[g] != 0,
+ * NULL = all), shaded views clear and draw all groups with flags[g] and
+ * alpha_index[g] (as axr_draw_all).  Asynchronous on the handle's stream. */
+int axr_batch_render(axr_batch *b, const int32_t *flags, const int32_t *alpha_index, const uint8_t *cast,
+                     int ngroups);
+
+/* Copies a view's result: colour planes + depth of a shaded view, or the
+ * depth map of a depth view (into `depth`).  Synchronises. */
+int axr_batch_get_frame(axr_batch *b, int view, uint16_t *r, uint16_t *g, uint16_t *bb, float *depth);
+
+/* Triangle id / coverage of a shaded view of the last render. */
+int axr_batch_get_ids(axr_batch *b, int view, int32_t *tri_id, uint8_t *coverage);
+
+/* Number of renders, whether renders replay a captured graph (1) or launch
+ * directly (0), and the persistent grid size in blocks. */
+int axr_batch_stats(axr_batch *b, int64_t *renders, int *graph, int *grid);
+
+/* Tuning knobs (picked by axi_visualizer_b200/autotune.py): persistent grid
+ * size in blocks per SM (1..occupancy limit) and the minimum number of rows
+ * per small-triangle work item.  Results do not depend on them. */
+int axr_batch_set_tuning(axr_batch *b, int blocks_per_sm, int min_chunk);
+int axr_set_tuning(axr_ctx *ctx, int min_chunk);
+
+int axr_batch_destroy(axr_batch *b);
+
 /* Shadow-map depth pass that allocates no device memory.  No counterpart in
  * the reference: it exists for callers that cannot call cudaMalloc/cudaFree
  * while rendering (an engine whose own allocator owns all device memory, or
