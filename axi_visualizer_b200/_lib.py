@@ -21,7 +21,8 @@ EXPORTS = [
     "axr_last_stats", "axr_launch_count", "axr_set_kernel_timing", "axr_kernel_times",
     "axr_shadow_map_noalloc", "axr_batch_create", "axr_batch_set_views", "axr_batch_render",
     "axr_batch_get_frame", "axr_batch_get_ids", "axr_batch_stats", "axr_batch_destroy",
-    "axr_batch_set_tuning", "axr_set_tuning",
+    "axr_batch_set_tuning", "axr_set_tuning", "axr_batch_query", "axr_batch_read_async", "axr_batch_bytes",
+    "axr_clear_color", "axr_batch_phase_times",
 ]
 
 
@@ -29,7 +30,8 @@ class ViewDesc(C.Structure):
     """axr_view_desc of include/axr.h"""
     _fields_ = [("kind", C.c_int), ("w", C.c_int), ("h", C.c_int), ("pos", C.c_float * 3), ("vm", C.c_float * 9),
                 ("scale", C.c_float), ("cax", C.c_float), ("cay", C.c_float), ("bias", C.c_float),
-                ("cascades", C.c_int * 2), ("ncascades", C.c_int)]
+                ("cascades", C.c_int * 2), ("ncascades", C.c_int), ("group_first", C.c_int),
+                ("group_count", C.c_int), ("clear_color", C.c_int), ("bg", C.c_int * 3)]
 
 vp = C.c_void_p
 i32 = C.c_int
@@ -78,6 +80,11 @@ _SIGS = {
     "axr_batch_destroy": (i32, [vp]),
     "axr_batch_set_tuning": (i32, [vp, i32, i32]),
     "axr_set_tuning": (i32, [vp, i32]),
+    "axr_batch_query": (i32, [vp]),
+    "axr_batch_read_async": (i32, [vp, i32, vp, vp, vp, vp]),
+    "axr_batch_bytes": (i32, [vp, C.POINTER(C.c_int64)]),
+    "axr_clear_color": (i32, [vp, i32, i32, i32]),
+    "axr_batch_phase_times": (i32, [vp, vp]),
 }
 
 _lib = None

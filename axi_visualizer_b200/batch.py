@@ -16,10 +16,19 @@ import numpy as np
 from ._lib import ViewDesc, check, lib
 from . import scenes as S
 
-SHADED, DEPTH = 0, 1
+SHADED, DEPTH, SKIP = 0, 1, 2
 
 
-def shaded(view: S.View, cascades=()):
+def _groups(d, groups):
+    if groups is not None:
+        d.group_first, d.group_count = int(groups[0]), int(groups[1])
+    return d
+
+
+def shaded(view: S.View, cascades=(), groups=None, clear=None):
+    """A shaded view sampling `cascades` (batch view indices, or -1-i for the
+    handle's shadow map i), drawing the group range groups = (first, count)
+    (None: every group); clear = (r, g, b) fills the colour planes first."""
     d = ViewDesc()
     d.kind, d.w, d.h = SHADED, view.w, view.h
     d.pos[:] = [float(x) for x in view.pos]
@@ -28,17 +37,27 @@ def shaded(view: S.View, cascades=()):
     d.ncascades = len(cascades)
     for k, c in enumerate(cascades):
         d.cascades[k] = int(c)
+    if clear is not None:
+        d.clear_color = 1
+        d.bg[:] = [int(x) for x in clear]
+    return _groups(d, groups)
+
+
+def skip(w, h):
+    """An unused shaded slot of size w x h."""
+    d = ViewDesc()
+    d.kind, d.w, d.h = SKIP, w, h
     return d
 
 
-def depth(cam: S.ShadowCam, bias: float):
+def depth(cam: S.ShadowCam, bias: float, groups=None):
     d = ViewDesc()
     d.kind, d.w, d.h = DEPTH, cam.dim, cam.dim
     d.pos[:] = [float(x) for x in cam.pos]
     d.vm[:] = [float(x) for x in np.asarray(cam.vv, np.float32).reshape(-1)]
     d.scale = cam.scale
     d.bias = float(np.float32(bias))
-    return d
+    return _groups(d, groups)
 
 
 # camera angles (alpha, beta) of the six cube faces: +x, -x, +y, -y, +z, -z
@@ -74,6 +93,12 @@ class Batch:
         arr = (ViewDesc * len(self.descs))(*self.descs)
         check(self._L.axr_batch_set_views(self._h, arr, len(self.descs)), "axr_batch_set_views")
 
+    def set_views_array(self, arr):
+        """set_views from a ctypes ViewDesc array the caller keeps and edits
+        in place (no per-call conversion)."""
+        self.descs = arr
+        check(self._L.axr_batch_set_views(self._h, arr, len(arr)), "axr_batch_set_views")
+
     def render(self, flags, alpha_index=None, cast=None):
         f = np.ascontiguousarray(np.asarray(flags, np.int32))
         a = None if alpha_index is None else np.ascontiguousarray(np.asarray(alpha_index, np.int32))
@@ -101,6 +126,34 @@ class Batch:
         c = np.empty((d.h, d.w), np.uint8)
         check(self._L.axr_batch_get_ids(self._h, k, t.ctypes.data, c.ctypes.data), "axr_batch_get_ids")
         return t, c
+
+    def read_async(self, k, r, g, b, db=None):
+        """Queue the copy of shaded view k's planes into host arrays (pinned
+        for an asynchronous copy); they hold the data once query() is True."""
+        for a in (r, g, b) + ((db,) if db is not None else ()):
+            d = self.descs[k]
+            assert a.flags.c_contiguous and a.size == d.w * d.h
+        check(self._L.axr_batch_read_async(self._h, k, r.ctypes.data, g.ctypes.data, b.ctypes.data,
+                                           None if db is None else db.ctypes.data), "axr_batch_read_async")
+
+    def query(self):
+        """True once the last render and its read-backs have finished."""
+        rc = self._L.axr_batch_query(self._h)
+        if rc < 0:
+            check(rc, "axr_batch_query")
+        return rc == 1
+
+    def phase_times(self):
+        """ms of the last render's phases: clear, setup, coarse + small
+        triangles + depth maps, tiled large triangles, shading."""
+        t = (C.c_float * 5)()
+        check(self._L.axr_batch_phase_times(self._h, t), "axr_batch_phase_times")
+        return list(t)
+
+    def bytes(self):
+        n = C.c_int64()
+        check(self._L.axr_batch_bytes(self._h, C.byref(n)), "axr_batch_bytes")
+        return n.value
 
     def set_tuning(self, blocks_per_sm, min_chunk):
         check(self._L.axr_batch_set_tuning(self._h, int(blocks_per_sm), int(min_chunk)), "axr_batch_set_tuning")

@@ -254,11 +254,10 @@ int grid_for(axr_ctx *c, long n, int block, int per_sm) {
   return (int)g;
 }
 
-// Builds the per-call group table on the device.
-int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *enabled_mask,
-                  bool mask_means_enabled, int ngroups) {
-  GroupDev tab[MAX_GROUPS];
-  memset(tab, 0, sizeof tab);
+// Builds the per-call group table (host copy).
+int group_table(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *enabled_mask,
+                bool mask_means_enabled, int ngroups, GroupDev *tab) {
+  memset(tab, 0, sizeof(GroupDev) * MAX_GROUPS);
   for (int g = 0; g < ngroups; g++) {
     const Group &G = c->groups[g];
     GroupDev &d = tab[g];
@@ -287,6 +286,15 @@ int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, 
       d.alen = c->alphas[ai].side;
     }
   }
+  return 0;
+}
+
+// Builds the per-call group table on the device.
+int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *enabled_mask,
+                  bool mask_means_enabled, int ngroups) {
+  GroupDev tab[MAX_GROUPS];
+  int rc = group_table(c, flags, alpha_index, enabled_mask, mask_means_enabled, ngroups, tab);
+  if (rc) return rc;
   CK(cudaMemcpyAsync(c->d_groups, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, c->stream));
   return 0;
 }
@@ -335,10 +343,7 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
     return rc;
   }
   // reference initial state: colour planes of ones (Ops0.py:111-113), depth cleared
-  std::vector<uint16_t> ones(n, 1);
-  cudaMemcpyAsync(c->ro, ones.data(), n * 2, cudaMemcpyHostToDevice, c->stream);
-  cudaMemcpyAsync(c->go, ones.data(), n * 2, cudaMemcpyHostToDevice, c->stream);
-  cudaMemcpyAsync(c->bo, ones.data(), n * 2, cudaMemcpyHostToDevice, c->stream);
+  k_fill_rgb<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, 1, 1, 1);
   k_clear_depth<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(c->db, w, h, 1);
   cudaMemsetAsync(c->keys, 0xff, n * 8, c->stream);
   cudaMemsetAsync(c->ctr, 0, sizeof(uint32_t) * CTR_N, c->stream);
@@ -521,6 +526,20 @@ int axr_clear_zbuffer(axr_ctx *c) {
   int rc = check_ctx(c);
   if (rc) return rc;
   launch(c, c->stream, "k_clear_depth", [&] { k_clear_depth<<<grid_for(c, (long)c->w * c->h, 256, 8), 256, 0, c->stream>>>(c->db, c->w, c->h, 4); });
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_clear_color(axr_ctx *c, int r, int g, int b) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (r < 0 || g < 0 || b < 0 || r > 65535 || g > 65535 || b > 65535)
+    return fail(AXR_EINVAL, "colour (%d, %d, %d) outside [0, 65535]", r, g, b);
+  long n = (long)c->w * c->h;
+  launch(c, c->stream, "k_fill_rgb", [&] {
+    k_fill_rgb<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, (uint16_t)r, (uint16_t)g,
+                                                                (uint16_t)b);
+  });
   CK(cudaGetLastError());
   return 0;
 }
@@ -867,13 +886,17 @@ struct axr_batch {
   std::vector<Buf> buf;
   uint32_t cap_list = 0;
   BatchView *d_views = nullptr, *h_views = nullptr;
+  // material tables: one segment per distinct group range of the views, each
+  // with tri_base counted from the range's first triangle
   GroupDev *d_gdraw = nullptr, *d_gshadow = nullptr, *h_gdraw = nullptr, *h_gshadow = nullptr;
+  std::vector<int> goff;        // per view: first entry of its segment
   uint32_t *d_bar = nullptr, *h_bar = nullptr, *h_ctrs = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaEvent_t done = nullptr;
-  bool graph = false, pending = false;
+  cudaStream_t cs = nullptr;    // read-back copies
+  cudaEvent_t done = nullptr, read_done = nullptr;
+  bool graph = false, pending = false, reads = false;
   int grid = 0, per_sm_max = 0, min_chunk = MIN_CHUNK;
-  int64_t launches = 0;
+  int64_t launches = 0, bytes = 0;
 };
 
 namespace {
@@ -889,23 +912,49 @@ void batch_free_buffers(axr_batch *b) {
 int batch_check_views(axr_ctx *c, const axr_view_desc *v, int n) {
   if (!v || n < 1 || n > 64) return fail(AXR_EINVAL, "a batch holds 1..64 views");
   for (int k = 0; k < n; k++) {
-    if (v[k].kind == AXR_VIEW_SHADED) {
+    if (v[k].kind == AXR_VIEW_SHADED || v[k].kind == AXR_VIEW_SKIP) {
       if (v[k].w <= 0 || v[k].h <= 0 || v[k].w % TILE || (long)v[k].w * v[k].h > (1L << 27))
         return fail(AXR_EINVAL, "view %d: shaded views need w a positive multiple of 16", k);
       if (v[k].ncascades < 0 || v[k].ncascades > 2) return fail(AXR_EINVAL, "view %d: at most two cascades", k);
       for (int j = 0; j < v[k].ncascades; j++) {
         int cv = v[k].cascades[j];
-        if (cv < 0 || cv >= n || v[cv].kind != AXR_VIEW_DEPTH)
+        if (cv < 0) {
+          int m = -1 - cv;   // a shadow map of the handle (addShadowMap / shadowMap)
+          if (m >= MAX_SHADOWS || !c->shadows[m].map)
+            return fail(AXR_EINVAL, "view %d: handle shadow map %d does not exist", k, m);
+        } else if (cv >= n || v[cv].kind != AXR_VIEW_DEPTH) {
           return fail(AXR_EINVAL, "view %d: cascade %d is not a depth view of the batch", k, cv);
+        }
       }
     } else if (v[k].kind == AXR_VIEW_DEPTH) {
       if (v[k].w < 4 || v[k].w > 16384) return fail(AXR_EINVAL, "view %d: depth map side %d", k, v[k].w);
     } else {
       return fail(AXR_EINVAL, "view %d: unknown kind %d", k, v[k].kind);
     }
+    for (int j = 0; j < 3; j++)
+      if (v[k].clear_color && (v[k].bg[j] < 0 || v[k].bg[j] > 65535))
+        return fail(AXR_EINVAL, "view %d: background colour outside [0, 65535]", k);
+    int ng = (int)c->groups.size();
+    if (v[k].group_count < 0 || v[k].group_first < 0 ||
+        (v[k].group_count > 0 && v[k].group_first + v[k].group_count > ng) ||
+        (v[k].group_count == 0 && v[k].group_first != 0))
+      return fail(AXR_EINVAL, "view %d: group range [%d, +%d) outside the handle's %d groups", k, v[k].group_first,
+                  v[k].group_count, ng);
   }
-  (void)c;
   return 0;
+}
+
+// The group range [first, first + count) a view draws.
+void view_range(const axr_ctx *c, const axr_view_desc &v, int &first, int &count) {
+  first = v.group_count > 0 ? v.group_first : 0;
+  count = v.group_count > 0 ? v.group_count : (int)c->groups.size();
+}
+
+template <class T>
+bool dalloc(T **p, size_t n, int64_t &bytes) {
+  if (cudaMalloc(p, n) != cudaSuccess) return false;
+  bytes += (int64_t)n;
+  return true;
 }
 
 int batch_alloc(axr_batch *b, uint32_t units_per_view) {
@@ -913,31 +962,28 @@ int batch_alloc(axr_batch *b, uint32_t units_per_view) {
   uint32_t cap = (uint32_t)std::max(c->total_tris, 1);
   b->cap_list = cap;
   b->buf.assign(b->desc.size(), axr_batch::Buf());
+  int64_t &B = b->bytes;
   for (size_t k = 0; k < b->desc.size(); k++) {
     const axr_view_desc &v = b->desc[k];
     axr_batch::Buf &x = b->buf[k];
-    bool ok = cudaMalloc(&x.ctr, sizeof(uint32_t) * CTR_N) == cudaSuccess;
-    if (v.kind == AXR_VIEW_SHADED) {
+    bool ok = dalloc(&x.ctr, sizeof(uint32_t) * CTR_N, B);
+    if (v.kind == AXR_VIEW_SHADED || v.kind == AXR_VIEW_SKIP) {
       size_t n = (size_t)v.w * v.h;
-      ok = ok && cudaMalloc(&x.ro, n * 2) == cudaSuccess && cudaMalloc(&x.go, n * 2) == cudaSuccess &&
-           cudaMalloc(&x.bo, n * 2) == cudaSuccess && cudaMalloc(&x.db, n * 4) == cudaSuccess &&
-           cudaMalloc(&x.keys, n * 8) == cudaSuccess && cudaMalloc(&x.small, 4ull * cap) == cudaSuccess &&
-           cudaMalloc(&x.large, 4ull * cap) == cudaSuccess && cudaMalloc(&x.items, 4ull * cap * MAX_CHUNKS) == cudaSuccess &&
-           cudaMalloc(&x.units, sizeof(uint2) * (size_t)units_per_view) == cudaSuccess;
+      ok = ok && dalloc(&x.ro, n * 2, B) && dalloc(&x.go, n * 2, B) && dalloc(&x.bo, n * 2, B) &&
+           dalloc(&x.db, n * 4, B) && dalloc(&x.keys, n * 8, B) && dalloc(&x.small, 4ull * cap, B) &&
+           dalloc(&x.large, 4ull * cap, B) && dalloc(&x.items, 4ull * cap * MAX_CHUNKS, B) &&
+           dalloc(&x.units, sizeof(uint2) * (size_t)units_per_view, B);
       x.cap_units = units_per_view;
-      if (ok) {
-        std::vector<uint16_t> ones(n, 1);
-        ok = cudaMemcpy(x.ro, ones.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(x.go, ones.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(x.bo, ones.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemset(x.db, 0, n * 4) == cudaSuccess;
+      if (ok) {   // a new frame buffer: colour planes of ones (Ops0.py:111-113), depth 0
+        k_fill_rgb<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(x.ro, x.go, x.bo, (int)n, 1, 1, 1);
+        ok = cudaGetLastError() == cudaSuccess && cudaMemsetAsync(x.db, 0, n * 4, c->stream) == cudaSuccess;
       }
     } else {
       size_t n = (size_t)v.w * v.w;
-      ok = ok && cudaMalloc(&x.map, n * 4) == cudaSuccess && cudaMalloc(&x.list, 4ull * cap) == cudaSuccess;
+      ok = ok && dalloc(&x.map, n * 4, B) && dalloc(&x.list, 4ull * cap, B);
       if (ok) {
-        std::vector<float> f(n, 65535.f);
-        ok = cudaMemcpy(x.map, f.data(), n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
+        k_clear_depth<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(x.map, v.w, v.w, 1);
+        ok = cudaGetLastError() == cudaSuccess;
       }
     }
     if (!ok) return fail(AXR_ENOMEM, "batch view %zu buffers", k);
@@ -955,10 +1001,17 @@ void batch_fill_views(axr_batch *b) {
     memset(&V, 0, sizeof V);
     V.kind = v.kind;
     V.w = v.w;
-    V.h = v.kind == AXR_VIEW_SHADED ? v.h : v.w;
-    if (v.kind == AXR_VIEW_SHADED) {
+    V.h = v.kind == AXR_VIEW_DEPTH ? v.w : v.h;
+    int gf, gn;
+    view_range(c, v, gf, gn);
+    int tris = 0;
+    for (int g = gf; g < gf + gn; g++) tris += c->groups[g].ntris;
+    V.goff = b->goff[k];
+    V.clear_rgb = v.kind == AXR_VIEW_SHADED && v.clear_color;
+    for (int j = 0; j < 3; j++) V.bg[j] = (uint16_t)v.bg[j];
+    if (v.kind == AXR_VIEW_SHADED || v.kind == AXR_VIEW_SKIP) {
       DrawParams &P = V.dp;
-      P.groups = b->d_gdraw; P.ngroups = (int)c->groups.size(); P.total_tris = c->total_tris;
+      P.groups = b->d_gdraw + V.goff; P.ngroups = gn; P.total_tris = tris;
       P.view.w = v.w; P.view.h = v.h;
       memcpy(P.view.pos, v.pos, sizeof v.pos); memcpy(P.view.vv, v.vm, sizeof v.vm);
       P.view.sscale = v.scale; P.view.cax = v.cax; P.view.cay = v.cay;
@@ -966,9 +1019,16 @@ void batch_fill_views(axr_batch *b) {
       P.light.amb = c->amb;
       P.nsh = v.ncascades;
       for (int j = 0; j < v.ncascades; j++) {
-        const axr_view_desc &sv = b->desc[v.cascades[j]];
-        P.sh[j].map = b->buf[v.cascades[j]].map; P.sh[j].dim = sv.w; P.sh[j].scale = sv.scale;
-        memcpy(P.sh[j].pos, sv.pos, sizeof sv.pos); memcpy(P.sh[j].vv, sv.vm, sizeof sv.vm);
+        int cv = v.cascades[j];
+        if (cv < 0) {
+          const Shadow &hm = c->shadows[-1 - cv];
+          P.sh[j].map = hm.map; P.sh[j].dim = hm.dim; P.sh[j].scale = hm.scale;
+          memcpy(P.sh[j].pos, hm.pos, sizeof hm.pos); memcpy(P.sh[j].vv, hm.vv, sizeof hm.vv);
+        } else {
+          const axr_view_desc &sv = b->desc[cv];
+          P.sh[j].map = b->buf[cv].map; P.sh[j].dim = sv.w; P.sh[j].scale = sv.scale;
+          memcpy(P.sh[j].pos, sv.pos, sizeof sv.pos); memcpy(P.sh[j].vv, sv.vm, sizeof sv.vm);
+        }
       }
       P.keys = x.keys; P.ro = x.ro; P.go = x.go; P.bo = x.bo; P.db = x.db;
       P.small_list = x.small; P.items = x.items; P.large_list = x.large; P.units = x.units; P.ctr = x.ctr;
@@ -976,7 +1036,7 @@ void batch_fill_views(axr_batch *b) {
       P.min_chunk = b->min_chunk;
     } else {
       ShadowParams &S = V.sp;
-      S.groups = b->d_gshadow; S.ngroups = (int)c->groups.size(); S.total_tris = c->total_tris;
+      S.groups = b->d_gshadow + V.goff; S.ngroups = gn; S.total_tris = tris;
       S.sh.map = x.map; S.sh.dim = v.w; S.sh.scale = v.scale;
       memcpy(S.sh.pos, v.pos, sizeof v.pos); memcpy(S.sh.vv, v.vm, sizeof v.vm);
       S.map = x.map; S.bias = v.bias; S.list = x.list; S.cap_list = b->cap_list; S.ctr = x.ctr;
@@ -988,20 +1048,20 @@ void batch_fill_views(axr_batch *b) {
 int batch_enqueue(axr_batch *b) {
   axr_ctx *c = b->c;
   cudaStream_t s = c->stream;
-  size_t nv = b->desc.size(), ng = std::max<size_t>(c->groups.size(), 1);
+  size_t nv = b->desc.size(), ng = BATCH_TABLE;
   CK(cudaMemcpyAsync(b->d_views, b->h_views, sizeof(BatchView) * nv, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(b->d_gdraw, b->h_gdraw, sizeof(GroupDev) * ng, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(b->d_gshadow, b->h_gshadow, sizeof(GroupDev) * ng, cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(b->d_bar, 0, sizeof(uint32_t) * 4, s));
+  CK(cudaMemsetAsync(b->d_bar, 0, sizeof(uint32_t) * BAR_WORDS, s));
   BatchParams B;
   B.views = b->d_views; B.nviews = (int)nv;
-  B.groups_draw = b->d_gdraw; B.groups_shadow = b->d_gshadow; B.ngroups = (int)c->groups.size();
+  B.groups_draw = b->d_gdraw; B.groups_shadow = b->d_gshadow; B.ngroups = BATCH_TABLE;
   B.bar = b->d_bar; B.nblocks = (uint32_t)b->grid;
   void *args[] = {&B};
   CK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(b->grid), dim3(128), args, 0, s));
   for (size_t k = 0; k < nv; k++)
     CK(cudaMemcpyAsync(b->h_ctrs + k * CTR_N, b->buf[k].ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(b->h_bar, b->d_bar, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(b->h_bar, b->d_bar, sizeof(uint32_t) * BAR_WORDS, cudaMemcpyDeviceToHost, s));
   return 0;
 }
 
@@ -1044,7 +1104,9 @@ int batch_settle(axr_batch *b) {
       if (need > 0x7fffffffull) need = 0x7fffffffull;
       cudaFree(x.units);
       x.units = nullptr;
-      if (cudaMalloc(&x.units, sizeof(uint2) * need) != cudaSuccess) return fail(AXR_ENOMEM, "batch unit queue");
+      b->bytes -= (int64_t)sizeof(uint2) * x.cap_units;
+      x.cap_units = 0;
+      if (!dalloc(&x.units, sizeof(uint2) * need, b->bytes)) return fail(AXR_ENOMEM, "batch unit queue");
       x.cap_units = (uint32_t)need;
       rebuild = true;
     }
@@ -1073,18 +1135,22 @@ int axr_batch_create(axr_ctx *c, const axr_view_desc *views, int nviews, axr_bat
     long v = atol(e);
     if (v >= 1 && v <= (1L << 30)) units0 = (uint32_t)v;
   }
-  size_t ng = std::max<size_t>(c->groups.size(), 1);
+  size_t ng = BATCH_TABLE;
+  b->goff.assign(nviews, 0);
   bool ok = cudaMalloc(&b->d_views, sizeof(BatchView) * nviews) == cudaSuccess &&
             cudaMallocHost(&b->h_views, sizeof(BatchView) * nviews) == cudaSuccess &&
             cudaMalloc(&b->d_gdraw, sizeof(GroupDev) * ng) == cudaSuccess &&
             cudaMalloc(&b->d_gshadow, sizeof(GroupDev) * ng) == cudaSuccess &&
             cudaMallocHost(&b->h_gdraw, sizeof(GroupDev) * ng) == cudaSuccess &&
             cudaMallocHost(&b->h_gshadow, sizeof(GroupDev) * ng) == cudaSuccess &&
-            cudaMalloc(&b->d_bar, sizeof(uint32_t) * 4) == cudaSuccess &&
-            cudaMallocHost(&b->h_bar, sizeof(uint32_t) * 4) == cudaSuccess &&
+            cudaMalloc(&b->d_bar, sizeof(uint32_t) * BAR_WORDS) == cudaSuccess &&
+            cudaMallocHost(&b->h_bar, sizeof(uint32_t) * BAR_WORDS) == cudaSuccess &&
             cudaMallocHost(&b->h_ctrs, sizeof(uint32_t) * CTR_N * nviews) == cudaSuccess &&
-            cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+            cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->read_done, cudaEventDisableTiming) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) == cudaSuccess;
   if (!ok) rc = fail(AXR_ENOMEM, "batch tables");
+  b->bytes += (int64_t)(sizeof(BatchView) * nviews + 2 * sizeof(GroupDev) * ng + sizeof(uint32_t) * BAR_WORDS);
   if (!rc) rc = batch_alloc(b, units0);
   if (!rc) {
     int per_sm = 0;
@@ -1097,7 +1163,7 @@ int axr_batch_create(axr_ctx *c, const axr_view_desc *views, int nviews, axr_bat
     axr_batch_destroy(b);
     return rc;
   }
-  memset(b->h_bar, 0, sizeof(uint32_t) * 4);
+  memset(b->h_bar, 0, sizeof(uint32_t) * BAR_WORDS);
   memset(b->h_ctrs, 0, sizeof(uint32_t) * CTR_N * nviews);
   *out = b;
   return 0;
@@ -1108,10 +1174,11 @@ int axr_batch_set_views(axr_batch *b, const axr_view_desc *views, int nviews) {
   int rc = batch_check_views(b->c, views, nviews);
   if (rc) return rc;
   if (nviews != (int)b->desc.size()) return fail(AXR_EINVAL, "batch has %zu views", b->desc.size());
-  for (int k = 0; k < nviews; k++)
-    if (views[k].kind != b->desc[k].kind || views[k].w != b->desc[k].w ||
-        (views[k].kind == AXR_VIEW_SHADED && views[k].h != b->desc[k].h))
+  for (int k = 0; k < nviews; k++) {
+    bool was_depth = b->desc[k].kind == AXR_VIEW_DEPTH, is_depth = views[k].kind == AXR_VIEW_DEPTH;
+    if (was_depth != is_depth || views[k].w != b->desc[k].w || (!is_depth && views[k].h != b->desc[k].h))
       return fail(AXR_EINVAL, "view %d changes kind or size; create a new batch", k);
+  }
   b->desc.assign(views, views + nviews);
   return 0;
 }
@@ -1125,25 +1192,54 @@ int axr_batch_render(axr_batch *b, const int32_t *flags, const int32_t *alpha_in
                                                     c->groups.size());
   if ((uint32_t)std::max(c->total_tris, 1) > b->cap_list) return fail(AXR_ESTATE, "groups were added after the batch was created");
   if ((rc = batch_settle(b))) return rc;       // the previous render has left the pinned tables
-  for (int g = 0; g < ngroups; g++)
-    if (flags && (flags[g] & F_SHADOW)) {
-      for (auto &v : b->desc)
-        if (v.kind == AXR_VIEW_SHADED && v.ncascades == 0)
-          return fail(AXR_ESTATE, "shadow materials in a shaded view without cascades");
-    }
-  // material tables: shaded views use every group, depth views the casters
-  if ((rc = upload_groups(c, flags, alpha_index, nullptr, false, ngroups))) return rc;
+  for (auto &v : b->desc) {
+    if (v.kind != AXR_VIEW_SHADED || v.ncascades > 0 || !flags) continue;
+    int gf, gn;
+    view_range(c, v, gf, gn);
+    for (int g = gf; g < gf + gn; g++)
+      if (flags[g] & F_SHADOW) return fail(AXR_ESTATE, "shadow materials in a shaded view without cascades");
+  }
+  // material tables: shaded views use their range's groups, depth views the
+  // casters of their range; one segment per distinct range, rebased so that
+  // triangle ids count from the range's first triangle
   GroupDev tab[MAX_GROUPS];
-  CK(cudaMemcpyAsync(tab, c->d_groups, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  memcpy(b->h_gdraw, tab, sizeof(GroupDev) * ngroups);
-  for (int g = 0; g < ngroups; g++) {
-    GroupDev d = tab[g];
-    d.flags &= F_ALPHA;
-    d.enabled = cast ? (cast[g] ? 1 : 0) : 1;
-    b->h_gshadow[g] = d;
+  if ((rc = group_table(c, flags, alpha_index, nullptr, false, ngroups, tab))) return rc;
+  memset(b->h_gdraw, 0, sizeof(GroupDev) * BATCH_TABLE);
+  memset(b->h_gshadow, 0, sizeof(GroupDev) * BATCH_TABLE);
+  std::vector<std::pair<int, int>> segs;
+  std::vector<int> seg_off;
+  int used = 0;
+  for (size_t k = 0; k < b->desc.size(); k++) {
+    int gf, gn;
+    view_range(c, b->desc[k], gf, gn);
+    size_t j = 0;
+    while (j < segs.size() && segs[j] != std::make_pair(gf, gn)) j++;
+    if (j == segs.size()) {
+      if (used + gn > BATCH_TABLE)
+        return fail(AXR_EINVAL, "the batch's views use more than %d group-table entries", BATCH_TABLE);
+      segs.push_back({gf, gn});
+      seg_off.push_back(used);
+      int base = c->groups[gf].tri_base;
+      for (int g = 0; g < gn; g++) {
+        GroupDev d = tab[gf + g];
+        d.tri_base -= base;
+        b->h_gdraw[used + g] = d;
+        d.flags &= F_ALPHA;
+        d.enabled = cast ? (cast[gf + g] ? 1 : 0) : 1;
+        b->h_gshadow[used + g] = d;
+      }
+      used += gn;
+    }
+    b->goff[k] = seg_off[j];
   }
   batch_fill_views(b);
+  // shaded views sampling the handle's own shadow maps wait for their writers
+  for (auto &v : b->desc)
+    for (int j = 0; j < v.ncascades; j++)
+      if (v.cascades[j] < 0) CK(cudaStreamWaitEvent(c->stream, c->shadows[-1 - v.cascades[j]].ev_write, 0));
+  // the framebuffers are free once the last render's read-back has left them
+  if (b->reads) CK(cudaStreamWaitEvent(c->stream, b->read_done, 0));
+  b->reads = false;
   if (!b->exec) {
     if ((rc = batch_build_graph(b))) return rc;
   }
@@ -1167,7 +1263,7 @@ int axr_batch_get_frame(axr_batch *b, int view, uint16_t *r, uint16_t *g, uint16
   if (view < 0 || view >= (int)b->desc.size()) return fail(AXR_EINVAL, "view %d", view);
   const axr_view_desc &v = b->desc[view];
   axr_batch::Buf &x = b->buf[view];
-  if (v.kind == AXR_VIEW_SHADED) {
+  if (v.kind != AXR_VIEW_DEPTH) {
     size_t n = (size_t)v.w * v.h;
     if (r) CK(cudaMemcpyAsync(r, x.ro, n * 2, cudaMemcpyDeviceToHost, c->stream));
     if (g) CK(cudaMemcpyAsync(g, x.go, n * 2, cudaMemcpyDeviceToHost, c->stream));
@@ -1206,6 +1302,56 @@ int axr_batch_get_ids(axr_batch *b, int view, int32_t *tri_id, uint8_t *cov) {
   return 0;
 }
 
+int axr_batch_read_async(axr_batch *b, int view, uint16_t *r, uint16_t *g, uint16_t *bb, float *depth) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  int rc = check_ctx(b->c);
+  if (rc) return rc;
+  if (view < 0 || view >= (int)b->desc.size() || b->desc[view].kind != AXR_VIEW_SHADED)
+    return fail(AXR_EINVAL, "view %d is not a shaded view of the last render", view);
+  const axr_view_desc &v = b->desc[view];
+  axr_batch::Buf &x = b->buf[view];
+  size_t n = (size_t)v.w * v.h;
+  CK(cudaStreamWaitEvent(b->cs, b->done, 0));
+  if (r) CK(cudaMemcpyAsync(r, x.ro, n * 2, cudaMemcpyDeviceToHost, b->cs));
+  if (g) CK(cudaMemcpyAsync(g, x.go, n * 2, cudaMemcpyDeviceToHost, b->cs));
+  if (bb) CK(cudaMemcpyAsync(bb, x.bo, n * 2, cudaMemcpyDeviceToHost, b->cs));
+  if (depth) CK(cudaMemcpyAsync(depth, x.db, n * 4, cudaMemcpyDeviceToHost, b->cs));
+  CK(cudaEventRecord(b->read_done, b->cs));
+  b->reads = true;
+  return 0;
+}
+
+int axr_batch_query(axr_batch *b) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  if (b->pending) {
+    cudaError_t e = cudaEventQuery(b->done);
+    if (e == cudaErrorNotReady) return 0;
+    if (e != cudaSuccess) return fail(AXR_ECUDA, "batch query: %s", cudaGetErrorString(e));
+  }
+  if (b->reads) {
+    cudaError_t e = cudaEventQuery(b->read_done);
+    if (e == cudaErrorNotReady) return 0;
+    if (e != cudaSuccess) return fail(AXR_ECUDA, "batch read-back: %s", cudaGetErrorString(e));
+  }
+  int rc = batch_settle(b);
+  return rc ? rc : 1;
+}
+
+int axr_batch_phase_times(axr_batch *b, float ms[5]) {
+  if (!b || !ms) return fail(AXR_EINVAL, "null batch or output");
+  int rc = batch_settle(b);
+  if (rc) return rc;
+  const uint64_t *t = reinterpret_cast<const uint64_t *>(b->h_bar + 4);
+  for (int k = 0; k < 5; k++) ms[k] = t[k + 1] >= t[k] ? (float)((t[k + 1] - t[k]) * 1e-6) : 0.f;
+  return 0;
+}
+
+int axr_batch_bytes(axr_batch *b, int64_t *bytes) {
+  if (!b || !bytes) return fail(AXR_EINVAL, "null batch or output");
+  *bytes = b->bytes;
+  return 0;
+}
+
 int axr_batch_stats(axr_batch *b, int64_t *renders, int *graph, int *grid) {
   if (!b) return fail(AXR_EINVAL, "null batch");
   if (renders) *renders = b->launches;
@@ -1238,6 +1384,8 @@ int axr_set_tuning(axr_ctx *c, int min_chunk) {
 int axr_batch_destroy(axr_batch *b) {
   if (!b) return 0;
   if (b->c) cudaStreamSynchronize(b->c->stream);
+  if (b->cs) { cudaStreamSynchronize(b->cs); cudaStreamDestroy(b->cs); }
+  if (b->read_done) cudaEventDestroy(b->read_done);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   batch_free_buffers(b);
   cudaFree(b->d_views); cudaFree(b->d_gdraw); cudaFree(b->d_gshadow); cudaFree(b->d_bar);

@@ -3,7 +3,7 @@
 // One cooperative kernel renders a batch of views of uneven size -- shaded
 // perspective views (main view, cubemap faces) and depth-only orthographic
 // views (shadow cascades) -- through five phases separated by grid barriers:
-//   0 clear depth / visibility words / counters of every view
+//   0 clear depth / visibility words / counters (and colour, where asked) of every view
 //   1 triangle setup of every view (perspective and orthographic)
 //   2 coarse binning, small-triangle raster and shadow-map raster
 //   3 tiled raster of the large triangles' (triangle, tile) units
@@ -17,11 +17,16 @@
 
 namespace axr {
 
-enum { VIEW_SHADED = 0, VIEW_DEPTH = 1 };
+enum { VIEW_SHADED = 0, VIEW_DEPTH = 1, VIEW_SKIP = 2 };
+
+constexpr int BATCH_TABLE = 64;   // group-table entries staged in shared memory
 
 struct BatchView {
   int kind;
   int w, h;          // framebuffer, or map side
+  int goff;          // first entry of the view's segment of the group tables
+  int clear_rgb;     // shaded: colour planes := bg before drawing
+  uint16_t bg[4];
   DrawParams dp;     // shaded views
   ShadowParams sp;   // depth views
 };
@@ -31,9 +36,20 @@ struct BatchParams {
   int nviews;
   const GroupDev *groups_draw, *groups_shadow;
   int ngroups;
-  uint32_t *bar;     // [0] arrivals, [1] generation, [2] barrier error
+  uint32_t *bar;     // [0] arrivals, [1] generation, [2] barrier error, [3] blocks done,
+                     // [4..15] six u64 globaltimer stamps: start, after phases 0-3, end
   uint32_t nblocks;
 };
+
+constexpr int BAR_WORDS = 16;
+
+__device__ __forceinline__ void stamp(uint32_t *bar, int k) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    reinterpret_cast<uint64_t *>(bar + 4)[k] = t;
+  }
+}
 
 constexpr long BARRIER_SPIN_LIMIT = 1L << 26;   // ~6 s of polling, then give up
 
@@ -77,13 +93,14 @@ union WarpQueue {
 };
 
 __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
-  __shared__ GroupDev sgd[64], sgs[64];
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
   __shared__ WarpQueue wq[4];
   for (int i = threadIdx.x; i < B.ngroups; i += blockDim.x) {
     sgd[i] = B.groups_draw[i];
     sgs[i] = B.groups_shadow[i];
   }
   __syncthreads();
+  stamp(B.bar, 0);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int first = blockIdx.x * blockDim.x, step = gridDim.x * blockDim.x;
   const int tid = first + threadIdx.x;
@@ -93,6 +110,7 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   // phase 0: clears (clearzb.c regions) and visibility words, counters
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
+    if (V.kind == VIEW_SKIP) continue;
     if (tid < CTR_N) (V.kind == VIEW_SHADED ? V.dp.ctr : V.sp.ctr)[tid] = 0;
     if (V.kind == VIEW_SHADED) {
       int W = V.w, H = V.h, bw = (W / 4) * 4, bh = (H / 4) * 4;
@@ -102,8 +120,16 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
         if (y < bh && x < bw) {
           d = 65535.f;
           V.dp.db[i] = d;
+        } else if (V.clear_rgb) {
+          d = 0.f;              // outside the clearzb.c region: the value of a new frame buffer
+          V.dp.db[i] = d;
         }
         V.dp.keys[i] = ((uint64_t)depth_key(d) << 32) | 0xffffffffull;
+        if (V.clear_rgb) {
+          V.dp.ro[i] = V.bg[0];
+          V.dp.go[i] = V.bg[1];
+          V.dp.bo[i] = V.bg[2];
+        }
       }
     } else {
       int D = V.w, bd = (D / 16) * 16;
@@ -114,41 +140,45 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
     }
   }
   if (!grid_sync(B.bar, B.nblocks)) return;
+  stamp(B.bar, 1);
 
   // phase 1: setup of every view
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
-    if (V.kind == VIEW_SHADED) setup_phase(V.dp, sgd, first, step);
-    else shadow_setup_phase(V.sp, sgs, first, step);
+    if (V.kind == VIEW_SHADED) setup_phase(V.dp, sgd + V.goff, first, step);
+    else if (V.kind == VIEW_DEPTH) shadow_setup_phase(V.sp, sgs + V.goff, first, step);
   }
   if (!grid_sync(B.bar, B.nblocks)) return;
+  stamp(B.bar, 2);
 
   // phase 2: coarse units, small triangles, shadow maps
   for (int v = 0; v < B.nviews; v++)
-    if (B.views[v].kind == VIEW_SHADED) coarse_loop(B.views[v].dp, sgd, lane);
+    if (B.views[v].kind == VIEW_SHADED) coarse_loop(B.views[v].dp, sgd + B.views[v].goff, lane);
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind != VIEW_DEPTH) continue;
-    shadow_warp_loop<false>(V.sp, sgs, q.so, lane, CTR_SH_LIST, CTR_SH_WORK);
-    shadow_warp_loop<true>(V.sp, sgs, q.sa, lane, CTR_SH_LIST_A, CTR_SH_WORK_A);
+    shadow_warp_loop<false>(V.sp, sgs + V.goff, q.so, lane, CTR_SH_LIST, CTR_SH_WORK);
+    shadow_warp_loop<true>(V.sp, sgs + V.goff, q.sa, lane, CTR_SH_LIST_A, CTR_SH_WORK_A);
   }
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind != VIEW_SHADED) continue;
-    raster_small_loop<true>(V.dp, sgd, q.va, lane);
-    raster_small_loop<false>(V.dp, sgd, q.vo, lane);
+    raster_small_loop<true>(V.dp, sgd + V.goff, q.va, lane);
+    raster_small_loop<false>(V.dp, sgd + V.goff, q.vo, lane);
   }
   if (!grid_sync(B.bar, B.nblocks)) return;
+  stamp(B.bar, 3);
 
   // phase 3: large triangles, tile by tile
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind != VIEW_SHADED) continue;
-    raster_tiled_loop<true>(V.dp, sgd, q.va, lane);
-    raster_tiled_loop<false>(V.dp, sgd, q.vo, lane);
-    fallback_loop(V.dp, sgd, q.vo, q.va, lane, gw, nw);
+    raster_tiled_loop<true>(V.dp, sgd + V.goff, q.va, lane);
+    raster_tiled_loop<false>(V.dp, sgd + V.goff, q.vo, lane);
+    fallback_loop(V.dp, sgd + V.goff, q.vo, q.va, lane, gw, nw);
   }
   if (!grid_sync(B.bar, B.nblocks)) return;
+  stamp(B.bar, 4);
 
   // phase 4: shading
   for (int v = 0; v < B.nviews; v++) {
@@ -157,7 +187,17 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
     int W = V.w, n = V.w * V.h;
     for (int i = tid; i < n; i += step) {
       int y = i / W, x = i - y * W;
-      shade_pixel(V.dp, sgd, x, y, V.dp.keys[i]);
+      shade_pixel(V.dp, sgd + V.goff, x, y, V.dp.keys[i]);
+    }
+  }
+  // the last block to finish stamps the end
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(B.bar + 3, 1u) == B.nblocks - 1) {
+      uint64_t t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      reinterpret_cast<uint64_t *>(B.bar + 4)[5] = t;
     }
   }
 }

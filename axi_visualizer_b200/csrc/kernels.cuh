@@ -108,6 +108,17 @@ __global__ void k_clear_depth(float *__restrict__ f, int w, int h, int lenP) {
   }
 }
 
+// Colour half of the current reference's clearZBuffer (Ops.py:939-946):
+// every pixel of the three colour planes := (r, g, b).
+__global__ void k_fill_rgb(uint16_t *__restrict__ ro, uint16_t *__restrict__ go, uint16_t *__restrict__ bo, int n,
+                           uint16_t r, uint16_t g, uint16_t b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    ro[i] = r;
+    go[i] = g;
+    bo[i] = b;
+  }
+}
+
 // Post/gamma.c:38-52
 __global__ void k_gamma(uint16_t *r, uint16_t *g, uint16_t *b, int n, float exposure) {
   float e8 = 8 * exposure;

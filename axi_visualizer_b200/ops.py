@@ -22,6 +22,11 @@ from ._lib import AxrError, check, lib
 from .scenes import flags_from_string, view_mat
 
 
+# sky colour the current reference's clearZBuffer fills the frame with
+# (Ops.py:941: (60, 110, 255)^2 / 3 as int32)
+SKY_COLOR = tuple(int(x) for x in (np.array([60, 110, 255.0]) ** 2 / 3).astype(np.int32))
+
+
 def _p(a):
     return None if a is None else a.ctypes.data
 
@@ -136,6 +141,12 @@ class CLDraw:
     # ------------------------------------------------------------ frame
     def clearZBuffer(self):
         check(self._L.axr_clear_zbuffer(self._h), "clearZBuffer")
+
+    def clearColor(self, col):
+        """Colour half of the current reference's clearZBuffer (Ops.py:939-946):
+        fills the colour planes with `col` (three u16 values, e.g. SKY_COLOR)."""
+        r, g, b = (int(x) for x in col)
+        check(self._L.axr_clear_color(self._h, r, g, b), "clearColor")
 
     def _material_args(self, shaders):
         n = len(self.gSize)

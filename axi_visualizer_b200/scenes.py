@@ -390,6 +390,40 @@ def scene_small(seed=3, terrain_n=16, spheres=24, nquads=40, tex=64, alpha_tex=6
     return _finish(groups, alphas, shadows)
 
 
+SERVING_SEEDS = tuple(range(10, 18))
+
+
+def scene_served(seed, tmin=50_000, tmax=1_000_000, tex=1024, alpha_tex=512, cascades=(2048, 1024)):
+    """One of the resident scenes of the serving workload: a triangle budget T
+    drawn log-uniform in [tmin, tmax] from the seed, split about half terrain,
+    45% icospheres, 5% alpha-tested quads, over 4 materials (two trilinear
+    terrain/sphere textures, one sphere material without mip, the alpha quads);
+    two shadow cascades of the same sun."""
+    rng = np.random.default_rng(seed)
+    T = float(np.exp(rng.uniform(math.log(tmin), math.log(tmax))))
+    n = max(8, int(round(math.sqrt(T * 0.5 / 2))))
+    spheres = max(2, int(T * 0.45 / 80))
+    nquads = max(2, int(T * 0.05 / 2))
+    extent = 16.0 + 48.0 * math.sqrt(T / tmax)
+    cell = 2 * extent / n
+    xyz, vn, uv = terrain(rng, n, cell, (-extent, 0.0, -extent), 2.0 * cell)
+    sx, sn, su = icospheres(rng, spheres, 0.2, 1.0, -extent * 0.6, extent * 0.6)
+    qx, qn, qu = quads(rng, nquads, -extent * 0.6, extent * 0.6, 0.3, 1.0)
+    texs = [noise_texture(rng, tex)[0] for _ in range(3)]
+    qrgb, qmask = noise_texture(rng, alpha_tex, alpha_p=0.6)
+    half_s = (spheres // 2) * 80 * 3
+    f = MIP | SHADOW
+    groups = [
+        _group(xyz, vn, uv, texs[0], f, 0.2),
+        _group(sx[:half_s], sn[:half_s], su[:half_s], texs[1], f | CULL, 0.2),
+        _group(sx[half_s:], sn[half_s:], su[half_s:], texs[2], SHADOW | CULL, 0.2),
+        _group(qx, qn, qu, qrgb, ALPHA | SHADOW, 0.2, alpha_index=0),
+    ]
+    shadows = [ShadowCam.facing(cascades[0], cascades[0] / 2 / (extent * 0.75), (0, 0, 0), SUN),
+               ShadowCam.facing(cascades[1], cascades[1] / 2 / (extent * 1.5), (0, 0, 0), SUN)]
+    return _finish(groups, [(qmask.reshape(-1), alpha_tex)], shadows)
+
+
 def default_view(w, h, pos=(0.0, 5.0, -25.0), target=(0.0, 0.0, 0.0), fov=70.0):
     return View.perspective(w, h, pos, target, fov)
 

@@ -286,6 +286,57 @@ def batched_section(steps, device, log=progress):
             "tuning": {k: tuned[k] for k in ("blocks_per_sm", "min_chunk", "ms", "cached")}}
 
 
+# ------------------------------------------------------------------ serving
+
+def served_section(device, n_poisson=1000, n_burst=400, rates=(200.0, 1000.0), tuning=None, log=progress):
+    """Serving workload: 8 resident scenes (seeds 10-17, 50k-1M triangles
+    each), Poisson arrivals, resolutions 640x360 / 1280x720 / 1920x1080 /
+    2560x1440 with p = 0.4/0.3/0.2/0.1, random camera poses, a 150 GB HBM
+    budget; each request's colour planes and depth are copied back to pinned
+    host memory.  Runs the named rate (200 requests/s), a rate near the plain
+    path's capacity, and a burst of requests all arriving at t=0 (the
+    saturated rate); the same traces run through the plain per-view path
+    (first come first served, one drawAll + getFrame each)."""
+    from axi_visualizer_b200 import scenes as S
+    from axi_visualizer_b200 import serve as SV
+
+    log("served: building scenes")
+    scenes = [S.scene_served(s) for s in S.SERVING_SEEDS]
+    res = SV.ResidentScenes(scenes, device=device)
+    srv = SV.Server(SV.GpuBackend(res, tuning=tuning), budget_bytes=SV.HBM_BUDGET, resident_bytes=res.nbytes,
+                    max_slabs=8, depth=2)
+    plain = SV.PlainServer(scenes, SV.RESOLUTIONS, device=device)
+    warm = SV.poisson_trace(40, 1e6, len(scenes), seed=99, burst=True)
+    log("served: warm-up")
+    srv.prepare(srv.max_slabs)
+    srv.run(warm)
+    plain.run(SV.poisson_trace(40, 1e6, len(scenes), seed=99, burst=True))
+    keep = ("frames_per_s", "Mpix_per_s", "p50_ms", "p99_ms", "max_ms", "done")
+    sched = ("views_per_launch", "launches", "max_inflight", "slabs")
+    runs, peak = [], 0
+    cases = [(f"poisson_{r:g}", SV.poisson_trace(n_poisson if r <= 200 else 2 * n_poisson, r, len(scenes), seed=1 + i),
+              r) for i, r in enumerate(rates)]
+    cases.append(("burst", SV.poisson_trace(n_burst, 1.0, len(scenes), seed=7, burst=True), None))
+    for name, trace, rate in cases:
+        log(f"served: {name}")
+        srv.reset_stats()
+        st = srv.run(trace)
+        peak = max(peak, st["hbm_used_peak_bytes"])
+        twin = [SV.Request(r.rid, r.scene, r.w, r.h, r.pos, r.target, r.arrival) for r in trace]
+        pst = plain.run(twin)
+        runs.append({"trace": name, "rate_req_per_s": rate, "requests": len(trace),
+                     "served": {k: st[k] for k in keep + sched}, "plain": {k: pst[k] for k in keep},
+                     "speedup_vs_plain": st["frames_per_s"] / pst["frames_per_s"]})
+    srv.close()
+    return {
+        "workload": "c4_served", "scenes": len(scenes), "scene_triangles": [d["tris"] for d in res.info],
+        "resolutions": [f"{w}x{h}" for w, h in SV.RESOLUTIONS], "probs": list(SV.RES_PROBS),
+        "slab_layout": {f"{w}x{h}": n for (w, h), n in SV.DEFAULT_LAYOUT.items()}, "pipeline_depth": srv.depth,
+        "hbm_budget_gb": SV.HBM_BUDGET / 1e9, "resident_gb": res.nbytes / 1e9, "hbm_used_peak_gb": peak / 1e9,
+        "slab_gb": srv.slab_bytes / 1e9, "d2h": "colour planes + depth per request", "runs": runs,
+    }
+
+
 # ------------------------------------------------------------------ GPU arm
 
 def _smi_index(torch, local):
@@ -307,6 +358,7 @@ def main():
     ap.add_argument("--impl", default="axr", choices=["axr", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -428,6 +480,12 @@ def main():
         progress("batched multi-view")
         batched = batched_section(min(args.steps, 100), local)
 
+    served = None
+    if not args.no_served:
+        progress("served")
+        tun = (batched["tuning"]["blocks_per_sm"], batched["tuning"]["min_chunk"]) if batched else None
+        served = served_section(local, tuning=tun)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_oracle_baseline(scene, view)
@@ -453,6 +511,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "batched": batched,
+            "served": served,
         }
         print(json.dumps(line))
     if world > 1:

@@ -96,6 +96,11 @@ int axr_set_vm(axr_ctx *ctx, const float vm[9]);
  * [0, w/4*4) x [0, h/4*4) region the reference's 4x4 work-items cover. */
 int axr_clear_zbuffer(axr_ctx *ctx);
 
+/* Colour half of the current reference's clearZBuffer (Ops.py:939-946, which
+ * also fills the colour planes with the sky colour): every pixel of the
+ * colour planes := (r, g, b), each in [0, 65535]. */
+int axr_clear_color(axr_ctx *ctx, int r, int g, int b);
+
 /* CLDraw.drawAll(shaders, mask, shadowIds) (Ops0.py:471-648, Ops.py:716-937):
  * flags[g] (AXR_*), alpha_index[g] (alpha mask of alpha groups; may be
  * NULL = 0), mask[g] != 0 skips group g (may be NULL).  shadow_ids lists
@@ -177,6 +182,7 @@ int axr_kernel_times(axr_ctx *ctx, int max, char *names, int name_len, double *t
  * ------------------------------------------------------------------------ */
 #define AXR_VIEW_SHADED 0
 #define AXR_VIEW_DEPTH 1
+#define AXR_VIEW_SKIP 2    /* a shaded view's slot that this render leaves untouched */
 
 typedef struct axr_view_desc {
   int kind;          /* AXR_VIEW_SHADED or AXR_VIEW_DEPTH */
@@ -186,8 +192,17 @@ typedef struct axr_view_desc {
   float scale;       /* shaded: sScale; depth: orthographic scale */
   float cax, cay;    /* shaded: cull bounds (setScaleCull) */
   float bias;        /* depth: shBias of shadowMap */
-  int cascades[2];   /* shaded: batch indices of the depth views it samples */
+  int cascades[2];   /* shaded: batch indices of the depth views it samples, or -1-i for
+                        the handle's shadow map i (rendered by axr_shadow_map) */
   int ncascades;
+  int group_first;   /* the view draws groups [group_first, group_first + group_count) */
+  int group_count;   /* 0 = every group of the handle.  Triangle ids count from the
+                        range's first triangle, so a scene kept as a group range of a
+                        shared handle renders exactly as in a handle of its own */
+  int clear_color;   /* shaded: 1 = colour planes := bg before drawing (as axr_clear_color)
+                        and depth outside the clearzb region := 0 (a new buffer's value),
+                        so the result does not depend on what the slot held before */
+  int bg[3];
 } axr_view_desc;
 
 typedef struct axr_batch axr_batch;
@@ -196,12 +211,16 @@ typedef struct axr_batch axr_batch;
  * first).  Allocates the views' framebuffers, maps and work queues. */
 int axr_batch_create(axr_ctx *ctx, const axr_view_desc *views, int nviews, axr_batch **out);
 
-/* New cameras (same kinds and sizes) for the next render. */
+/* New cameras (same sizes; a shaded slot may switch between AXR_VIEW_SHADED and
+ * AXR_VIEW_SKIP) for the next render. */
 int axr_batch_set_views(axr_batch *b, const axr_view_desc *views, int nviews);
 
 /* Renders every view: depth views clear and draw the casters (cast[g] != 0,
- * NULL = all), shaded views clear and draw all groups with flags[g] and
- * alpha_index[g] (as axr_draw_all).  Asynchronous on the handle's stream. */
+ * NULL = all) of their group range, shaded views clear and draw their group
+ * range with flags[g] and alpha_index[g] (as axr_draw_all); AXR_VIEW_SKIP
+ * slots are left as they are.  Asynchronous on the handle's stream: renders
+ * of several batches of one handle queue behind each other on the GPU while
+ * the host prepares the next. */
 int axr_batch_render(axr_batch *b, const int32_t *flags, const int32_t *alpha_index, const uint8_t *cast,
                      int ngroups);
 
@@ -211,6 +230,25 @@ int axr_batch_get_frame(axr_batch *b, int view, uint16_t *r, uint16_t *g, uint16
 
 /* Triangle id / coverage of a shaded view of the last render. */
 int axr_batch_get_ids(axr_batch *b, int view, int32_t *tri_id, uint8_t *coverage);
+
+/* Queues the copy of a shaded view's colour planes (and depth, if not NULL)
+ * of the last render into host memory (pinned for an asynchronous copy) on
+ * the batch's copy stream, behind the render; does not block.  The data is
+ * there once axr_batch_query returns 1. */
+int axr_batch_read_async(axr_batch *b, int view, uint16_t *r, uint16_t *g, uint16_t *bb, float *depth);
+
+/* 1 if the last render and the reads queued after it have finished and the
+ * render's work counters were checked, 0 if still running (does not block),
+ * negative on an error of that render. */
+int axr_batch_query(axr_batch *b);
+
+/* Durations in ms of the five phases of the last render (clear, setup,
+ * coarse + small triangles + depth maps, tiled large triangles, shading), from
+ * the GPU's global timer at the grid barriers; waits for the render. */
+int axr_batch_phase_times(axr_batch *b, float ms[5]);
+
+/* Device memory held by the batch (framebuffers, maps, work queues, tables). */
+int axr_batch_bytes(axr_batch *b, int64_t *bytes);
 
 /* Number of renders, whether renders replay a captured graph (1) or launch
  * directly (0), and the persistent grid size in blocks. */
