@@ -310,17 +310,22 @@ class RefDraw:
         self.R.ref_get_frame(self.h, _ptr(r), _ptr(g), _ptr(b), _ptr(db))
         return r, g, b, db
 
-    def shadow_map(self, k, cast=None, nthreads=1):
+    def shadow_map(self, k, cast=None, nthreads=1, clear=True, read=True):
+        """Renders the casters into shadow map k; clear=False draws over the
+        map's current contents, read=False skips the copy out."""
         sc = self.scene.shadows[k]
-        self.R.ref_add_shadow_map(self.h, k, sc.dim, sc.scale)
-        self.R.ref_place_shadow_map(self.h, k, _ptr(np.asarray(sc.pos, np.float32)),
-                                    _ptr(np.ascontiguousarray(sc.vv, np.float32)))
-        self.R.ref_clear_shadow_map(self.h, k)
+        if clear:
+            self.R.ref_add_shadow_map(self.h, k, sc.dim, sc.scale)
+            self.R.ref_place_shadow_map(self.h, k, _ptr(np.asarray(sc.pos, np.float32)),
+                                        _ptr(np.ascontiguousarray(sc.vv, np.float32)))
+            self.R.ref_clear_shadow_map(self.h, k)
         if cast is None:
             cast = [g.cast for g in self.scene.groups]
         cast = np.asarray(cast, np.uint8)
         rc = self.R.ref_shadow_map(self.h, k, _ptr(cast), _ptr(self.flags), _ptr(self.aidx), len(self.flags),
                                    self.scene.bias, nthreads)
+        if not read:
+            return rc, None
         out = np.empty((sc.dim, sc.dim), np.float32)
         self.R.ref_get_shadow_map(self.h, k, _ptr(out))
         return rc, out
