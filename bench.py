@@ -39,8 +39,9 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
 # each kernel on this workload, from the ncu capture summarised in
 # profiles/ncu_kernels_1080p_1m.md; None until captured.
-NCU_TRAFFIC = {"k_raster_small": 34465536 + 512, "k_shadow_raster": 46918400 + 7424,
-               "k_shade": 29610752 + 670976}
+NCU_TRAFFIC = {"k_raster_small": 33005312, "k_raster_small_alpha": 13483264,
+               "k_shadow_raster": 43307520 + 2304, "k_shadow_raster_alpha": 9635584,
+               "k_shade": 30226944 + 503808}
 
 
 def progress(msg):
