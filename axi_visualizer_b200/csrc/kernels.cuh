@@ -240,63 +240,105 @@ __global__ void __launch_bounds__(256) k_setup(DrawParams P) {
 // and two fused multiply-adds instead of a division.
 template <bool ALPHA>
 struct VisQ {
-  int cyw[32], lo[32];
-  uint32_t ord[32];
-  float cx2[32], d[32], rd[32], cz1[32], cz2[32];
-  float u1x[ALPHA ? 32 : 1], u1y[ALPHA ? 32 : 1], u2x[ALPHA ? 32 : 1], u2y[ALPHA ? 32 : 1];
+  float4 a[32];                  // cx2, d, 1/d (0: divide), cz1
+  float4 b[32];                  // cz2, pixel address - first pixel number, x - first pixel number, order
+  float4 c[ALPHA ? 32 : 1];      // u1, u2 (uv / z at the span's ends)
   int g[ALPHA ? 32 : 1];
-  int pre[32];
+  int r2l[32];                   // rank among the round's non-empty spans -> span
 };
 
-// Exclusive offsets of the lanes' pixel counts; returns the round's total.
-__device__ __forceinline__ int warp_offsets(int cnt, int lane, int *pre) {
+// Pixels of a round are numbered 0..total-1 in span (lane) order.  Returns
+// the total, sets `pre` to this lane's first pixel number and fills the
+// rank -> span table of the non-empty spans.
+__device__ __forceinline__ int fill_prepare(int cnt, int lane, int *r2l, int &pre) {
   int incl = cnt;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     int v = __shfl_up_sync(FULL, incl, o);
     if (lane >= o) incl += v;
   }
-  pre[lane] = incl - cnt;
+  pre = incl - cnt;
+  unsigned ne = __ballot_sync(FULL, cnt > 0);
+  if (cnt > 0) r2l[__popc(ne & ((1u << lane) - 1u))] = lane;
   return __shfl_sync(FULL, incl, 31);
 }
 
-// index of the span holding pixel p: the largest s with pre[s] <= p
-__device__ __forceinline__ int span_of(const int *pre, int p) {
-  int s = 0;
-#pragma unroll
-  for (int step = 16; step; step >>= 1)
-    if (pre[s + step] <= p) s += step;     // s + step <= 31
-  return s;
+// Calls pix(span, p) for every pixel p < total, lane j taking pixels j,
+// j + 32, ...  A pixel's span is the last non-empty span starting at or
+// before it: its rank = (non-empty spans starting before the window, one
+// ballot) + (starts inside the window up to this lane, from one OR-reduction
+// of the start bits) - 1.
+template <class F>
+__device__ __forceinline__ void fill_windows(int total, int cnt, int pre, int lane, const int *r2l, F &&pix) {
+  const unsigned upto = 0xffffffffu >> (31 - lane);
+  for (int base = 0; base < total; base += 32) {
+    int rel = pre - base;
+    unsigned bit = (cnt > 0 && (unsigned)rel < 32u) ? (1u << rel) : 0u;
+    unsigned starts = __reduce_or_sync(FULL, bit);
+    int before = __popc(__ballot_sync(FULL, cnt > 0 && rel < 0));
+    int p = base + lane;
+    if (p < total) pix(r2l[before + __popc(starts & upto) - 1], p);
+  }
+}
+
+// One round of a span queue: numbering, record fix-up (address and x made
+// relative to the span's first pixel number), pixel-parallel fill.
+template <class Q, class F>
+__device__ __forceinline__ void fill_round(Q &q, int lane, int cnt, F &&pix) {
+  int pre;
+  int total = fill_prepare(cnt, lane, q.r2l, pre);
+  if (total == 0) return;
+  if (cnt) {
+    float4 b = q.b[lane];
+    b.y = __int_as_float(__float_as_int(b.y) - pre);
+    b.z = __int_as_float(__float_as_int(b.z) - pre);
+    q.b[lane] = b;
+  }
+  __syncwarp();
+  fill_windows(total, cnt, pre, lane, q.r2l, pix);
+  __syncwarp();
+}
+
+// Writes lane's span record: row offset cyw, first pixel lo, ends cx1 / cx2.
+template <bool ALPHA>
+__device__ __forceinline__ void vis_put(VisQ<ALPHA> &q, int lane, int cyw, int lo, uint32_t ord, float cx1, float cx2,
+                                        float cz1, float cz2, V2 cu1, V2 cu2, int g) {
+  float d = cx1 - cx2;
+  q.a[lane] = make_float4(cx2, d, span_recip_exact(d, cx2, lo), cz1);
+  q.b[lane] = make_float4(cz2, __int_as_float(cyw + lo), __int_as_float(lo), __uint_as_float(ord));
+  if (ALPHA) {
+    q.c[lane] = make_float4(cu1.x, cu1.y, cu2.x, cu2.y);
+    q.g[lane] = g;
+  }
 }
 
 // Per-fragment visibility: alpha test (av_draw_alpha.c:80-97) then the
 // packed depth/order atomicMin.
+// Pixel number p of span s (x = p + b.z, address = p + b.y).  The reciprocal
+// of the interpolated 1/z is correctly rounded (__frcp_rn), i.e. 1.0f / x.
 template <bool ALPHA>
-__device__ __forceinline__ void vis_pixel(const DrawParams &P, const GroupDev *sg, const VisQ<ALPHA> &q, int s, int ax) {
-  float t = quot_by_recip((float)ax - q.cx2[s], q.d[s], q.rd[s]);
+__device__ __forceinline__ void vis_pixel(const DrawParams &P, const GroupDev *sg, const VisQ<ALPHA> &q, int s, int p) {
+  const float4 a = q.a[s], b = q.b[s];
+  float n = (float)(p + __float_as_int(b.z)) - a.x;
+  float t = a.z != 0.f ? quot_fast(n, a.y, a.z) : n / a.y;
   t = clamp_t(t);
-  float tz = 1.0f / ((1 - t) * q.cz2[s] + t * q.cz1[s]);
+  float tz = __frcp_rn((1 - t) * b.x + t * a.w);
   if (tz != tz) return;
   if (ALPHA) {
+    const float4 c = q.c[s];
     const GroupDev &G = sg[q.g[s]];
     float omt = 1 - t;
-    V2 uvi{omt * q.u2x[s] + t * q.u1x[s], omt * q.u2y[s] + t * q.u1y[s]};
+    V2 uvi{omt * c.z + t * c.x, omt * c.w + t * c.y};
     Taps tp = make_taps(uvi, tz, G.alen, 0);
     if (!(bilerp_quad(tp, G.aquad) > 0.5f)) return;
   }
-  atomicMin((unsigned long long *)&P.keys[(size_t)q.cyw[s] + ax], (unsigned long long)frag_key(tz, q.ord[s]));
+  atomicMin((unsigned long long *)&P.keys[(size_t)(p + __float_as_int(b.y))],
+            (unsigned long long)frag_key(tz, __float_as_uint(b.w)));
 }
 
 template <bool ALPHA>
 __device__ __forceinline__ void vis_fill(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, int cnt) {
-  int total = warp_offsets(cnt, lane, q.pre);
-  if (total == 0) return;
-  __syncwarp();
-  for (int p = lane; p < total; p += 32) {
-    int s = span_of(q.pre, p);
-    vis_pixel<ALPHA>(P, sg, q, s, q.lo[s] + (p - q.pre[s]));
-  }
-  __syncwarp();
+  fill_round(q, lane, cnt, [&](int s, int p) { vis_pixel<ALPHA>(P, sg, q, s, p); });
 }
 
 // ------------------------------------------------------------ small triangles
@@ -422,15 +464,7 @@ struct SmallLane {
       if (half == 0) span_clip(f2i(cx2), cx1, P.view.w, lo, cnt);
       else span_clip(f2i(cx1), cx2, P.view.w, lo, cnt);
     }
-    if (cnt) {
-      float d = cx1 - cx2;
-      q.cyw[lane] = cy * P.view.w;
-      q.lo[lane] = lo;
-      q.ord[lane] = make_order(0, gtri, half);
-      q.cx2[lane] = cx2; q.d[lane] = d; q.rd[lane] = span_recip(d);
-      q.cz1[lane] = cz1; q.cz2[lane] = cz2;
-      if (ALPHA) { q.u1x[lane] = cu1.x; q.u1y[lane] = cu1.y; q.u2x[lane] = cu2.x; q.u2y[lane] = cu2.y; q.g[lane] = g; }
-    }
+    if (cnt) vis_put<ALPHA>(q, lane, cy * P.view.w, lo, make_order(0, gtri, half), cx1, cx2, cz1, cz2, cu1, cu2, g);
     skip_row();
     live = --left > 0;
     return cnt;
@@ -708,13 +742,7 @@ struct TileLane {
   }
 
   __device__ __forceinline__ void put(const DrawParams &P, VisQ<ALPHA> &q, int lane, int lo) {
-    float d = cx1 - cx2;
-    q.cyw[lane] = cy * P.view.w;
-    q.lo[lane] = lo;
-    q.ord[lane] = make_order(1, gtri, half);
-    q.cx2[lane] = cx2; q.d[lane] = d; q.rd[lane] = span_recip(d);
-    q.cz1[lane] = cz1; q.cz2[lane] = cz2;
-    if (ALPHA) { q.u1x[lane] = cu1.x; q.u1y[lane] = cu1.y; q.u2x[lane] = cu2.x; q.u2y[lane] = cu2.y; q.g[lane] = g; }
+    vis_put<ALPHA>(q, lane, cy * P.view.w, lo, make_order(1, gtri, half), cx1, cx2, cz1, cz2, cu1, cu2, g);
   }
 
   __device__ __forceinline__ int emit(const DrawParams &P, VisQ<ALPHA> &q, int lane, bool &live) {
@@ -794,8 +822,8 @@ __device__ __forceinline__ void fallback_unit(const DrawParams &P, const GroupDe
   TileLane<ALPHA> L;
   bool live = L.init(P, sg, make_uint2(gt, (uint32_t)tile));
   for (int round = 0; live && round < LOOP_LIMIT; round++) {
-    int cnt = L.emit(P, q, lane, live);
-    for (int j = 0; j < cnt; j++) vis_pixel<ALPHA>(P, sg, q, lane, q.lo[lane] + j);
+    int cnt = L.emit(P, q, lane, live);   // the lane's own record: pixel j is x = lo + j
+    for (int j = 0; j < cnt; j++) vis_pixel<ALPHA>(P, sg, q, lane, j);
   }
 }
 
@@ -1099,11 +1127,11 @@ __device__ __forceinline__ void atomic_min_depth(float *addr, float v) {
 
 template <bool ALPHA>
 struct ShadowQ {
-  int cyw[32], lo[32];
-  float cx2[32], d[32], rd[32], cz1[32], cz2[32];
-  float cu1[ALPHA ? 32 : 1], cv1[ALPHA ? 32 : 1], cu2[ALPHA ? 32 : 1], cv2[ALPHA ? 32 : 1];
+  float4 a[32];                  // cx2, d, 1/d (0: divide), cz1
+  float4 b[32];                  // cz2, texel address - first pixel number, x - first pixel number, unused
+  float4 c[ALPHA ? 32 : 1];      // cu1, cv1, cu2, cv2
   int g[ALPHA ? 32 : 1];
-  int pre[32];
+  int r2l[32];
 };
 
 template <bool ALPHA>
@@ -1114,13 +1142,19 @@ struct ShadowLane {
   float s1, s2, sz1, sz2, su1, su2, sv1, sv2;
   float cx1, cx2, cz1, cz2, cu1, cu2, cv1, cv2;
 
+  // drawmin.c divides each slope by the row count; one reciprocal serves
+  // them all (quot_by_recip: the same correctly rounded quotients)
   __device__ __forceinline__ void start_half0() {
     half = 0;
     float d = (float)(y2 - y1);
-    s1 = (float)(x2 - x1) / d;
-    s2 = (float)(x4 - x1) / d;
-    if (ALPHA) { su1 = (u2 - u1) / d; sv1 = (v2 - v1) / d; su2 = (u4 - u1) / d; sv2 = (v4 - v1) / d; }
-    sz1 = (z2 - z1) / d; sz2 = (z4 - z1) / d;
+    float y = span_recip(d);
+    s1 = quot_by_recip((float)(x2 - x1), d, y);
+    s2 = quot_by_recip((float)(x4 - x1), d, y);
+    if (ALPHA) {
+      su1 = quot_by_recip(u2 - u1, d, y); sv1 = quot_by_recip(v2 - v1, d, y);
+      su2 = quot_by_recip(u4 - u1, d, y); sv2 = quot_by_recip(v4 - v1, d, y);
+    }
+    sz1 = quot_by_recip(z2 - z1, d, y); sz2 = quot_by_recip(z4 - z1, d, y);
     cx1 = cx2 = (float)x1; cz1 = cz2 = z1;
     if (ALPHA) { cu1 = cu2 = u1; cv1 = cv2 = v1; }
     if (s1 < s2) {
@@ -1132,10 +1166,14 @@ struct ShadowLane {
   __device__ __forceinline__ void start_half1() {
     half = 1;
     float d = (float)(y3 - y2);
-    s1 = (float)(x3 - x2) / d;
-    s2 = (float)(x3 - x4) / d;
-    if (ALPHA) { su1 = (u3 - u2) / d; sv1 = (v3 - v2) / d; su2 = (u3 - u4) / d; sv2 = (v3 - v4) / d; }
-    sz1 = (z3 - z2) / d; sz2 = (z3 - z4) / d;
+    float y = span_recip(d);
+    s1 = quot_by_recip((float)(x3 - x2), d, y);
+    s2 = quot_by_recip((float)(x3 - x4), d, y);
+    if (ALPHA) {
+      su1 = quot_by_recip(u3 - u2, d, y); sv1 = quot_by_recip(v3 - v2, d, y);
+      su2 = quot_by_recip(u3 - u4, d, y); sv2 = quot_by_recip(v3 - v4, d, y);
+    }
+    sz1 = quot_by_recip(z3 - z2, d, y); sz2 = quot_by_recip(z3 - z4, d, y);
     cx1 = cx2 = (float)x3; cz1 = cz2 = z3;
     if (ALPHA) { cu1 = cu2 = u3; cv1 = cv2 = v3; }
     if (s1 < s2) {
@@ -1184,11 +1222,12 @@ struct ShadowLane {
       cnt = hi >= lo ? hi - lo + 1 : 0;
       if (cnt) {
         float d = cx1 - cx2;
-        q.cyw[lane] = cy * dim;
-        q.lo[lane] = lo;
-        q.cx2[lane] = cx2; q.d[lane] = d; q.rd[lane] = span_recip(d);
-        q.cz1[lane] = cz1; q.cz2[lane] = cz2;
-        if (ALPHA) { q.cu1[lane] = cu1; q.cv1[lane] = cv1; q.cu2[lane] = cu2; q.cv2[lane] = cv2; q.g[lane] = g; }
+        q.a[lane] = make_float4(cx2, d, span_recip_exact(d, cx2, lo), cz1);
+        q.b[lane] = make_float4(cz2, __int_as_float(cy * dim + lo), __int_as_float(lo), 0.f);
+        if (ALPHA) {
+          q.c[lane] = make_float4(cu1, cv1, cu2, cv2);
+          q.g[lane] = g;
+        }
       }
     }
     if (half == 0) {
@@ -1211,22 +1250,25 @@ struct ShadowLane {
 
 // drawmin.c:71-76 / drawminalpha.c:83-97 for one pixel of span s
 template <bool ALPHA>
-__device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int ax) {
-  float t = quot_by_recip((float)ax - q.cx2[s], q.d[s], q.rd[s]);
+__device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p) {
+  const float4 a = q.a[s], b = q.b[s];
+  float n = (float)(p + __float_as_int(b.z)) - a.x;
+  float t = a.z != 0.f ? quot_fast(n, a.y, a.z) : n / a.y;
   t = clamp_t(t);
-  float tz = 1.0f / ((1 - t) * q.cz2[s] + t * q.cz1[s]);
+  float tz = __frcp_rn((1 - t) * b.x + t * a.w);
   if (tz != tz) return;
   if (ALPHA) {
+    const float4 c = q.c[s];
     const GroupDev &G = sg[q.g[s]];
     int len = G.alen;
     float lm1 = (float)(len - 1);
-    int t1 = f2i((((1 - t) * q.cu2[s] + t * q.cu1[s]) * tz) * lm1);
+    int t1 = f2i((((1 - t) * c.z + t * c.x) * tz) * lm1);
     t1 = iabs_(t1) & (len - 1);
-    int t2 = f2i((lm1 * ((1 - t) * q.cv2[s] + t * q.cv1[s])) * tz);
+    int t2 = f2i((lm1 * ((1 - t) * c.w + t * c.y)) * tz);
     t2 = iabs_(t2) & (len - 1);
     if (!__ldg(G.amask + t1 + t2 * len)) return;
   }
-  atomic_min_depth(map + (size_t)q.cyw[s] + ax, tz);
+  atomic_min_depth(map + (size_t)(p + __float_as_int(b.y)), tz);
 }
 
 template <bool ALPHA>
@@ -1252,14 +1294,7 @@ __device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const Gr
       }
       int cnt = 0;
       if (live) cnt = L.emit(dim, q, lane, live);
-      int total = warp_offsets(cnt, lane, q.pre);
-      if (total == 0) continue;
-      __syncwarp();
-      for (int p = lane; p < total; p += 32) {
-        int s = span_of(q.pre, p);
-        shadow_pixel<ALPHA>(S.map, sg, q, s, q.lo[s] + (p - q.pre[s]));
-      }
-      __syncwarp();
+      fill_round(q, lane, cnt, [&](int s, int p) { shadow_pixel<ALPHA>(S.map, sg, q, s, p); });
     }
   }
 }

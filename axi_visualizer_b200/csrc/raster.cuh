@@ -105,6 +105,26 @@ __device__ __forceinline__ float span_recip(float d) {
   float a = fabsf(d);
   return (a >= 8.6736174e-19f && a <= 1.1529215e18f) ? __frcp_rn(d) : 0.f;
 }
+// y of span_recip(d) when, in addition, every quotient (ax - cx2) / d of the
+// span's pixels (integer ax >= lo >= 0) can take the reciprocal path: then
+// |ax - cx2| <= 2^60 and it is 0 or >= 2^-60 (for |cx2| >= 2^-36 the exact
+// difference is a multiple of ulp(cx2) >= 2^-59; for smaller cx2 it is
+// either cx2 itself, when ax = 0 and cx2 = 0, or at least 1 - 2^-36).
+// Returns 0 when a pixel might need the true division.
+__device__ __forceinline__ float span_recip_exact(float d, float cx2, int lo) {
+  float y = span_recip(d);
+  float a = fabsf(cx2);
+  bool ok = a <= 0x1p59f && (a >= 0x1p-36f || cx2 == 0.f || lo > 0);
+  return ok ? y : 0.f;
+}
+
+// The quotient of quot_by_recip when the operands are known to be in range.
+__device__ __forceinline__ float quot_fast(float n, float d, float y) {
+  float q = __fmul_rn(n, y);
+  float r = __fmaf_rn(-d, q, n);
+  return __fmaf_rn(r, y, q);
+}
+
 __device__ __forceinline__ float quot_by_recip(float n, float d, float y) {
   float an = fabsf(n);
   if (y != 0.f && an <= 1.1529215e18f && (an >= 8.6736174e-19f || n == 0.f)) {
