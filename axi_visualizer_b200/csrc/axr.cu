@@ -67,7 +67,7 @@ struct Shadow {
   float vv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   cudaStream_t st = nullptr;
   cudaEvent_t ev_write = nullptr, ev_read = nullptr;
-  uint32_t *list = nullptr, *ctr = nullptr;
+  uint32_t *list = nullptr, *ctr = nullptr, *items = nullptr;
   uint32_t cap = 0;
   GroupDev *tab = nullptr;
 };
@@ -116,14 +116,17 @@ struct axr_ctx {
 
 namespace {
 
+// list positions travel in work items as position << CHUNK_BITS | chunk
+constexpr uint32_t MAX_LIST = 0xffffffffu >> CHUNK_BITS;
+
 int ensure_lists(axr_ctx *c) {
   uint32_t need = (uint32_t)std::max(c->total_tris, 1);
   if (need <= c->cap_list) return 0;
-  uint32_t cap = std::max(need, c->cap_list * 2);
+  if (need > MAX_LIST) return fail(AXR_EINVAL, "more than %u triangles", MAX_LIST);
+  uint32_t cap = (uint32_t)std::max<uint64_t>(need, std::min<uint64_t>(2ull * c->cap_list, MAX_LIST));
   cudaStreamSynchronize(c->stream);
   cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items);
   c->small_list = c->large_list = c->items = nullptr;
-  if (cap > 0x3fffffffu / MAX_CHUNKS) return fail(AXR_EINVAL, "too many triangles");
   if (cudaMalloc(&c->small_list, sizeof(uint32_t) * cap) != cudaSuccess ||
       cudaMalloc(&c->large_list, sizeof(uint32_t) * cap) != cudaSuccess ||
       cudaMalloc(&c->items, sizeof(uint32_t) * cap * MAX_CHUNKS) != cudaSuccess)
@@ -369,7 +372,7 @@ int axr_destroy(axr_ctx *c) {
     if (sm.st) { cudaStreamSynchronize(sm.st); cudaStreamDestroy(sm.st); }
     if (sm.ev_write) cudaEventDestroy(sm.ev_write);
     if (sm.ev_read) cudaEventDestroy(sm.ev_read);
-    cudaFree(sm.map); cudaFree(sm.list); cudaFree(sm.ctr); cudaFree(sm.tab);
+    cudaFree(sm.map); cudaFree(sm.list); cudaFree(sm.items); cudaFree(sm.ctr); cudaFree(sm.tab);
   }
   if (c->s_alpha) { cudaStreamSynchronize(c->s_alpha); cudaStreamDestroy(c->s_alpha); }
   if (c->ev_setup) cudaEventDestroy(c->ev_setup);
@@ -753,8 +756,11 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   if (sm.cap < c->cap_list) {
     CK(cudaStreamSynchronize(sm.st));
     cudaFree(sm.list);
-    sm.list = nullptr;
-    if (cudaMalloc(&sm.list, sizeof(uint32_t) * c->cap_list) != cudaSuccess)
+    cudaFree(sm.items);
+    sm.list = sm.items = nullptr;
+    sm.cap = 0;
+    if (cudaMalloc(&sm.list, sizeof(uint32_t) * c->cap_list) != cudaSuccess ||
+        cudaMalloc(&sm.items, sizeof(uint32_t) * c->cap_list * MAX_CHUNKS) != cudaSuccess)
       return fail(AXR_ENOMEM, "caster list of shadow map %d", i);
     sm.cap = c->cap_list;
   }
@@ -767,6 +773,7 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   memcpy(S.sh.pos, sm.pos, sizeof sm.pos);
   memcpy(S.sh.vv, sm.vv, sizeof sm.vv);
   S.map = sm.map; S.bias = bias; S.list = sm.list; S.cap_list = sm.cap; S.ctr = sm.ctr;
+  S.items = sm.items; S.min_chunk = c->min_chunk;
   if (c->total_tris == 0) return 0;
   bool any_alpha = false;
   for (int g = 0; g < ngroups; g++)
@@ -960,6 +967,7 @@ bool dalloc(T **p, size_t n, int64_t &bytes) {
 int batch_alloc(axr_batch *b, uint32_t units_per_view) {
   axr_ctx *c = b->c;
   uint32_t cap = (uint32_t)std::max(c->total_tris, 1);
+  if (cap > MAX_LIST) return fail(AXR_EINVAL, "more than %u triangles", MAX_LIST);
   b->cap_list = cap;
   b->buf.assign(b->desc.size(), axr_batch::Buf());
   int64_t &B = b->bytes;
@@ -980,7 +988,8 @@ int batch_alloc(axr_batch *b, uint32_t units_per_view) {
       }
     } else {
       size_t n = (size_t)v.w * v.w;
-      ok = ok && dalloc(&x.map, n * 4, B) && dalloc(&x.list, 4ull * cap, B);
+      ok = ok && dalloc(&x.map, n * 4, B) && dalloc(&x.list, 4ull * cap, B) &&
+           dalloc(&x.items, 4ull * cap * MAX_CHUNKS, B);
       if (ok) {
         k_clear_depth<<<grid_for(c, (long)n, 256, 8), 256, 0, c->stream>>>(x.map, v.w, v.w, 1);
         ok = cudaGetLastError() == cudaSuccess;
@@ -1040,6 +1049,7 @@ void batch_fill_views(axr_batch *b) {
       S.sh.map = x.map; S.sh.dim = v.w; S.sh.scale = v.scale;
       memcpy(S.sh.pos, v.pos, sizeof v.pos); memcpy(S.sh.vv, v.vm, sizeof v.vm);
       S.map = x.map; S.bias = v.bias; S.list = x.list; S.cap_list = b->cap_list; S.ctr = x.ctr;
+      S.items = x.items; S.min_chunk = b->min_chunk;
     }
   }
 }
@@ -1433,8 +1443,9 @@ __global__ void __launch_bounds__(256) k_shadow_setup_noalloc(GroupDev G, Shadow
   for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
     int t = base + threadIdx.x;
     bool ok, alpha;
-    shadow_classify(sg, S, t, ok, alpha);
-    shadow_append(S, t, ok, alpha, lane);
+    int rows;
+    shadow_classify(sg, S, t, ok, alpha, rows);
+    shadow_append(S, t, ok, alpha, rows, lane);   // S.items is null: no row chunks
   }
 }
 

@@ -47,7 +47,7 @@ struct DrawParams {
 enum {
   CTR_SMALL = 0, CTR_SMALL_A, CTR_LARGE, CTR_UNITS, CTR_UNITS_A, CTR_WORK_SMALL, CTR_WORK_SMALL_A, CTR_WORK_LARGE,
   CTR_WORK_UNITS, CTR_WORK_UNITS_A, CTR_OVERFLOW, CTR_SH_LIST, CTR_SH_LIST_A, CTR_SH_WORK, CTR_SH_WORK_A,
-  CTR_UNITS_RESERVED, CTR_LIMIT, CTR_ITEMS, CTR_ITEMS_A, CTR_N = 32
+  CTR_UNITS_RESERVED, CTR_LIMIT, CTR_ITEMS, CTR_ITEMS_A, CTR_SH_ITEMS, CTR_SH_ITEMS_A, CTR_N = 32
 };
 
 // Every data-dependent loop is bounded by construction (rows of a small
@@ -82,8 +82,9 @@ __device__ __forceinline__ void span_clip(int ax0, float bound, int w, int &lo, 
 // rows, so that large "small" triangles spread over several lanes; a lane
 // replays the row accumulation up to its chunk, which keeps every
 // interpolant bit-identical to the serial walk.
-constexpr int MIN_CHUNK = 16;   // default of DrawParams::min_chunk
-constexpr int MAX_CHUNKS = 3;
+constexpr int MIN_CHUNK = 12;   // default of DrawParams::min_chunk
+constexpr int CHUNK_BITS = 3;   // work item = list position << CHUNK_BITS | chunk
+constexpr int MAX_CHUNKS = 1 << CHUNK_BITS;
 __device__ __forceinline__ int small_rows(int y1, int y3) { return y3 - y1 + 2; }
 __device__ __forceinline__ int chunk_len(int rows, int min_chunk) {
   int c = (rows + MAX_CHUNKS - 1) / MAX_CHUNKS;
@@ -218,7 +219,7 @@ __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev 
     oa = __shfl_sync(FULL, oa, 31) + (uint32_t)(ia - ca);
     uint32_t cap_items = P.cap_list * MAX_CHUNKS;
     for (int c = 0; c < nch; c++) {
-      uint32_t item = (pos << 2) | (uint32_t)c;
+      uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
       if (!alpha) P.items[oo + c] = item;
       else P.items[cap_items - 1 - (oa + c)] = item;
     }
@@ -485,8 +486,8 @@ __device__ __forceinline__ void raster_small_loop(const DrawParams &P, const Gro
     if (live) {
       uint32_t idx = base + lane;
       uint32_t item = P.items[ALPHA ? cap_items - 1 - idx : idx];
-      uint32_t pos = item >> 2;
-      L.init_chunk(P, sg, P.small_list[ALPHA ? P.cap_list - 1 - pos : pos], (int)(item & 3));
+      uint32_t pos = item >> CHUNK_BITS;
+      L.init_chunk(P, sg, P.small_list[ALPHA ? P.cap_list - 1 - pos : pos], (int)(item & (MAX_CHUNKS - 1)));
     }
     for (int round = 0; __any_sync(FULL, live); round++) {
       if (round == LOOP_LIMIT) {
@@ -1040,7 +1041,7 @@ __device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev 
   P.db[pix] = tz;
 }
 
-__global__ void __launch_bounds__(256) k_shade(DrawParams P) {
+__global__ void __launch_bounds__(256, 3) k_shade(DrawParams P) {   // 80 registers: 3 blocks per SM
   __shared__ GroupDev sg[64];
   for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < P.ngroups; i += blockDim.x * blockDim.y)
     sg[i] = P.groups[i];
@@ -1073,11 +1074,17 @@ struct ShadowParams {
   uint32_t *list;      // opaque casters from the front, alpha-tested from the back
   uint32_t cap_list;
   uint32_t *ctr;
+  uint32_t *items;     // row chunks of the casters, same two ends (cap_list * MAX_CHUNKS);
+                       // null: one work item per caster
+  int min_chunk;       // rows per chunk (at least)
 };
 
-__device__ __forceinline__ void shadow_classify(const GroupDev *sg, const ShadowParams &S, int t, bool &ok, bool &alpha) {
+// rows = the caster's row count in the map (drawmin.c: y1..y2 up, y3..y2+1 down)
+__device__ __forceinline__ void shadow_classify(const GroupDev *sg, const ShadowParams &S, int t, bool &ok, bool &alpha,
+                                                int &rows) {
   ok = false;
   alpha = false;
+  rows = 0;
   if (t < S.total_tris) {
     const GroupDev &G = sg[find_group(sg, S.ngroups, (uint32_t)t)];
     if (G.enabled) {
@@ -1085,11 +1092,12 @@ __device__ __forceinline__ void shadow_classify(const GroupDev *sg, const Shadow
       float z[3];
       ok = project_ortho(G, t - G.tri_base, S.sh, S.bias, ix, iy, z);
       alpha = (G.flags & F_ALPHA) != 0;
+      rows = max(iy[0], max(iy[1], iy[2])) - min(iy[0], min(iy[1], iy[2])) + 1;
     }
   }
 }
 
-__device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int lane) {
+__device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int rows, int lane) {
   unsigned mo = __ballot_sync(FULL, ok && !alpha), ma = __ballot_sync(FULL, ok && alpha);
   uint32_t bo = 0, ba = 0;
   if (lane == 0) {
@@ -1099,8 +1107,37 @@ __device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool
   bo = __shfl_sync(FULL, bo, 0);
   ba = __shfl_sync(FULL, ba, 0);
   unsigned lt = (1u << lane) - 1;
-  if (ok && !alpha) S.list[bo + __popc(mo & lt)] = (uint32_t)t;
-  if (ok && alpha) S.list[S.cap_list - 1 - (ba + __popc(ma & lt))] = (uint32_t)t;
+  uint32_t pos = 0;
+  if (ok && !alpha) { pos = bo + __popc(mo & lt); S.list[pos] = (uint32_t)t; }
+  if (ok && alpha) { pos = ba + __popc(ma & lt); S.list[S.cap_list - 1 - pos] = (uint32_t)t; }
+  if (!S.items) return;
+  // row chunks of the casters, as for the small triangles of the view
+  int nch = 0;
+  if (ok) {
+    int cl = chunk_len(rows, S.min_chunk);
+    nch = (rows + cl - 1) / cl;
+  }
+  int co = (ok && !alpha) ? nch : 0, ca = (ok && alpha) ? nch : 0;
+  int io = co, ia = ca;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int v = __shfl_up_sync(FULL, io, o), va = __shfl_up_sync(FULL, ia, o);
+    if (lane >= o) { io += v; ia += va; }
+  }
+  uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
+  uint32_t oo = 0, oa = 0;
+  if (lane == 31) {
+    if (to) oo = atomicAdd(&S.ctr[CTR_SH_ITEMS], to);
+    if (ta) oa = atomicAdd(&S.ctr[CTR_SH_ITEMS_A], ta);
+  }
+  oo = __shfl_sync(FULL, oo, 31) + (uint32_t)(io - co);
+  oa = __shfl_sync(FULL, oa, 31) + (uint32_t)(ia - ca);
+  uint32_t cap_items = S.cap_list * MAX_CHUNKS;
+  for (int c = 0; c < nch; c++) {
+    uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
+    if (!alpha) S.items[oo + c] = item;
+    else S.items[cap_items - 1 - (oa + c)] = item;
+  }
 }
 
 __device__ __forceinline__ void shadow_setup_phase(const ShadowParams &S, const GroupDev *sg, int first, int step) {
@@ -1108,8 +1145,9 @@ __device__ __forceinline__ void shadow_setup_phase(const ShadowParams &S, const 
   for (int base = first; base < S.total_tris; base += step) {
     int t = base + threadIdx.x;
     bool ok, alpha;
-    shadow_classify(sg, S, t, ok, alpha);
-    shadow_append(S, t, ok, alpha, lane);
+    int rows;
+    shadow_classify(sg, S, t, ok, alpha, rows);
+    shadow_append(S, t, ok, alpha, rows, lane);
   }
 }
 
@@ -1210,6 +1248,36 @@ struct ShadowLane {
       v4 = v1 + q * (v3 - v1);
     }
     start_half0();
+    left = y3 - y1 + 1;
+    return true;
+  }
+
+  int left;   // rows left in this lane's chunk (a whole caster: y3 - y1 + 1)
+
+  // advances one row without drawing (the replay up to a chunk's first row)
+  __device__ __forceinline__ void skip_row() {
+    if (half == 0) {
+      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
+      if (ALPHA) { cu1 += su1; cv1 += sv1; cu2 += su2; cv2 += sv2; }
+      cy++;
+      if (cy > y2) start_half1();
+    } else {
+      cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
+      if (ALPHA) { cu1 -= su1; cv1 -= sv1; cu2 -= su2; cv2 -= sv2; }
+      cy--;
+    }
+  }
+
+  // chunk `chunk` of the caster's rows: replays the accumulation up to its
+  // first row, so every interpolant equals the serial walk's
+  __device__ __forceinline__ bool init_chunk(const ShadowParams &S, const GroupDev *sg, uint32_t t, int chunk) {
+    if (!init(S, sg, t)) return false;
+    int rows = left;
+    int cl = chunk_len(rows, S.min_chunk);
+    int first = chunk * cl;
+    if (first >= rows) return false;
+    left = min(cl, rows - first);
+    for (int r = 0; r < first; r++) skip_row();
     return true;
   }
 
@@ -1230,20 +1298,8 @@ struct ShadowLane {
         }
       }
     }
-    if (half == 0) {
-      cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
-      if (ALPHA) { cu1 += su1; cv1 += sv1; cu2 += su2; cv2 += sv2; }
-      cy++;
-      if (cy > y2) {
-        start_half1();
-        live = cy > y2;
-      }
-      return cnt;
-    }
-    cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
-    if (ALPHA) { cu1 -= su1; cv1 -= sv1; cu2 -= su2; cv2 -= sv2; }
-    cy--;
-    live = cy > y2;
+    skip_row();
+    live = --left > 0;
     return cnt;
   }
 };
@@ -1274,7 +1330,10 @@ __device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, con
 template <bool ALPHA>
 __device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const GroupDev *sg, ShadowQ<ALPHA> &q, int lane,
                                                  int ctr_list, int ctr_work) {
-  uint32_t n = S.ctr[ctr_list];
+  // work items: row chunks of the casters when S.items is given, else casters
+  const bool chunked = S.items != nullptr;
+  uint32_t n = chunked ? S.ctr[ALPHA ? CTR_SH_ITEMS_A : CTR_SH_ITEMS] : S.ctr[ctr_list];
+  uint32_t cap_items = S.cap_list * MAX_CHUNKS;
   int dim = S.sh.dim;
   while (true) {
     uint32_t base = 0;
@@ -1285,7 +1344,13 @@ __device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const Gr
     bool live = false;
     if (base + lane < n) {
       uint32_t idx = base + lane;
-      live = L.init(S, sg, S.list[ALPHA ? S.cap_list - 1 - idx : idx]);
+      if (chunked) {
+        uint32_t item = S.items[ALPHA ? cap_items - 1 - idx : idx];
+        uint32_t pos = item >> CHUNK_BITS;
+        live = L.init_chunk(S, sg, S.list[ALPHA ? S.cap_list - 1 - pos : pos], (int)(item & (MAX_CHUNKS - 1)));
+      } else {
+        live = L.init(S, sg, S.list[ALPHA ? S.cap_list - 1 - idx : idx]);
+      }
     }
     for (int round = 0; __any_sync(FULL, live); round++) {
       if (round == LOOP_LIMIT) {

@@ -436,7 +436,7 @@ class ResidentScenes:
         self.total_tris = sum(d["tris"] for d in self.info)
 
 
-MAX_CHUNKS = 3           # small-triangle work items per triangle (kernels.cuh)
+MAX_CHUNKS = 8           # small-triangle work items per triangle (kernels.cuh)
 CTR_WORDS = 32
 
 

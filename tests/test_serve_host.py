@@ -222,7 +222,7 @@ def test_slab_bytes_formula():
     be = SV.GpuBackend.__new__(SV.GpuBackend)
     be.res = R()
     n = be.slab_bytes([(640, 360), (1280, 720)])
-    per_view = 4 * 1000 * 5 + 8 * (1 << 20) + 128
+    per_view = 4 * 1000 * (2 + SV.MAX_CHUNKS) + 8 * (1 << 20) + 128
     assert n == 18 * (640 * 360 + 1280 * 720) + 2 * per_view + (1 << 20)
 
 
