@@ -390,6 +390,44 @@ def scene_small(seed=3, terrain_n=16, spheres=24, nquads=40, tex=64, alpha_tex=6
     return _finish(groups, alphas, shadows)
 
 
+def noise_rgb_fast(rng, n):
+    """n x n RGB uniform noise preprocessed as c*c/8 (uint16), computed in
+    integers (exact: c*c <= 65025), for the large textures of the stress
+    scene."""
+    c = rng.integers(0, 256, (n, n, 3), dtype=np.uint16).astype(np.uint32)
+    return ((c * c) >> 3).astype(np.uint16)
+
+
+def scene_c5(seed=5, terrain_n=2048, spheres=20000, tex=4096, terrain_groups=12, sphere_groups=4,
+             alpha_terrain=(2, 5, 8), alpha_spheres=(0, 2), cascades=(4096, 4096), extent=128.0):
+    """3840x2160 stress scene: a 2048x2048 terrain (8,388,608 tris) in 12
+    row bands plus 20,000 icospheres (1,600,000) in 4 groups = 9,988,608
+    triangles over 16 materials, each with its own 4096^2 trilinear noise
+    texture; 3 terrain bands and 2 sphere groups (29% of the triangles) are
+    alpha-tested against one 4096^2 thresholded-noise mask; two 4096^2
+    cascades (64 and 256 units across)."""
+    rng = np.random.default_rng(seed)
+    cell = 2 * extent / terrain_n
+    xyz, vn, uv = terrain(rng, terrain_n, cell, (-extent, 0.0, -extent), 2.0 * cell)
+    sx, sn, su = icospheres(rng, spheres, 0.2, 1.0, -extent * 0.3, extent * 0.3)
+    amask = (rng.random((tex, tex)) < 0.6).astype(np.uint8)        # alpha 255 (kept) with p = 0.6
+    groups = []
+    f = MIP | SHADOW
+    nt = len(xyz) // 3
+    for k in range(terrain_groups):
+        a, b = 3 * (nt * k // terrain_groups), 3 * (nt * (k + 1) // terrain_groups)
+        fl = f | (ALPHA if k in alpha_terrain else 0)
+        groups.append(_group(xyz[a:b], vn[a:b], uv[a:b], noise_rgb_fast(rng, tex), fl, 0.2))
+    ns = len(sx) // 3
+    for k in range(sphere_groups):
+        a, b = 3 * (ns * k // sphere_groups), 3 * (ns * (k + 1) // sphere_groups)
+        fl = f | CULL | (ALPHA if k in alpha_spheres else 0)
+        groups.append(_group(sx[a:b], sn[a:b], su[a:b], noise_rgb_fast(rng, tex), fl, 0.2))
+    shadows = [ShadowCam.facing(cascades[0], cascades[0] / 2 / 32.0, (0, 0, 0), SUN),
+               ShadowCam.facing(cascades[1], cascades[1] / 2 / 128.0, (0, 0, 0), SUN)]
+    return _finish(groups, [(amask.reshape(-1), tex)], shadows)
+
+
 SERVING_SEEDS = tuple(range(10, 18))
 
 

@@ -340,6 +340,94 @@ def batched_section(steps, device, log=progress):
             "tuning": {k: tuned[k] for k in ("blocks_per_sm", "min_chunk", "ms", "cached")}}
 
 
+# ------------------------------------------------------------------ stress
+
+def stress_section(device, frames=10, log=progress):
+    """Stress workload: 3840x2160, 9,988,608 triangles (2048^2 terrain in 12
+    bands + 20,000 icospheres in 4 groups), 16 trilinear 4096^2 textures, 29%
+    of the triangles alpha-tested, two 4096^2 cascades.  Plain frame (both
+    cascades + drawAll) and the batched launch of the cascades, the main view
+    and six 1024^2 cube faces, each device-timed with CUDA events."""
+    import torch
+    from axi_visualizer_b200 import scenes as S
+    from axi_visualizer_b200.batch import Batch, scene_batch_views
+    from axi_visualizer_b200.ops import SceneRenderer
+
+    log("stress: building scene")
+    t0 = time.perf_counter()
+    sc = S.scene_c5()
+    gen_s = time.perf_counter() - t0
+    w, h = 3840, 2160
+    main = S.default_view(w, h, pos=(0.0, 8.0, -40.0))
+    R = SceneRenderer(sc, w, h, device=device)
+    D = R.draw
+    stream = torch.cuda.ExternalStream(D.stream_ptr(), device=f"cuda:{device}")
+
+    def timed(step, n):
+        for _ in range(2):
+            step()
+        D.sync()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(n + 1)]
+        ev[0].record(stream)
+        for i in range(n):
+            step()
+            ev[i + 1].record(stream)
+        D.sync()
+        return np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(n)])
+
+    log("stress: plain frames")
+    plain = timed(lambda: R.frame(main), frames)
+    st = D.lastStats()
+    log("stress: batched launch")
+    descs = scene_batch_views(sc, main, faces_at=(0.0, 8.0, -30.0), face_side=1024)
+    B = Batch(D, descs)
+    flags = [g.flags for g in sc.groups]
+    aidx = [g.alpha_index for g in sc.groups]
+    batched = timed(lambda: B.render(flags, aidx), frames)
+    graph = B.stats()["graph"]
+    del B
+    log("stress: the same views as plain per-view calls")
+    from axi_visualizer_b200.batch import cube_faces
+    F = SceneRenderer(sc, 1024, 1024, device=device)
+    faces = cube_faces((0.0, 8.0, -30.0), 1024)
+
+    def plain_views():
+        R.frame(main)
+        F.shadow_pass()                 # the plain API keeps shadow maps per handle
+        for fv in faces:
+            F.set_view(fv)
+            F.draw.clearZBuffer()
+            F.draw.drawAll(F.shaders, shadowIds=[0, 1])
+
+    for _ in range(2):
+        plain_views()
+    D.sync()
+    F.draw.sync()
+    t1 = time.perf_counter()
+    for _ in range(frames):
+        plain_views()
+    D.sync()
+    F.draw.sync()
+    plain_views_ms = 1000 * (time.perf_counter() - t1) / frames
+    del F
+    pix = sum(d.w * (d.h if d.kind == 0 else d.w) for d in descs)
+    ntri = sc.ntris
+    alpha = sum(g.ntris for g in sc.groups if g.flags & S.ALPHA) / ntri
+    pm, bm = float(np.median(plain)), float(np.median(batched))
+    return {"workload": "c5_stress_4k_10m_tris", "width": w, "height": h, "triangles": ntri,
+            "materials": len(sc.groups), "texture_side": 4096, "alpha_fraction": round(alpha, 4),
+            "shadow_cascades": [c.dim for c in sc.shadows], "scene_build_s": round(gen_s, 1),
+            "queues": st,
+            "plain": {"frames_per_s": 1000.0 / pm, "ms_per_frame": pm, "p99_ms": float(np.percentile(plain, 99)),
+                      "Mtri_per_s": ntri / pm / 1e3, "Mpix_per_s": w * h / pm / 1e3},
+            "batched": {"views": [f"{'shaded' if d.kind == 0 else 'depth'} {d.w}x{d.h if d.kind == 0 else d.w}"
+                                  for d in descs],
+                        "frames_per_s": 1000.0 / bm, "ms_per_frame": bm, "p99_ms": float(np.percentile(batched, 99)),
+                        "Mpix_per_s": pix / bm / 1e3, "graph": graph, "plain_views_ms": plain_views_ms,
+                        "plain_views_frames_per_s": 1000.0 / plain_views_ms,
+                        "speedup_vs_plain": plain_views_ms / bm}}
+
+
 # ------------------------------------------------------------------ serving
 
 def served_section(device, n_poisson=1000, n_burst=400, rates=(200.0, 1000.0), tuning=None, log=progress):
@@ -459,6 +547,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-stress", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -564,6 +653,11 @@ def main():
         progress("batched multi-view")
         batched = batched_section(min(args.steps, 100), local)
 
+    stress = None
+    if not args.no_stress:
+        progress("stress")
+        stress = stress_section(local)
+
     served = None
     if not args.no_served:
         progress("served")
@@ -596,6 +690,7 @@ def main():
             "cpu_baseline": cpu,
             "batched": batched,
             "served": served,
+            "stress": stress,
         }
         print(json.dumps(line))
     ranks.close()

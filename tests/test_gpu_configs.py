@@ -77,3 +77,33 @@ def test_batched_view_set_equals_single_views():
         for a, w in zip(got, want):
             assert np.array_equal(a.view(np.uint8), w.view(np.uint8)), f"cube face {j}"
     assert B.stats()["graph"]
+
+
+def test_stress_scene_batched_launch_equals_plain_frame():
+    """3840x2160 / 9,988,608 triangles, 16 trilinear 4096^2 textures, 29%
+    alpha-tested, 4096^2 cascades (too large for the oracle to finish in
+    seconds): the batched launch of both cascades, the main view and six
+    1024^2 cube faces gives the main view and the cascades bit for bit as the
+    plain shadowMap + drawAll path, whose arithmetic the smaller cases pin to
+    the oracle."""
+    from axi_visualizer_b200.batch import Batch, scene_batch_views
+    from axi_visualizer_b200.ops import SceneRenderer
+    sc = S.scene_c5()
+    assert sc.ntris == 9_988_608 and len(sc.groups) == 16
+    main = S.default_view(3840, 2160, pos=(0.0, 8.0, -40.0))
+    R = SceneRenderer(sc, 3840, 2160)
+    descs = scene_batch_views(sc, main, faces_at=(0.0, 8.0, -30.0), face_side=1024)
+    B = Batch(R.draw, descs)
+    B.render([g.flags for g in sc.groups], [g.alpha_index for g in sc.groups])
+    R.frame(main)
+    nd = len(sc.shadows)
+    for k in range(nd):
+        assert np.array_equal(B.frame(k).view(np.uint32), R.draw.getSHM(k).view(np.uint32)), f"cascade {k}"
+    want = [x.copy() for x in R.draw.getFrame()]
+    tid, cov = R.draw.getIDs()
+    got = B.frame(nd)
+    for a, w in zip(got, want):
+        assert np.array_equal(a.view(np.uint8), w.view(np.uint8))
+    assert np.array_equal(B.ids(nd)[0], tid)
+    st = R.draw.lastStats()
+    assert st["n_small"] > 1_000_000 and cov.mean() > 0.5

@@ -84,3 +84,19 @@ def test_vert_light_matches_formula():
     s = max(0.0, float(np.float32(vn[0] @ d1)) + 0.5) * 0.66
     assert abs(li[0, 0] - max(0.2, s * 0.5 + max(0.0, float(vn[0] @ S.LIGHT_DIRS[2]) + 0.5) * 0.66 * 0.1)) < 1e-5
     assert (li >= 0.2).all()
+
+
+def test_stress_scene_composition():
+    """The stress scene's layout at a reduced size: 12 terrain bands + 4
+    sphere groups, one texture each, alpha-tested bands 2, 5, 8 and sphere
+    groups 0, 2 against one mask of the texture side; the full size has
+    2 * 2048^2 + 80 * 20000 = 9,988,608 triangles, 29.0% alpha-tested."""
+    sc = S.scene_c5(terrain_n=64, spheres=400, tex=64)
+    assert len(sc.groups) == 16
+    assert sc.ntris == 2 * 64 * 64 + 80 * 400
+    alpha = [k for k, g in enumerate(sc.groups) if g.flags & S.ALPHA]
+    assert alpha == [2, 5, 8, 12, 14]
+    assert all(g.flags & S.MIP and g.tex_size == 6 for g in sc.groups)
+    assert sc.alphas[0][1] == 64 and sc.alphas[0][0].size == 64 * 64
+    full_alpha = (3 * 2 * 2048 * 2048 // 12 + 2 * 20000 * 80 // 4) / (2 * 2048 * 2048 + 80 * 20000)
+    assert abs(full_alpha - 0.29) < 0.001
