@@ -22,7 +22,7 @@ EXPORTS = [
     "axr_shadow_map_noalloc", "axr_batch_create", "axr_batch_set_views", "axr_batch_render",
     "axr_batch_get_frame", "axr_batch_get_ids", "axr_batch_stats", "axr_batch_destroy",
     "axr_batch_set_tuning", "axr_set_tuning", "axr_batch_query", "axr_batch_read_async", "axr_batch_bytes",
-    "axr_clear_color", "axr_batch_phase_times",
+    "axr_clear_color", "axr_batch_phase_times", "axr_batch_set_mode",
 ]
 
 
@@ -85,6 +85,7 @@ _SIGS = {
     "axr_batch_bytes": (i32, [vp, C.POINTER(C.c_int64)]),
     "axr_clear_color": (i32, [vp, i32, i32, i32]),
     "axr_batch_phase_times": (i32, [vp, vp]),
+    "axr_batch_set_mode": (i32, [vp, i32]),
 }
 
 _lib = None

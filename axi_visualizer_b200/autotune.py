@@ -1,11 +1,15 @@
 """Autotuner for the batched renderer's scheduling knobs.
 
 Knobs (none of them changes a result; views stay bit-identical):
+  mode           persistent (one cooperative kernel, grid barriers between the
+                 phases: fewest launches) or phased (one kernel per phase in
+                 the graph, each at its own occupancy, alpha-tested work on a
+                 parallel branch: better for heavy views)
   blocks_per_sm  size of the persistent cooperative grid (1 .. occupancy limit):
                  more blocks hide latency, fewer make the grid barriers cheaper
-  min_chunk      rows per small-triangle work item (8/16/32): finer items
-                 balance big triangles over more lanes, coarser ones repeat
-                 less row replay
+  min_chunk      rows per small-triangle / caster work item (8/16/32): finer
+                 items balance big triangles over more lanes, coarser ones
+                 repeat less row replay
 
 The semantic tile stays 16 px: the reference restarts its interpolants at
 every 16-px tile border, so the tile size is part of the arithmetic that the
@@ -23,6 +27,7 @@ import time
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "axr_tuning.json")
 BLOCKS = (1, 2, 3, 4)
 CHUNKS = (8, 16, 32)
+PERSISTENT, PHASED = 0, 1
 
 
 def _cache_path():
@@ -57,26 +62,29 @@ def _time_renders(batch, flags, aidx, cast, reps):
 
 
 def tune(batch, flags, aidx=None, cast=None, ntris=0, reps=5, gpu="", use_cache=True, log=None):
-    """Sweeps the knobs, applies and returns the fastest {blocks_per_sm, min_chunk, ms}."""
+    """Sweeps the knobs, applies and returns the fastest {mode, blocks_per_sm, min_chunk, ms}."""
     path = _cache_path()
     key = f"{gpu}|{signature(batch, ntris)}"
     cache = _load(path) if use_cache else {}
-    if key in cache:
+    if key in cache and "mode" in cache[key]:
         best = cache[key]
+        batch.set_mode(best["mode"])
         batch.set_tuning(best["blocks_per_sm"], best["min_chunk"])
         return dict(best, cached=True)
     results = []
-    for bps in BLOCKS:
-        for ch in CHUNKS:
-            try:
-                batch.set_tuning(bps, ch)
-            except Exception:
-                continue          # beyond the occupancy limit of this build
-            ms = _time_renders(batch, flags, aidx, cast, reps)
-            results.append({"blocks_per_sm": bps, "min_chunk": ch, "ms": ms})
-            if log:
-                log(f"autotune blocks/SM={bps} chunk={ch}: {ms:.3f} ms")
+    points = [(PERSISTENT, b, c) for b in BLOCKS for c in CHUNKS] + [(PHASED, BLOCKS[-1], c) for c in CHUNKS]
+    for mode, bps, ch in points:
+        try:
+            batch.set_mode(mode)
+            batch.set_tuning(bps, ch)
+        except Exception:
+            continue              # beyond the occupancy limit of this build
+        ms = _time_renders(batch, flags, aidx, cast, reps)
+        results.append({"mode": mode, "blocks_per_sm": bps, "min_chunk": ch, "ms": ms})
+        if log:
+            log(f"autotune mode={'phased' if mode else 'persistent'} blocks/SM={bps} chunk={ch}: {ms:.3f} ms")
     best = min(results, key=lambda r: r["ms"])
+    batch.set_mode(best["mode"])
     batch.set_tuning(best["blocks_per_sm"], best["min_chunk"])
     if use_cache:
         cache = _load(path)

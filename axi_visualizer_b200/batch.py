@@ -17,6 +17,7 @@ from ._lib import ViewDesc, check, lib
 from . import scenes as S
 
 SHADED, DEPTH, SKIP = 0, 1, 2
+PERSISTENT, PHASED = 0, 1
 
 
 def _groups(d, groups):
@@ -154,6 +155,11 @@ class Batch:
         n = C.c_int64()
         check(self._L.axr_batch_bytes(self._h, C.byref(n)), "axr_batch_bytes")
         return n.value
+
+    def set_mode(self, mode):
+        """PERSISTENT (one cooperative kernel) or PHASED (one kernel per phase
+        in the graph); results are identical."""
+        check(self._L.axr_batch_set_mode(self._h, int(mode)), "axr_batch_set_mode")
 
     def set_tuning(self, blocks_per_sm, min_chunk):
         check(self._L.axr_batch_set_tuning(self._h, int(blocks_per_sm), int(min_chunk)), "axr_batch_set_tuning")

@@ -900,7 +900,9 @@ struct axr_batch {
   uint32_t *d_bar = nullptr, *h_bar = nullptr, *h_ctrs = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t cs = nullptr;    // read-back copies
-  cudaEvent_t done = nullptr, read_done = nullptr;
+  cudaStream_t side = nullptr;  // phased form: the alpha-tested branch
+  cudaEvent_t done = nullptr, read_done = nullptr, ev_fork = nullptr, ev_coarse = nullptr, ev_join = nullptr;
+  int mode = AXR_BATCH_PERSISTENT;
   bool graph = false, pending = false, reads = false;
   int grid = 0, per_sm_max = 0, min_chunk = MIN_CHUNK;
   int64_t launches = 0, bytes = 0;
@@ -1067,8 +1069,29 @@ int batch_enqueue(axr_batch *b) {
   B.views = b->d_views; B.nviews = (int)nv;
   B.groups_draw = b->d_gdraw; B.groups_shadow = b->d_gshadow; B.ngroups = BATCH_TABLE;
   B.bar = b->d_bar; B.nblocks = (uint32_t)b->grid;
-  void *args[] = {&B};
-  CK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(b->grid), dim3(128), args, 0, s));
+  if (b->mode == AXR_BATCH_PERSISTENT) {
+    void *args[] = {&B};
+    CK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(b->grid), dim3(128), args, 0, s));
+  } else {
+    // phased: clear, setup | opaque raster -> tiled opaque | (fork) alpha
+    // raster -> (after the coarse units) tiled alpha | (join) fallback, shade
+    int sms = c->sms;
+    kb_clear<<<sms * 8, 256, 0, s>>>(B);
+    kb_setup<<<sms * 8, 256, 0, s>>>(B);
+    CK(cudaEventRecord(b->ev_fork, s));
+    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+    kb_raster<false><<<sms * 8, 128, 0, s>>>(B);
+    CK(cudaEventRecord(b->ev_coarse, s));
+    kb_raster<true><<<sms * 6, 128, 0, b->side>>>(B);
+    CK(cudaStreamWaitEvent(b->side, b->ev_coarse, 0));
+    kb_tiled<true><<<sms * 6, 128, 0, b->side>>>(B);
+    CK(cudaEventRecord(b->ev_join, b->side));
+    kb_tiled<false><<<sms * 8, 128, 0, s>>>(B);
+    CK(cudaStreamWaitEvent(s, b->ev_join, 0));
+    kb_fallback<<<sms * 4, 128, 0, s>>>(B);
+    kb_shade<<<sms * 3, 256, 0, s>>>(B);
+    CK(cudaGetLastError());
+  }
   for (size_t k = 0; k < nv; k++)
     CK(cudaMemcpyAsync(b->h_ctrs + k * CTR_N, b->buf[k].ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(b->h_bar, b->d_bar, sizeof(uint32_t) * BAR_WORDS, cudaMemcpyDeviceToHost, s));
@@ -1158,7 +1181,11 @@ int axr_batch_create(axr_ctx *c, const axr_view_desc *views, int nviews, axr_bat
             cudaMallocHost(&b->h_ctrs, sizeof(uint32_t) * CTR_N * nviews) == cudaSuccess &&
             cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&b->read_done, cudaEventDisableTiming) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) == cudaSuccess;
+            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->ev_coarse, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess;
   if (!ok) rc = fail(AXR_ENOMEM, "batch tables");
   b->bytes += (int64_t)(sizeof(BatchView) * nviews + 2 * sizeof(GroupDev) * ng + sizeof(uint32_t) * BAR_WORDS);
   if (!rc) rc = batch_alloc(b, units0);
@@ -1384,6 +1411,17 @@ int axr_batch_set_tuning(axr_batch *b, int blocks_per_sm, int min_chunk) {
   return 0;
 }
 
+int axr_batch_set_mode(axr_batch *b, int mode) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  if (mode != AXR_BATCH_PERSISTENT && mode != AXR_BATCH_PHASED) return fail(AXR_EINVAL, "batch mode %d", mode);
+  int rc = batch_settle(b);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(b->c->stream));
+  b->mode = mode;
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->graph = false; }
+  return 0;
+}
+
 int axr_set_tuning(axr_ctx *c, int min_chunk) {
   if (!c) return fail(AXR_EINVAL, "null handle");
   if (min_chunk < 1 || min_chunk > 256) return fail(AXR_EINVAL, "chunk rows %d outside [1, 256]", min_chunk);
@@ -1395,7 +1433,11 @@ int axr_batch_destroy(axr_batch *b) {
   if (!b) return 0;
   if (b->c) cudaStreamSynchronize(b->c->stream);
   if (b->cs) { cudaStreamSynchronize(b->cs); cudaStreamDestroy(b->cs); }
+  if (b->side) { cudaStreamSynchronize(b->side); cudaStreamDestroy(b->side); }
   if (b->read_done) cudaEventDestroy(b->read_done);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_coarse) cudaEventDestroy(b->ev_coarse);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   batch_free_buffers(b);
   cudaFree(b->d_views); cudaFree(b->d_gdraw); cudaFree(b->d_gshadow); cudaFree(b->d_bar);

@@ -92,22 +92,18 @@ union WarpQueue {
   ShadowQ<true> sa;
 };
 
-__global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
-  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
-  __shared__ WarpQueue wq[4];
+// ---- the phases, shared by the persistent kernel and the phased graph
+
+__device__ __forceinline__ void load_tables(const BatchParams &B, GroupDev *sgd, GroupDev *sgs) {
   for (int i = threadIdx.x; i < B.ngroups; i += blockDim.x) {
     sgd[i] = B.groups_draw[i];
     sgs[i] = B.groups_shadow[i];
   }
   __syncthreads();
-  stamp(B.bar, 0);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int first = blockIdx.x * blockDim.x, step = gridDim.x * blockDim.x;
-  const int tid = first + threadIdx.x;
-  const int gw = tid >> 5, nw = step >> 5;
-  WarpQueue &q = wq[w];
+}
 
-  // phase 0: clears (clearzb.c regions) and visibility words, counters
+// phase 0: clears (clearzb.c regions) and visibility words, counters
+__device__ __forceinline__ void batch_clear(const BatchParams &B, int tid, int step) {
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind == VIEW_SKIP) continue;
@@ -139,33 +135,73 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
       }
     }
   }
-  if (!grid_sync(B.bar, B.nblocks)) return;
-  stamp(B.bar, 1);
+}
 
-  // phase 1: setup of every view
+// phase 1: setup of every view
+__device__ __forceinline__ void batch_setup(const BatchParams &B, const GroupDev *sgd, const GroupDev *sgs, int first,
+                                            int step) {
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind == VIEW_SHADED) setup_phase(V.dp, sgd + V.goff, first, step);
     else if (V.kind == VIEW_DEPTH) shadow_setup_phase(V.sp, sgs + V.goff, first, step);
   }
-  if (!grid_sync(B.bar, B.nblocks)) return;
-  stamp(B.bar, 2);
+}
 
-  // phase 2: coarse units, small triangles, shadow maps
-  for (int v = 0; v < B.nviews; v++)
-    if (B.views[v].kind == VIEW_SHADED) coarse_loop(B.views[v].dp, sgd + B.views[v].goff, lane);
+// phase 2 for one material kind: (opaque only) coarse units, then the depth
+// maps' casters, then the small triangles of the shaded views
+template <bool ALPHA>
+__device__ __forceinline__ void batch_raster(const BatchParams &B, const GroupDev *sgd, const GroupDev *sgs,
+                                             ShadowQ<ALPHA> &sq, VisQ<ALPHA> &vq, int lane) {
+  if (!ALPHA)
+    for (int v = 0; v < B.nviews; v++)
+      if (B.views[v].kind == VIEW_SHADED) coarse_loop(B.views[v].dp, sgd + B.views[v].goff, lane);
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
-    if (V.kind != VIEW_DEPTH) continue;
-    shadow_warp_loop<false>(V.sp, sgs + V.goff, q.so, lane, CTR_SH_LIST, CTR_SH_WORK);
-    shadow_warp_loop<true>(V.sp, sgs + V.goff, q.sa, lane, CTR_SH_LIST_A, CTR_SH_WORK_A);
+    if (V.kind == VIEW_DEPTH)
+      shadow_warp_loop<ALPHA>(V.sp, sgs + V.goff, sq, lane, ALPHA ? CTR_SH_LIST_A : CTR_SH_LIST,
+                              ALPHA ? CTR_SH_WORK_A : CTR_SH_WORK);
   }
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind == VIEW_SHADED) raster_small_loop<ALPHA>(V.dp, sgd + V.goff, vq, lane);
+  }
+}
+
+// phase 4: shading
+__device__ __forceinline__ void batch_shade(const BatchParams &B, const GroupDev *sgd, int tid, int step) {
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind != VIEW_SHADED) continue;
-    raster_small_loop<true>(V.dp, sgd + V.goff, q.va, lane);
-    raster_small_loop<false>(V.dp, sgd + V.goff, q.vo, lane);
+    int W = V.w, n = V.w * V.h;
+    for (int i = tid; i < n; i += step) {
+      int y = i / W, x = i - y * W;
+      shade_pixel(V.dp, sgd + V.goff, x, y, V.dp.keys[i]);
+    }
   }
+}
+
+__global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
+  __shared__ WarpQueue wq[4];
+  load_tables(B, sgd, sgs);
+  stamp(B.bar, 0);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int first = blockIdx.x * blockDim.x, step = gridDim.x * blockDim.x;
+  const int tid = first + threadIdx.x;
+  const int gw = tid >> 5, nw = step >> 5;
+  WarpQueue &q = wq[w];
+
+  batch_clear(B, tid, step);
+  if (!grid_sync(B.bar, B.nblocks)) return;
+  stamp(B.bar, 1);
+
+  batch_setup(B, sgd, sgs, first, step);
+  if (!grid_sync(B.bar, B.nblocks)) return;
+  stamp(B.bar, 2);
+
+  // phase 2: coarse units, small triangles, shadow maps (alpha-tested first)
+  batch_raster<true>(B, sgd, sgs, q.sa, q.va, lane);
+  batch_raster<false>(B, sgd, sgs, q.so, q.vo, lane);
   if (!grid_sync(B.bar, B.nblocks)) return;
   stamp(B.bar, 3);
 
@@ -180,16 +216,7 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   if (!grid_sync(B.bar, B.nblocks)) return;
   stamp(B.bar, 4);
 
-  // phase 4: shading
-  for (int v = 0; v < B.nviews; v++) {
-    const BatchView &V = B.views[v];
-    if (V.kind != VIEW_SHADED) continue;
-    int W = V.w, n = V.w * V.h;
-    for (int i = tid; i < n; i += step) {
-      int y = i / W, x = i - y * W;
-      shade_pixel(V.dp, sgd + V.goff, x, y, V.dp.keys[i]);
-    }
-  }
+  batch_shade(B, sgd, tid, step);
   // the last block to finish stamps the end
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -200,6 +227,59 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
       reinterpret_cast<uint64_t *>(B.bar + 4)[5] = t;
     }
   }
+}
+
+// ---- phased form: the same phases as separate kernels, captured in one
+// graph; each kernel runs at its own occupancy, and the alpha-tested
+// rasterizers run on a parallel branch of the graph.  No grid barriers.
+
+__global__ void __launch_bounds__(256) kb_clear(BatchParams B) {
+  batch_clear(B, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+__global__ void __launch_bounds__(256) kb_setup(BatchParams B) {
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
+  load_tables(B, sgd, sgs);
+  batch_setup(B, sgd, sgs, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
+}
+
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) kb_raster(BatchParams B) {
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
+  __shared__ union Q { ShadowQ<ALPHA> s; VisQ<ALPHA> v; } qs[4];
+  load_tables(B, sgd, sgs);
+  Q &q = qs[threadIdx.x >> 5];
+  batch_raster<ALPHA>(B, sgd, sgs, q.s, q.v, threadIdx.x & 31);
+}
+
+template <bool ALPHA>
+__global__ void __launch_bounds__(128, ALPHA ? 6 : 8) kb_tiled(BatchParams B) {
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
+  __shared__ VisQ<ALPHA> qs[4];
+  load_tables(B, sgd, sgs);
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind == VIEW_SHADED) raster_tiled_loop<ALPHA>(V.dp, sgd + V.goff, qs[threadIdx.x >> 5], threadIdx.x & 31);
+  }
+}
+
+__global__ void __launch_bounds__(128) kb_fallback(BatchParams B) {
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
+  __shared__ VisQ<false> qo[4];
+  __shared__ VisQ<true> qa[4];
+  load_tables(B, sgd, sgs);
+  int w = threadIdx.x >> 5, tid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int v = 0; v < B.nviews; v++) {
+    const BatchView &V = B.views[v];
+    if (V.kind == VIEW_SHADED)
+      fallback_loop(V.dp, sgd + V.goff, qo[w], qa[w], threadIdx.x & 31, tid >> 5, (gridDim.x * blockDim.x) >> 5);
+  }
+}
+
+__global__ void __launch_bounds__(256, 3) kb_shade(BatchParams B) {
+  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
+  load_tables(B, sgd, sgs);
+  batch_shade(B, sgd, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 }  // namespace axr

@@ -443,12 +443,15 @@ CTR_WORDS = 32
 class GpuBackend:
     """Slabs as axr_batch objects over a ResidentScenes handle."""
 
-    def __init__(self, resident: ResidentScenes, tuning=None, read_depth=True):
+    def __init__(self, resident: ResidentScenes, tuning=None, read_depth=True, mode=1):
         from . import batch as B
         self.B = B
         self.res = resident
         self.scenes = len(resident.scenes)
         self.tuning = tuning
+        # batch.PHASED by default: slabs hold heavy views (50k-1M triangles at
+        # up to 2560x1440), where one kernel per phase beats the persistent one
+        self.mode = mode
         self.read_depth = read_depth
 
     def slab_bytes(self, slots):
@@ -465,6 +468,8 @@ class GpuBackend:
         graph is captured now), its view table and pinned result buffers."""
         skips = [self.B.skip(w, h) for w, h in slots]
         bt = self.B.Batch(self.res.draw, skips)
+        if self.mode is not None:
+            bt.set_mode(self.mode)
         if self.tuning:
             bt.set_tuning(*self.tuning)
         bt.render(self.res.flags, self.res.aidx)

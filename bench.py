@@ -337,7 +337,7 @@ def batched_section(steps, device, log=progress):
             "Mpix_per_s": pix * 1000.0 / batch_ms / 1e6,
             "plain_frames_per_s": 1000.0 / plain_ms, "plain_ms_per_frame": plain_ms,
             "speedup_vs_plain": plain_ms / batch_ms, "graph": st["graph"], "grid_blocks": st["grid"],
-            "tuning": {k: tuned[k] for k in ("blocks_per_sm", "min_chunk", "ms", "cached")}}
+            "tuning": {k: tuned[k] for k in ("mode", "blocks_per_sm", "min_chunk", "ms", "cached")}}
 
 
 # ------------------------------------------------------------------ stress
@@ -383,6 +383,8 @@ def stress_section(device, frames=10, log=progress):
     B = Batch(D, descs)
     flags = [g.flags for g in sc.groups]
     aidx = [g.alpha_index for g in sc.groups]
+    from axi_visualizer_b200 import autotune
+    tuned = autotune.tune(B, flags, aidx, ntris=sc.ntris, reps=3, gpu=torch.cuda.get_device_name(device), log=log)
     batched = timed(lambda: B.render(flags, aidx), frames)
     graph = B.stats()["graph"]
     del B
@@ -423,7 +425,9 @@ def stress_section(device, frames=10, log=progress):
             "batched": {"views": [f"{'shaded' if d.kind == 0 else 'depth'} {d.w}x{d.h if d.kind == 0 else d.w}"
                                   for d in descs],
                         "frames_per_s": 1000.0 / bm, "ms_per_frame": bm, "p99_ms": float(np.percentile(batched, 99)),
-                        "Mpix_per_s": pix / bm / 1e3, "graph": graph, "plain_views_ms": plain_views_ms,
+                        "Mpix_per_s": pix / bm / 1e3, "graph": graph,
+                        "tuning": {k: tuned[k] for k in ("mode", "blocks_per_sm", "min_chunk", "ms", "cached")},
+                        "plain_views_ms": plain_views_ms,
                         "plain_views_frames_per_s": 1000.0 / plain_views_ms,
                         "speedup_vs_plain": plain_views_ms / bm}}
 
@@ -661,7 +665,7 @@ def main():
     served = None
     if not args.no_served:
         progress("served")
-        tun = (batched["tuning"]["blocks_per_sm"], batched["tuning"]["min_chunk"]) if batched else None
+        tun = (batched["tuning"]["blocks_per_sm"], batched["tuning"]["min_chunk"]) if batched else None   # grid, rows
         served = served_section(local, tuning=tun)
 
     cpu = None

@@ -258,6 +258,16 @@ int axr_batch_stats(axr_batch *b, int64_t *renders, int *graph, int *grid);
  * size in blocks per SM (1..occupancy limit) and the minimum number of rows
  * per small-triangle work item.  Results do not depend on them. */
 int axr_batch_set_tuning(axr_batch *b, int blocks_per_sm, int min_chunk);
+
+/* How a render runs: AXR_BATCH_PERSISTENT (default) = one cooperative
+ * persistent kernel whose phases are separated by grid barriers (fewest
+ * launches: best for many small views); AXR_BATCH_PHASED = the same phases
+ * as separate kernels in the captured graph, each at its own occupancy, the
+ * alpha-tested rasterizers on a parallel branch (best for heavy views;
+ * axr_batch_phase_times then reports zeros).  Results do not depend on it. */
+#define AXR_BATCH_PERSISTENT 0
+#define AXR_BATCH_PHASED 1
+int axr_batch_set_mode(axr_batch *b, int mode);
 int axr_set_tuning(axr_ctx *ctx, int min_chunk);
 
 int axr_batch_destroy(axr_batch *b);
