@@ -22,7 +22,8 @@ EXPORTS = [
     "axr_shadow_map_noalloc", "axr_batch_create", "axr_batch_set_views", "axr_batch_render",
     "axr_batch_get_frame", "axr_batch_get_ids", "axr_batch_stats", "axr_batch_destroy",
     "axr_batch_set_tuning", "axr_set_tuning", "axr_batch_query", "axr_batch_read_async", "axr_batch_bytes",
-    "axr_clear_color", "axr_batch_phase_times", "axr_batch_set_mode",
+    "axr_clear_color", "axr_batch_phase_times", "axr_batch_set_mode", "axr_read_frame_async", "axr_wait_frame",
+    "axr_frame_done",
 ]
 
 
@@ -86,6 +87,9 @@ _SIGS = {
     "axr_clear_color": (i32, [vp, i32, i32, i32]),
     "axr_batch_phase_times": (i32, [vp, vp]),
     "axr_batch_set_mode": (i32, [vp, i32]),
+    "axr_read_frame_async": (i32, [vp, vp, vp, vp, vp, C.POINTER(C.c_int64)]),
+    "axr_wait_frame": (i32, [vp, C.c_int64]),
+    "axr_frame_done": (i32, [vp, C.c_int64]),
 }
 
 _lib = None

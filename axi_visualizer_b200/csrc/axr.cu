@@ -98,11 +98,25 @@ struct axr_ctx {
   uint2 *units = nullptr;
   uint32_t cap_units = 0;
   uint32_t *ctr = nullptr;
-  uint32_t *h_ctr = nullptr;  // pinned copy of the counters of the last drawAll
+  // counters of the last two drawAlls (pinned, each with its event); checked
+  // without blocking once their frame has finished
+  uint32_t *h_ring = nullptr;
+  cudaEvent_t ev_ctr[2] = {nullptr, nullptr};
+  bool pend[2] = {false, false};
+  int last_slot = 1;
+  uint32_t *h_ctr = nullptr;  // counters of the last checked drawAll (lastStats)
   GroupDev *d_groups = nullptr;
   Shadow shadows[MAX_SHADOWS];
   int64_t last_kernels = 0;
-  bool pending = false;
+  // asynchronous frame read-back: two device staging slots, a copy stream
+  struct ReadSlot {
+    uint8_t *stage = nullptr;
+    cudaEvent_t staged = nullptr, done = nullptr;
+    int64_t seq = -1;
+    bool busy = false;
+  } rd[2];
+  cudaStream_t s_copy = nullptr;
+  int64_t read_seq = 0;
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
   int min_chunk = MIN_CHUNK;
@@ -153,21 +167,56 @@ void collect_times(axr_ctx *c);
 // overflow (that frame was completed by the fallback kernel).
 int sync_all(axr_ctx *c);
 
+// Checks the counters of drawAll slot k: a raster loop at its safety limit is
+// an error; an overflowed unit queue (that frame was completed by the
+// fallback kernel) grows for the next frames.  blocking = wait for the frame;
+// otherwise an unfinished frame is left for a later check.
+int check_slot(axr_ctx *c, int k, bool blocking) {
+  if (!c->pend[k]) return 0;
+  if (blocking) {
+    CK(cudaEventSynchronize(c->ev_ctr[k]));
+  } else {
+    cudaError_t e = cudaEventQuery(c->ev_ctr[k]);
+    if (e == cudaErrorNotReady) return 0;
+    if (e != cudaSuccess) return fail(AXR_ECUDA, "drawAll: %s", cudaGetErrorString(e));
+  }
+  c->pend[k] = false;
+  const uint32_t *h = c->h_ring + k * CTR_N;
+  memcpy(c->h_ctr, h, sizeof(uint32_t) * CTR_N);
+  if (h[CTR_LIMIT]) return fail(AXR_ECUDA, "a raster loop reached its safety limit; the frame is incomplete");
+  if (h[CTR_OVERFLOW] && h[CTR_UNITS_RESERVED] > c->cap_units) {
+    CK(cudaStreamSynchronize(c->stream));   // frames in flight still use the old queue
+    return grow_units(c, h[CTR_UNITS_RESERVED]);
+  }
+  return 0;
+}
+
+// Checks every drawAll whose frame has finished, oldest first (no waiting).
+int settle_ready(axr_ctx *c) {
+  int older = 1 - c->last_slot;
+  int rc = check_slot(c, older, false);
+  if (!rc && !c->pend[older]) rc = check_slot(c, c->last_slot, false);
+  return rc;
+}
+
+int settle(axr_ctx *c);
+
+// Before queueing more work: checks finished frames without waiting (with
+// per-kernel timing on, everything is synchronised as before).
+int settle_next(axr_ctx *c) {
+  if (!c->tpend.empty()) return settle(c);
+  return settle_ready(c);
+}
+
 int settle(axr_ctx *c) {
   if (!c->tpend.empty()) {
     int rc = sync_all(c);
     if (rc) return rc;
     collect_times(c);
   }
-  if (!c->pending) return 0;
-  CK(cudaStreamSynchronize(c->stream));
-  c->pending = false;
-  if (c->h_ctr[CTR_LIMIT]) {
-    c->h_ctr[CTR_LIMIT] = 0;
-    return fail(AXR_ECUDA, "a raster loop reached its safety limit; the frame is incomplete");
-  }
-  if (c->h_ctr[CTR_OVERFLOW]) return grow_units(c, c->h_ctr[CTR_UNITS_RESERVED]);
-  return 0;
+  int rc = check_slot(c, 1 - c->last_slot, true);
+  if (!rc) rc = check_slot(c, c->last_slot, true);
+  return rc;
 }
 
 int check_ctx(axr_ctx *c) {
@@ -331,7 +380,10 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
       cudaMalloc(&c->bo, n * 2) != cudaSuccess || cudaMalloc(&c->db, n * 4) != cudaSuccess ||
       cudaMalloc(&c->keys, n * 8) != cudaSuccess || cudaMalloc(&c->ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
       cudaMalloc(&c->d_groups, sizeof(GroupDev) * MAX_GROUPS) != cudaSuccess ||
-      cudaMallocHost(&c->h_ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess) {
+      cudaMallocHost(&c->h_ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
+      cudaMallocHost(&c->h_ring, sizeof(uint32_t) * CTR_N * 2) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_ctr[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_ctr[1], cudaEventDisableTiming) != cudaSuccess) {
     rc = fail(AXR_ENOMEM, "framebuffers for %dx%d", w, h);
   }
   // initial tile-unit queue (grows after an overflow); AXR_UNIT_QUEUE overrides
@@ -351,6 +403,7 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
   cudaMemsetAsync(c->keys, 0xff, n * 8, c->stream);
   cudaMemsetAsync(c->ctr, 0, sizeof(uint32_t) * CTR_N, c->stream);
   memset(c->h_ctr, 0, sizeof(uint32_t) * CTR_N);
+  memset(c->h_ring, 0, sizeof(uint32_t) * CTR_N * 2);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     axr_destroy(c);
     return fail(AXR_ECUDA, "initialising framebuffers");
@@ -382,6 +435,16 @@ int axr_destroy(axr_ctx *c) {
   cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items); cudaFree(c->units);
   cudaFree(c->ctr); cudaFree(c->d_groups);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  if (c->h_ring) cudaFreeHost(c->h_ring);
+  for (int k = 0; k < 2; k++) {
+    if (c->ev_ctr[k]) cudaEventDestroy(c->ev_ctr[k]);
+    auto &r = c->rd[k];
+    if (r.done) cudaEventSynchronize(r.done);
+    cudaFree(r.stage);
+    if (r.staged) cudaEventDestroy(r.staged);
+    if (r.done) cudaEventDestroy(r.done);
+  }
+  if (c->s_copy) { cudaStreamSynchronize(c->s_copy); cudaStreamDestroy(c->s_copy); }
   for (auto &p : c->tpend) { c->ev_pool.push_back(p.a); c->ev_pool.push_back(p.b); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -553,7 +616,7 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   if (rc) return rc;
   if (ngroups != (int)c->groups.size()) return fail(AXR_EINVAL, "drawAll with %d groups, handle has %zu", ngroups, c->groups.size());
   if (nshadow < 0 || nshadow > 2) return fail(AXR_EINVAL, "at most two shadow cascades");
-  if ((rc = settle(c))) return rc;
+  if ((rc = settle_next(c))) return rc;
   DrawParams P;
   memset(&P, 0, sizeof P);
   bool any_shadow = false, any_alpha = false;
@@ -618,8 +681,12 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   launch(c, s, "k_shade", [&] { k_shade<<<sgd, sb, 0, s>>>(P); }); nk++;
   for (int k = 0; k < nshadow; k++) CK(cudaEventRecord(c->shadows[shadow_ids[k]].ev_read, s));
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c->h_ctr, c->ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
-  c->pending = true;
+  int slot = 1 - c->last_slot;
+  if (c->pend[slot] && (rc = check_slot(c, slot, true))) return rc;   // the frame before last
+  CK(cudaMemcpyAsync(c->h_ring + slot * CTR_N, c->ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(c->ev_ctr[slot], s));
+  c->pend[slot] = true;
+  c->last_slot = slot;
   c->last_kernels = nk;
   return 0;
 }
@@ -634,6 +701,68 @@ int axr_get_frame(axr_ctx *c, uint16_t *r, uint16_t *g, uint16_t *b, float *dept
   if (depth) CK(cudaMemcpyAsync(depth, c->db, n * 4, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return settle(c);
+}
+
+int axr_read_frame_async(axr_ctx *c, uint16_t *r, uint16_t *g, uint16_t *b, float *depth, int64_t *ticket) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!ticket) return fail(AXR_EINVAL, "null ticket");
+  if ((rc = settle_next(c))) return rc;
+  size_t n = (size_t)c->w * c->h;
+  if (!c->s_copy) CK(cudaStreamCreateWithFlags(&c->s_copy, cudaStreamNonBlocking));
+  axr_ctx::ReadSlot &sl = c->rd[c->read_seq & 1];
+  if (sl.busy) {                       // the read two calls ago still holds this slot
+    CK(cudaEventSynchronize(sl.done));
+    sl.busy = false;
+  }
+  if (!sl.stage) {
+    if (cudaMalloc(&sl.stage, n * 10) != cudaSuccess) return fail(AXR_ENOMEM, "frame staging buffer");
+    CK(cudaEventCreateWithFlags(&sl.staged, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+  }
+  // device copies on the render stream (ordered before the next frame's
+  // writes), then the device-to-host copies on the copy stream
+  uint16_t *sr = (uint16_t *)sl.stage, *sg = sr + n, *sb = sg + n;
+  float *sd = (float *)(sb + n);
+  cudaStream_t s = c->stream;
+  if (r) CK(cudaMemcpyAsync(sr, c->ro, n * 2, cudaMemcpyDeviceToDevice, s));
+  if (g) CK(cudaMemcpyAsync(sg, c->go, n * 2, cudaMemcpyDeviceToDevice, s));
+  if (b) CK(cudaMemcpyAsync(sb, c->bo, n * 2, cudaMemcpyDeviceToDevice, s));
+  if (depth) CK(cudaMemcpyAsync(sd, c->db, n * 4, cudaMemcpyDeviceToDevice, s));
+  CK(cudaEventRecord(sl.staged, s));
+  CK(cudaStreamWaitEvent(c->s_copy, sl.staged, 0));
+  if (r) CK(cudaMemcpyAsync(r, sr, n * 2, cudaMemcpyDeviceToHost, c->s_copy));
+  if (g) CK(cudaMemcpyAsync(g, sg, n * 2, cudaMemcpyDeviceToHost, c->s_copy));
+  if (b) CK(cudaMemcpyAsync(b, sb, n * 2, cudaMemcpyDeviceToHost, c->s_copy));
+  if (depth) CK(cudaMemcpyAsync(depth, sd, n * 4, cudaMemcpyDeviceToHost, c->s_copy));
+  CK(cudaEventRecord(sl.done, c->s_copy));
+  sl.busy = true;
+  sl.seq = c->read_seq;
+  *ticket = c->read_seq++;
+  return 0;
+}
+
+int axr_wait_frame(axr_ctx *c, int64_t ticket) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (ticket < 0 || ticket >= c->read_seq) return fail(AXR_EINVAL, "no read with ticket %lld", (long long)ticket);
+  axr_ctx::ReadSlot &sl = c->rd[ticket & 1];
+  if (sl.seq == ticket && sl.busy) {   // (an older ticket finished before its slot was reused)
+    CK(cudaEventSynchronize(sl.done));
+    sl.busy = false;
+  }
+  return settle_next(c);
+}
+
+int axr_frame_done(axr_ctx *c, int64_t ticket) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  if (ticket < 0 || ticket >= c->read_seq) return fail(AXR_EINVAL, "no read with ticket %lld", (long long)ticket);
+  axr_ctx::ReadSlot &sl = c->rd[ticket & 1];
+  if (sl.seq != ticket || !sl.busy) return 1;
+  cudaError_t e = cudaEventQuery(sl.done);
+  if (e == cudaErrorNotReady) return 0;
+  if (e != cudaSuccess) return fail(AXR_ECUDA, "frame read: %s", cudaGetErrorString(e));
+  return 1;
 }
 
 int axr_get_ids(axr_ctx *c, int32_t *tri_id, uint8_t *cov) {
@@ -733,7 +862,7 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   if (rc) return rc;
   if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
   if (ngroups != (int)c->groups.size() || !cast) return fail(AXR_EINVAL, "shadowMap arguments");
-  if ((rc = settle(c))) return rc;
+  if ((rc = settle_next(c))) return rc;
   // alpha casters use the alpha mask's own side as lenT (drawminalpha.c:86-96)
   std::vector<int32_t> fl(ngroups, 0);
   for (int g = 0; g < ngroups; g++) fl[g] = flags ? (flags[g] & (F_ALPHA | F_MIP)) : 0;

@@ -173,6 +173,32 @@ class CLDraw:
         check(self._L.axr_get_frame(self._h, _p(self.hro), _p(self.hgo), _p(self.hbo), _p(self.hdb)), "getFrame")
         return (self.hro, self.hgo, self.hbo, self.hdb)
 
+    def readFrameAsync(self):
+        """Starts reading the current frame back without waiting (new: the
+        reference's getFrame blocks).  Returns a ticket for waitFrame.  The
+        frame lands in one of two host buffer sets, reused every second read."""
+        if not hasattr(self, "_ring"):
+            self._ring = [tuple(self._host((self.H, self.W), t) for t in (np.uint16,) * 3 + (np.float32,))
+                          for _ in range(2)]
+            self._ring_next = 0
+        bufs = self._ring[self._ring_next]
+        t = C.c_int64()
+        check(self._L.axr_read_frame_async(self._h, *[_p(a) for a in bufs], C.byref(t)), "readFrameAsync")
+        self._ring_next ^= 1
+        return (t.value, bufs)
+
+    def waitFrame(self, ticket):
+        """Blocks until the read `ticket` is on the host; returns (r, g, b, depth)."""
+        tk, bufs = ticket
+        check(self._L.axr_wait_frame(self._h, tk), "waitFrame")
+        return bufs
+
+    def frameDone(self, ticket):
+        rc = self._L.axr_frame_done(self._h, ticket[0])
+        if rc < 0:
+            check(rc, "frameDone")
+        return rc == 1
+
     def getIDs(self):
         tid = np.empty((self.H, self.W), np.int32)
         cov = np.empty((self.H, self.W), np.uint8)

@@ -37,8 +37,8 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
-# each kernel on this workload, from the ncu capture summarised in
-# profiles/ncu_kernels_1080p_1m.md; None until captured.
+# each kernel on this workload, from the ncu capture summarised under
+# profiles/; None until captured.
 NCU_TRAFFIC = {"k_raster_small": 33005312, "k_raster_small_alpha": 13483264,
                "k_shadow_raster": 43307520 + 2304, "k_shadow_raster_alpha": 9635584,
                "k_shade": 30226944 + 503808}
@@ -109,8 +109,8 @@ class Clocks:
 # ------------------------------------------------------------------ roofline bookkeeping
 
 def algorithmic_bytes(scene, stats, visible_tris):
-    """Lower-bound bytes each kernel must move per launch:
-    geometry it has to read once, framebuffer/map bytes it has to write once."""
+    """Lower-bound bytes each kernel must move per launch: the geometry it has
+    to read once and the framebuffer / map bytes it has to write once."""
     T = scene.ntris
     cull_T = sum(g.ntris for g in scene.groups if g.flags & 8)
     alpha_T = sum(g.ntris for g in scene.groups if g.flags & 2)
@@ -636,18 +636,42 @@ def main():
     D.sync()
     t0 = time.perf_counter()
     e2e_lat = []
-    for i in range(args.steps):
-        t1 = time.perf_counter()
+
+    def render_step():
         R.shadow_pass()
         D.setScaleCull(view.sscale, view.cax, view.cay)
         D.setPos(pose[:3])
         D.setVM(pose[3:].reshape(3, 3))
         D.clearZBuffer()
         D.drawAll(R.shaders, shadowIds=[0, 1])
-        D.getFrame()                      # D2H of colour planes + depth into pinned buffers (synchronises)
-        e2e_lat.append(time.perf_counter() - t1)
+
+    # frame loop with the asynchronous read-back: frame i's colour planes and
+    # depth travel to pinned host memory while frame i + 1 renders
+    prev = None
+    for i in range(args.steps):
+        t1 = time.perf_counter()
+        render_step()
+        tk = D.readFrameAsync()
+        if prev is not None:
+            D.waitFrame(prev[0])
+            e2e_lat.append(time.perf_counter() - prev[1])
+        prev = (tk, t1)
+    D.waitFrame(prev[0])
+    e2e_lat.append(time.perf_counter() - prev[1])
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_fps = whole_job_rate(args.steps, world, e2e_s)
+    # the same with the blocking getFrame of the reference's API
+    barrier()
+    D.sync()
+    t0 = time.perf_counter()
+    blk_lat = []
+    for i in range(args.steps):
+        t1 = time.perf_counter()
+        render_step()
+        D.getFrame()                      # D2H of colour planes + depth into pinned buffers (synchronises)
+        blk_lat.append(time.perf_counter() - t1)
+    blk_s = max_over_ranks(time.perf_counter() - t0)
+    blk_fps = whole_job_rate(args.steps, world, blk_s)
     d2h = W * H * (3 * 2 + 4)
     h2d = 12 * 4 + 3 * 4 + 3 * len(scene.groups) * 96   # pose + scale/cull + 3 group tables per frame
 
@@ -684,7 +708,10 @@ def main():
             "Mtri_per_s": scene.ntris * fps / 1e6, "Mpix_per_s": W * H * fps / 1e6,
             "p50_ms": float(np.percentile(frame_ms, 50)), "p99_ms": float(np.percentile(frame_ms, 99)),
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "p50_ms": 1000 * float(np.percentile(e2e_lat, 50)), "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
+                    "p50_ms": 1000 * float(np.percentile(e2e_lat, 50)), "p99_ms": 1000 * float(np.percentile(e2e_lat, 99)),
+                    "read_back": "readFrameAsync / waitFrame (next frame renders during the copy)",
+                    "blocking_getFrame": {"value": blk_fps, "p50_ms": 1000 * float(np.percentile(blk_lat, 50)),
+                                          "p99_ms": 1000 * float(np.percentile(blk_lat, 99))}},
             "gpu_launches": int(gpu_launches),
             "roofline": roofline,
             "frame_roofline": frame_roof,

@@ -92,6 +92,19 @@ int axr_set_primary_light(axr_ctx *ctx, const float dir_int[3], const float dir_
 int axr_set_pos(axr_ctx *ctx, const float pos[3]);
 int axr_set_vm(axr_ctx *ctx, const float vm[9]);
 
+/* Asynchronous read-back of the frame (colour planes and/or depth; NULL
+ * skips a plane) for frame loops: the frame is copied on the device into one
+ * of two staging slots, ordered before the next frame's writes, then to the
+ * host on a copy stream while later frames render.  Host buffers should be
+ * pinned (pageable ones make the copy synchronous).  *ticket names the read;
+ * axr_wait_frame blocks until it is on the host, axr_frame_done polls (1 =
+ * done).  A third read waits for the first, whose slot it reuses, so keep
+ * at most two reads in flight per set of host buffers.  New (the reference's
+ * getFrame is synchronous). */
+int axr_read_frame_async(axr_ctx *ctx, uint16_t *r, uint16_t *g, uint16_t *b, float *depth, int64_t *ticket);
+int axr_wait_frame(axr_ctx *ctx, int64_t ticket);
+int axr_frame_done(axr_ctx *ctx, int64_t ticket);
+
 /* CLDraw.clearZBuffer() (Ops0.py:650-653, clearzb.c): depth := 65535 on the
  * [0, w/4*4) x [0, h/4*4) region the reference's 4x4 work-items cover. */
 int axr_clear_zbuffer(axr_ctx *ctx);

@@ -126,3 +126,33 @@ def test_row_chunking_does_not_change_the_frame():
     for f in frames[1:]:
         for a, b in zip(f, frames[0]):
             assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_async_frame_read_equals_get_frame():
+    """readFrameAsync / waitFrame deliver the same frame as getFrame, also
+    with two reads in flight and the next frames rendering meanwhile."""
+    sc = S.scene_small(seed=2, flags=S.MIP | S.SHADOW)
+    views = [S.default_view(256, 192, pos=p) for p in ((1, 3, -12), (4, 2, -9), (-3, 5, -10))]
+    from axi_visualizer_b200.ops import SceneRenderer
+    R = SceneRenderer(sc, 256, 192, pinned=True)
+    want = []
+    for v in views:
+        R.draw.clearColor((1, 1, 1))           # uncovered pixels would keep the previous frame's colour
+        R.frame(v)
+        want.append([x.copy() for x in R.draw.getFrame()])
+    tickets = []
+    for rep in range(2):
+        for k, v in enumerate(views):
+            R.draw.clearColor((1, 1, 1))
+            R.frame(v)
+            tickets.append((k, R.draw.readFrameAsync()))
+            if len(tickets) >= 2:              # at most two reads in flight
+                kk, t = tickets.pop(0)
+                got = R.draw.waitFrame(t)
+                for a, b in zip(got, want[kk]):
+                    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    for kk, t in tickets:
+        got = R.draw.waitFrame(t)
+        assert R.draw.frameDone(t)
+        for a, b in zip(got, want[kk]):
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
