@@ -1416,6 +1416,10 @@ int axr_batch_render(axr_batch *b, const int32_t *flags, const int32_t *alpha_in
   }
   b->launches++;
   c->launches++;
+  // the handle's shadow maps this render sampled: it is their last reader
+  for (auto &v : b->desc)
+    for (int j = 0; j < v.ncascades; j++)
+      if (v.kind == AXR_VIEW_SHADED && v.cascades[j] < 0) CK(cudaEventRecord(c->shadows[-1 - v.cascades[j]].ev_read, c->stream));
   CK(cudaEventRecord(b->done, c->stream));
   b->pending = true;
   return 0;
