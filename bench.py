@@ -39,9 +39,9 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
 # each kernel on this workload, from the ncu capture summarised under
 # profiles/; None until captured.
-NCU_TRAFFIC = {"k_raster_small": 33005312, "k_raster_small_alpha": 13483264,
-               "k_shadow_raster": 43307520 + 2304, "k_shadow_raster_alpha": 9635584,
-               "k_shade": 30226944 + 503808}
+NCU_TRAFFIC = {"k_raster_small": 33614848, "k_raster_small_alpha": 13604608,
+               "k_shadow_raster": 48411392 + 18432, "k_shadow_raster_alpha": 10116608,
+               "k_shade": 30231296 + 1395968}
 
 
 def progress(msg):
