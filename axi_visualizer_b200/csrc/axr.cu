@@ -117,6 +117,15 @@ struct axr_ctx {
   } rd[2];
   cudaStream_t s_copy = nullptr;
   int64_t read_seq = 0;
+  // pinned staging of the per-call group tables: a host-to-device copy from
+  // pageable memory would first synchronise its stream, i.e. wait for the
+  // previous frame; a slot is reused only after the copy that read it ran
+  struct Stage {
+    GroupDev *h = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool used = false;
+  } stage[8];
+  int stage_next = 0;
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
   int min_chunk = MIN_CHUNK;
@@ -341,13 +350,31 @@ int group_table(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, co
   return 0;
 }
 
+// Copies a group table to the device on stream s through the pinned ring.
+int upload_table(axr_ctx *c, GroupDev *dst, const GroupDev *tab, int n, cudaStream_t s) {
+  axr_ctx::Stage &st = c->stage[c->stage_next];
+  c->stage_next = (c->stage_next + 1) % 8;
+  if (!st.h) {
+    if (cudaMallocHost(&st.h, sizeof(GroupDev) * MAX_GROUPS) != cudaSuccess) return fail(AXR_ENOMEM, "group table");
+    CK(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
+  } else if (st.used) {
+    CK(cudaEventSynchronize(st.ev));
+  }
+  memcpy(st.h, tab, sizeof(GroupDev) * n);
+  CK(cudaMemcpyAsync(dst, st.h, sizeof(GroupDev) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(st.ev, s));
+  st.used = true;
+  return 0;
+}
+
 // Builds the per-call group table on the device.
 int upload_groups(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *enabled_mask,
                   bool mask_means_enabled, int ngroups) {
   GroupDev tab[MAX_GROUPS];
   int rc = group_table(c, flags, alpha_index, enabled_mask, mask_means_enabled, ngroups, tab);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(c->d_groups, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, c->stream));
+  rc = upload_table(c, c->d_groups, tab, std::max(ngroups, 1), c->stream);
+  if (rc) return rc;
   return 0;
 }
 
@@ -445,6 +472,10 @@ int axr_destroy(axr_ctx *c) {
     if (r.done) cudaEventDestroy(r.done);
   }
   if (c->s_copy) { cudaStreamSynchronize(c->s_copy); cudaStreamDestroy(c->s_copy); }
+  for (auto &st : c->stage) {
+    if (st.ev) { cudaEventSynchronize(st.ev); cudaEventDestroy(st.ev); }
+    if (st.h) cudaFreeHost(st.h);
+  }
   for (auto &p : c->tpend) { c->ev_pool.push_back(p.a); c->ev_pool.push_back(p.b); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -894,7 +925,7 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
     sm.cap = c->cap_list;
   }
   CK(cudaStreamWaitEvent(sm.st, sm.ev_read, 0));
-  CK(cudaMemcpyAsync(sm.tab, tab, sizeof(GroupDev) * std::max(ngroups, 1), cudaMemcpyHostToDevice, sm.st));
+  if ((rc = upload_table(c, sm.tab, tab, std::max(ngroups, 1), sm.st))) return rc;
   ShadowParams S;
   memset(&S, 0, sizeof S);
   S.groups = sm.tab; S.ngroups = ngroups; S.total_tris = c->total_tris;

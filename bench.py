@@ -634,7 +634,6 @@ def main():
     pose[:3] = view.pos
     pose[3:] = view.vv.reshape(-1)
     D.sync()
-    t0 = time.perf_counter()
     e2e_lat = []
 
     def render_step():
@@ -646,7 +645,14 @@ def main():
         D.drawAll(R.shaders, shadowIds=[0, 1])
 
     # frame loop with the asynchronous read-back: frame i's colour planes and
-    # depth travel to pinned host memory while frame i + 1 renders
+    # depth travel to pinned host memory while frame i + 1 renders (the
+    # untimed warm-up makes the pinned host ring and the staging slots)
+    for i in range(args.warmup):
+        render_step()
+        D.waitFrame(D.readFrameAsync())
+    D.sync()
+    barrier()
+    t0 = time.perf_counter()
     prev = None
     for i in range(args.steps):
         t1 = time.perf_counter()
