@@ -159,6 +159,8 @@ class Server:
         self.launch_sizes: list[int] = []
         self.max_inflight = 0
         self.alloc_failures = 0
+        self.low_memory = 0
+        self.hbm_reserve = 1 << 30        # free HBM kept back when making a slab
         self._next_alloc = -math.inf
         self._sid = 0
 
@@ -233,6 +235,10 @@ class Server:
         if len([s for s in self.slabs if s.state != "retired"]) >= self.max_slabs:
             return None
         if self.used + self.slab_bytes > self.budget or (now < self._next_alloc and not force):
+            return None
+        free = getattr(self.b, "free_bytes", None)
+        if free is not None and free() < self.slab_bytes + self.hbm_reserve:
+            self.low_memory += 1          # the device has less free HBM than the budget assumed
             return None
         try:
             h = self.b.create(self.slot_list)
@@ -347,7 +353,7 @@ class Server:
             "max_inflight": self.max_inflight,
             "slabs": len(self.slabs), "slab_bytes": self.slab_bytes,
             "hbm_used_peak_bytes": self.peak, "hbm_budget_bytes": self.budget, "resident_bytes": self.resident,
-            "alloc_failures": self.alloc_failures,
+            "alloc_failures": self.alloc_failures, "low_memory_skips": self.low_memory,
         }
 
 
@@ -453,6 +459,11 @@ class GpuBackend:
         # up to 2560x1440), where one kernel per phase beats the persistent one
         self.mode = mode
         self.read_depth = read_depth
+
+    def free_bytes(self):
+        """Free HBM on the device right now (other processes may hold some)."""
+        import torch
+        return torch.cuda.mem_get_info(self.res.device)[0]
 
     def slab_bytes(self, slots):
         """Device bytes of a slab: framebuffers (3 x u16 colour, f32 depth,

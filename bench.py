@@ -340,6 +340,38 @@ def batched_section(steps, device, log=progress):
             "tuning": {k: tuned[k] for k in ("mode", "blocks_per_sm", "min_chunk", "ms", "cached")}}
 
 
+# ------------------------------------------------------------------ 640x480
+
+def small_section(device, frames=300):
+    """The 640x480 scene (64x64 terrain + 200 icospheres = 24,192 triangles,
+    one 512^2 trilinear texture, one 1024^2 shadow map): frames/s of shadow
+    pass + drawAll, device-timed with CUDA events; a launch-bound frame."""
+    import torch
+    from axi_visualizer_b200 import scenes as S
+    from axi_visualizer_b200.ops import SceneRenderer
+    sc = S.scene_c1()
+    view = S.default_view(640, 480)
+    R = SceneRenderer(sc, 640, 480, device=device)
+    stream = torch.cuda.ExternalStream(R.draw.stream_ptr(), device=f"cuda:{device}")
+    for _ in range(10):
+        R.frame(view)
+    R.draw.sync()
+    launches0 = R.draw.launchCount()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(frames + 1)]
+    ev[0].record(stream)
+    for i in range(frames):
+        R.frame(view)
+        ev[i + 1].record(stream)
+    R.draw.sync()
+    launches = (R.draw.launchCount() - launches0) / frames
+    per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(frames)])
+    ms = ev[0].elapsed_time(ev[-1]) / frames
+    return {"workload": "c1_plain_640x480_24k_tris", "triangles": sc.ntris, "frames_per_s": 1000.0 / ms,
+            "ms_per_frame": ms, "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+            "Mtri_per_s": sc.ntris / ms / 1e3, "Mpix_per_s": 640 * 480 / ms / 1e3,
+            "launches_per_frame": launches}
+
+
 # ------------------------------------------------------------------ stress
 
 def stress_section(device, frames=10, log=progress):
@@ -552,6 +584,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-stress", action="store_true")
+    ap.add_argument("--no-small", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -681,19 +714,26 @@ def main():
     d2h = W * H * (3 * 2 + 4)
     h2d = 12 * 4 + 3 * 4 + 3 * len(scene.groups) * 96   # pose + scale/cull + 3 group tables per frame
 
-    progress("cpu baseline")
+    # the added sections are per-GPU measurements: rank 0 runs them (the
+    # other replicas are done once the whole-job numbers above are taken)
+    extra = rank == 0
+    small = None
+    if extra and not args.no_small:
+        progress("640x480 scene")
+        small = small_section(local)
+
     batched = None
-    if not args.no_batched:
+    if extra and not args.no_batched:
         progress("batched multi-view")
         batched = batched_section(min(args.steps, 100), local)
 
     stress = None
-    if not args.no_stress:
+    if extra and not args.no_stress:
         progress("stress")
         stress = stress_section(local)
 
     served = None
-    if not args.no_served:
+    if extra and not args.no_served:
         progress("served")
         tun = (batched["tuning"]["blocks_per_sm"], batched["tuning"]["min_chunk"]) if batched else None   # grid, rows
         served = served_section(local, tuning=tun)
@@ -728,6 +768,7 @@ def main():
             "batched": batched,
             "served": served,
             "stress": stress,
+            "small": small,
         }
         print(json.dumps(line))
     ranks.close()

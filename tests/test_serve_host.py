@@ -158,6 +158,23 @@ def test_rejects_what_can_never_be_served():
     assert tiny.requests[0].status == "rejected" and "budget" in tiny.requests[0].error
 
 
+def test_admission_checks_free_device_memory():
+    """Besides the budget, a slab is made only while the device reports
+    enough free HBM (another process may hold memory)."""
+    be = FakeBackend()
+    free = {"bytes": 10 ** 12}
+    be.free_bytes = lambda: free["bytes"]
+    srv = SV.Server(be, budget_bytes=1e9, layout={RES[0]: 1}, max_slabs=4)
+    srv.hbm_reserve = 1000
+    free["bytes"] = 500                                    # below slab + reserve
+    srv.submit(req(0), 0.0)
+    srv.step(0.0)
+    assert len(be.created) == 0 and srv.requests[0].status == "queued" and srv.low_memory == 1
+    free["bytes"] = 10 ** 12
+    drive(srv, 1.0, 0.01)
+    assert srv.requests[0].status == "done" and len(be.created) == 1
+
+
 def test_allocation_failure_is_retried():
     be = FakeBackend(fail_creates=2)
     srv = SV.Server(be, budget_bytes=1e9, layout={RES[0]: 1}, retry_after=0.05)
