@@ -23,7 +23,7 @@ EXPORTS = [
     "axr_batch_get_frame", "axr_batch_get_ids", "axr_batch_stats", "axr_batch_destroy",
     "axr_batch_set_tuning", "axr_set_tuning", "axr_batch_query", "axr_batch_read_async", "axr_batch_bytes",
     "axr_clear_color", "axr_batch_phase_times", "axr_batch_set_mode", "axr_read_frame_async", "axr_wait_frame",
-    "axr_frame_done",
+    "axr_frame_done", "axr_batch_inject_barrier_stall",
 ]
 
 
@@ -90,6 +90,7 @@ _SIGS = {
     "axr_read_frame_async": (i32, [vp, vp, vp, vp, vp, C.POINTER(C.c_int64)]),
     "axr_wait_frame": (i32, [vp, C.c_int64]),
     "axr_frame_done": (i32, [vp, C.c_int64]),
+    "axr_batch_inject_barrier_stall": (i32, [vp, i32, C.c_longlong]),
 }
 
 _lib = None

@@ -161,6 +161,14 @@ class Batch:
         in the graph); results are identical."""
         check(self._L.axr_batch_set_mode(self._h, int(mode)), "axr_batch_set_mode")
 
+    def inject_barrier_stall(self, phantom_blocks, spin_limit=1 << 26):
+        """Fault injection for failure-detection tests (persistent form): the
+        grid barriers of the next renders wait for `phantom_blocks` blocks
+        that never run and give up after `spin_limit` polls, so the render
+        reports an error instead of hanging.  (0, 1 << 26) restores it."""
+        check(self._L.axr_batch_inject_barrier_stall(self._h, int(phantom_blocks), int(spin_limit)),
+              "axr_batch_inject_barrier_stall")
+
     def set_tuning(self, blocks_per_sm, min_chunk):
         check(self._L.axr_batch_set_tuning(self._h, int(blocks_per_sm), int(min_chunk)), "axr_batch_set_tuning")
 

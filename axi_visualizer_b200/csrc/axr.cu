@@ -1063,6 +1063,8 @@ struct axr_batch {
   cudaStream_t side = nullptr;  // phased form: the alpha-tested branch
   cudaEvent_t done = nullptr, read_done = nullptr, ev_fork = nullptr, ev_coarse = nullptr, ev_join = nullptr;
   int mode = AXR_BATCH_PERSISTENT;
+  int phantom = 0;                  // fault injection: barrier waits for blocks never launched
+  long spin_limit = BARRIER_SPIN_LIMIT;
   bool graph = false, pending = false, reads = false;
   int grid = 0, per_sm_max = 0, min_chunk = MIN_CHUNK;
   int64_t launches = 0, bytes = 0;
@@ -1228,7 +1230,7 @@ int batch_enqueue(axr_batch *b) {
   BatchParams B;
   B.views = b->d_views; B.nviews = (int)nv;
   B.groups_draw = b->d_gdraw; B.groups_shadow = b->d_gshadow; B.ngroups = BATCH_TABLE;
-  B.bar = b->d_bar; B.nblocks = (uint32_t)b->grid;
+  B.bar = b->d_bar; B.nblocks = (uint32_t)(b->grid + b->phantom); B.spin_limit = b->spin_limit;
   if (b->mode == AXR_BATCH_PERSISTENT) {
     void *args[] = {&B};
     CK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(b->grid), dim3(128), args, 0, s));
@@ -1582,6 +1584,19 @@ int axr_batch_set_mode(axr_batch *b, int mode) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(b->c->stream));
   b->mode = mode;
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->graph = false; }
+  return 0;
+}
+
+int axr_batch_inject_barrier_stall(axr_batch *b, int phantom_blocks, long long spin_limit) {
+  if (!b) return fail(AXR_EINVAL, "null batch");
+  if (phantom_blocks < 0 || phantom_blocks > 1024) return fail(AXR_EINVAL, "phantom blocks %d", phantom_blocks);
+  if (spin_limit < 1 || spin_limit > BARRIER_SPIN_LIMIT) return fail(AXR_EINVAL, "spin limit %lld", spin_limit);
+  int rc = batch_settle(b);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(b->c->stream));
+  b->phantom = phantom_blocks;
+  b->spin_limit = (long)spin_limit;
   if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->graph = false; }
   return 0;
 }

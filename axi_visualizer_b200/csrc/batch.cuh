@@ -38,7 +38,8 @@ struct BatchParams {
   int ngroups;
   uint32_t *bar;     // [0] arrivals, [1] generation, [2] barrier error, [3] blocks done,
                      // [4..15] six u64 globaltimer stamps: start, after phases 0-3, end
-  uint32_t nblocks;
+  uint32_t nblocks;    // blocks the grid barrier waits for
+  long spin_limit;     // polls before a waiting block gives up
 };
 
 constexpr int BAR_WORDS = 16;
@@ -54,9 +55,10 @@ __device__ __forceinline__ void stamp(uint32_t *bar, int k) {
 constexpr long BARRIER_SPIN_LIMIT = 1L << 26;   // ~6 s of polling, then give up
 
 // Grid-wide barrier of a cooperative launch (all blocks are co-resident).  A
-// block that polls longer than BARRIER_SPIN_LIMIT records an error and the
-// kernel ends; returns false when the batch must stop.
-__device__ __forceinline__ bool grid_sync(uint32_t *bar, uint32_t nblocks) {
+// block that polls longer than spin_limit (BARRIER_SPIN_LIMIT by default)
+// records an error and the kernel ends; returns false when the batch must
+// stop.
+__device__ __forceinline__ bool grid_sync(uint32_t *bar, uint32_t nblocks, long spin_limit) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -71,7 +73,7 @@ __device__ __forceinline__ bool grid_sync(uint32_t *bar, uint32_t nblocks) {
     } else {
       long it = 0;
       while (*vgen == gen) {
-        if (++it > BARRIER_SPIN_LIMIT) {
+        if (++it > spin_limit) {
           atomicOr(bar + 2, 1u);
           break;
         }
@@ -192,17 +194,17 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   WarpQueue &q = wq[w];
 
   batch_clear(B, tid, step);
-  if (!grid_sync(B.bar, B.nblocks)) return;
+  if (!grid_sync(B.bar, B.nblocks, B.spin_limit)) return;
   stamp(B.bar, 1);
 
   batch_setup(B, sgd, sgs, first, step);
-  if (!grid_sync(B.bar, B.nblocks)) return;
+  if (!grid_sync(B.bar, B.nblocks, B.spin_limit)) return;
   stamp(B.bar, 2);
 
   // phase 2: coarse units, small triangles, shadow maps (alpha-tested first)
   batch_raster<true>(B, sgd, sgs, q.sa, q.va, lane);
   batch_raster<false>(B, sgd, sgs, q.so, q.vo, lane);
-  if (!grid_sync(B.bar, B.nblocks)) return;
+  if (!grid_sync(B.bar, B.nblocks, B.spin_limit)) return;
   stamp(B.bar, 3);
 
   // phase 3: large triangles, tile by tile
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
     raster_tiled_loop<false>(V.dp, sgd + V.goff, q.vo, lane);
     fallback_loop(V.dp, sgd + V.goff, q.vo, q.va, lane, gw, nw);
   }
-  if (!grid_sync(B.bar, B.nblocks)) return;
+  if (!grid_sync(B.bar, B.nblocks, B.spin_limit)) return;
   stamp(B.bar, 4);
 
   batch_shade(B, sgd, tid, step);

@@ -281,6 +281,14 @@ int axr_batch_set_tuning(axr_batch *b, int blocks_per_sm, int min_chunk);
 #define AXR_BATCH_PERSISTENT 0
 #define AXR_BATCH_PHASED 1
 int axr_batch_set_mode(axr_batch *b, int mode);
+
+/* Fault injection for tests of failure detection (persistent form): the next
+ * renders' grid barriers wait for phantom_blocks blocks that are never
+ * launched, and every waiting block gives up after spin_limit polls (at most
+ * the default, about 2^26), so the render ends with the error "batch grid
+ * barrier timed out" instead of hanging.  (0, 67108864) restores normal
+ * renders.  No GPU fault is involved. */
+int axr_batch_inject_barrier_stall(axr_batch *b, int phantom_blocks, long long spin_limit);
 int axr_set_tuning(axr_ctx *ctx, int min_chunk);
 
 int axr_batch_destroy(axr_batch *b);
