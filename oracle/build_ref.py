@@ -66,7 +66,11 @@ def translate(src: str, ns: str) -> str:
             f"{body}\n{defs}{getters}}} }}\n")
 
 
-def build(reference: str, verbose: bool = False) -> str | None:
+# where this recipe reads the reference checkout (read-only; nothing is copied)
+DEFAULT_REFERENCE = os.environ.get("AXR_REFERENCE", "/root/reference")
+
+
+def build(reference: str = DEFAULT_REFERENCE, verbose: bool = False) -> str | None:
     if not os.path.isdir(os.path.join(reference, "PyOpenCL27C")):
         print(f"build_ref: reference checkout not found at {reference}; skipped")
         return None
@@ -91,7 +95,7 @@ def build(reference: str, verbose: bool = False) -> str | None:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("AXR_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=DEFAULT_REFERENCE)
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
     lib = build(a.reference, a.verbose)
