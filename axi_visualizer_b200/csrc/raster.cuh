@@ -85,10 +85,13 @@ __device__ __forceinline__ float axr_log2f(float x) {
   double s = (m - 1.0) / (m + 1.0);
   double s2 = s * s;
   double term = s, sum = s;
+  // atanh series s + s^3/3 + ... + s^19/19, the divisions as products with the
+  // reciprocals (same constants and order as the oracle's orc_log2f)
+  const double inv[9] = {1.0 / 3, 1.0 / 5, 1.0 / 7, 1.0 / 9, 1.0 / 11, 1.0 / 13, 1.0 / 15, 1.0 / 17, 1.0 / 19};
 #pragma unroll
   for (int k = 1; k <= 9; k++) {
     term = term * s2;
-    sum = sum + term / (double)(2 * k + 1);
+    sum = sum + term * inv[k - 1];
   }
   double r = (double)e + sum * 2.8853900817779268;
   return (float)r;

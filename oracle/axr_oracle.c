@@ -90,9 +90,12 @@ float orc_log2f(float x) {
   double s = (m - 1.0) / (m + 1.0);
   double s2 = s * s;
   double term = s, sum = s;
+  /* atanh series s + s^3/3 + ... + s^19/19, the divisions as products with the
+     reciprocals (same constants and order as the CUDA side's axr_log2f) */
+  static const double inv[9] = {1.0 / 3, 1.0 / 5, 1.0 / 7, 1.0 / 9, 1.0 / 11, 1.0 / 13, 1.0 / 15, 1.0 / 17, 1.0 / 19};
   for (int k = 1; k <= 9; k++) {
     term = term * s2;
-    sum = sum + term / (double)(2 * k + 1);
+    sum = sum + term * inv[k - 1];
   }
   double r = (double)e + sum * 2.8853900817779268; /* 2/ln(2) */
   return (float)r;
