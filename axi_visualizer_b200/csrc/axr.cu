@@ -708,7 +708,7 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   }
   // shading samples the cascades: wait for their last writers
   for (int k = 0; k < nshadow; k++) CK(cudaStreamWaitEvent(s, c->shadows[shadow_ids[k]].ev_write, 0));
-  dim3 sb(16, 16), sgd((c->w + 15) / 16, (c->h + 15) / 16);
+  dim3 sb(256), sgd((c->w + 15) / 16, (c->h + 15) / 16);   // a 16x16 tile per block
   launch(c, s, "k_shade", [&] { k_shade<<<sgd, sb, 0, s>>>(P); }); nk++;
   for (int k = 0; k < nshadow; k++) CK(cudaEventRecord(c->shadows[shadow_ids[k]].ev_read, s));
   CK(cudaGetLastError());

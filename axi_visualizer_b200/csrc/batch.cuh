@@ -169,22 +169,23 @@ __device__ __forceinline__ void batch_raster(const BatchParams &B, const GroupDe
   }
 }
 
-// phase 4: shading
-__device__ __forceinline__ void batch_shade(const BatchParams &B, const GroupDev *sgd, int tid, int step) {
+// phase 4: shading, tile by tile (16 x NT/16 pixels per block and tile)
+template <int NT>
+__device__ __forceinline__ void batch_shade(const BatchParams &B, const GroupDev *sgd, ShadeSmem<NT> &sm) {
+  constexpr int TH = NT / 16;
   for (int v = 0; v < B.nviews; v++) {
     const BatchView &V = B.views[v];
     if (V.kind != VIEW_SHADED) continue;
-    int W = V.w, n = V.w * V.h;
-    for (int i = tid; i < n; i += step) {
-      int y = i / W, x = i - y * W;
-      shade_pixel(V.dp, sgd + V.goff, x, y, V.dp.keys[i]);
-    }
+    int tw = (V.w + 15) / 16, th = (V.h + TH - 1) / TH;
+    for (int t = blockIdx.x; t < tw * th; t += gridDim.x)
+      shade_tile<NT>(V.dp, sgd + V.goff, (t % tw) * 16, (t / tw) * TH, sm);
   }
 }
 
 __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
-  __shared__ WarpQueue wq[4];
+  __shared__ union U { WarpQueue wq[4]; ShadeSmem<128> sh; } u;   // phases 2-3 / phase 4
+  WarpQueue *wq = u.wq;
   load_tables(B, sgd, sgs);
   stamp(B.bar, 0);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   if (!grid_sync(B.bar, B.nblocks, B.spin_limit)) return;
   stamp(B.bar, 4);
 
-  batch_shade(B, sgd, tid, step);
+  batch_shade<128>(B, sgd, u.sh);
   // the last block to finish stamps the end
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -279,9 +280,11 @@ __global__ void __launch_bounds__(128) kb_fallback(BatchParams B) {
 }
 
 __global__ void __launch_bounds__(256, 3) kb_shade(BatchParams B) {
-  __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
-  load_tables(B, sgd, sgs);
-  batch_shade(B, sgd, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  __shared__ GroupDev sgd[BATCH_TABLE];
+  __shared__ ShadeSmem<256> sm;
+  for (int i = threadIdx.x; i < B.ngroups; i += blockDim.x) sgd[i] = B.groups_draw[i];
+  __syncthreads();
+  batch_shade<256>(B, sgd, sm);
 }
 
 }  // namespace axr

@@ -889,10 +889,17 @@ __device__ __forceinline__ float shadow_light(const DrawParams &P, V3 p) {
 template <class A>
 __device__ __forceinline__ void swap_(A &a, A &b) { A t = a; a = b; b = t; }
 
-// Replays the winning fragment of pixel (ax, cy) and shades it.
-__device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev *sg, int ax, int cy, uint64_t key) {
-  uint32_t ord = 0xffffffffu - (uint32_t)key;
-  if (ord == 0) return;
+// The interpolants of winner `ord` on row cy: triangle set-up, mip level and
+// the row accumulation (small triangles from their first row, large ones
+// from the tile's first row), as the rasterizer walked them.
+struct RowState {
+  float cx1, cx2, cz1, cz2;
+  Attr<true> c1, c2;
+  float fmip;
+  int mip, g;
+};
+
+__device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *sg, uint32_t ord, int cy, RowState &st) {
   uint32_t o = ord - 1;
   int phase = (int)(o >> 31);
   uint32_t gtri = (o >> 1) & 0x3fffffffu;
@@ -1001,6 +1008,23 @@ __device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev 
       }
     }
   }
+  st.cx1 = cx1; st.cx2 = cx2; st.cz1 = cz1; st.cz2 = cz2;
+  st.c1 = c1; st.c2 = c2;
+  st.fmip = ms.fmip; st.mip = ms.mip; st.g = g;
+}
+
+// Shades pixel ax of row cy from its winner's row state.
+__device__ __forceinline__ void shade_from_row(const DrawParams &P, const GroupDev *sg, int ax, int cy,
+                                               const RowState &st) {
+  const GroupDev &G = sg[st.g];
+  const bool mip = (G.flags & F_MIP) != 0;
+  MipSel ms;
+  ms.fmip = st.fmip; ms.mip = st.mip;
+  ms.len_mip = 1 << ms.mip; ms.len_mip2 = ms.len_mip << 1;
+  ms.start_mip = ((1 << (2 * ms.mip)) - 1) / 3;            // sum of 4^i for i < mip
+  ms.start_mip2 = ms.start_mip + ms.len_mip * ms.len_mip;
+  const float cx1 = st.cx1, cx2 = st.cx2, cz1 = st.cz1, cz2 = st.cz2;
+  const Attr<true> c1 = st.c1, c2 = st.c2;
   float t = ((float)ax - cx2) / (cx1 - cx2);
   t = clamp_t(t);
   float tz = 1.0f / ((1 - t) * cz2 + t * cz1);
@@ -1041,16 +1065,80 @@ __device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev 
   P.db[pix] = tz;
 }
 
+// Replays the winning fragment of pixel (ax, cy) and shades it.
+__device__ __forceinline__ void shade_pixel(const DrawParams &P, const GroupDev *sg, int ax, int cy, uint64_t key) {
+  uint32_t ord = 0xffffffffu - (uint32_t)key;
+  if (ord == 0) return;
+  RowState st;
+  shade_row(P, sg, ord, cy, st);
+  shade_from_row(P, sg, ax, cy, st);
+}
+
+// Shared memory of shade_tile for a block of NT threads (16 x NT/16 pixels).
+template <int NT>
+struct ShadeSmem {
+  unsigned long long hkey[NT];   // open-addressing table of (winner, row) keys
+  int hent[NT];                  // its entry numbers
+  unsigned long long ekey[NT];   // entry -> key
+  int nent;
+  RowState rs[NT];
+};
+
+// Shades the 16 x (NT/16) pixels at (x0, y0): the block finds the distinct
+// (winner, row) pairs among its pixels (a bounded open-addressing table in
+// shared memory), one thread per pair sets up the triangle and replays its
+// row, then every pixel shades from its pair's row state.  The arithmetic is
+// shade_pixel's, done once per pair instead of once per pixel.
+template <int NT>
+__device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *sg, int x0, int y0, ShadeSmem<NT> &sm) {
+  const unsigned long long EMPTY = ~0ull;
+  int tid = threadIdx.x;
+  int ax = x0 + (tid & 15), cy = y0 + (tid >> 4);
+  bool in = ax < P.view.w && cy < P.view.h;
+  uint32_t ord = in ? 0xffffffffu - (uint32_t)P.keys[(size_t)P.view.w * cy + ax] : 0u;
+  bool valid = ord != 0;
+  sm.hkey[tid] = EMPTY;
+  if (tid == 0) sm.nent = 0;
+  __syncthreads();
+  int slot = 0;
+  if (valid) {
+    unsigned long long k = ((unsigned long long)ord << 32) | (uint32_t)cy;
+    uint32_t h = ((ord * 2654435761u) ^ ((uint32_t)cy * 40503u)) % NT;
+    for (int i = 0; i < NT; i++) {       // at most NT keys: always finds a slot
+      unsigned long long prev = atomicCAS(&sm.hkey[h], EMPTY, k);
+      if (prev == EMPTY) {
+        int e = atomicAdd(&sm.nent, 1);
+        sm.hent[h] = e;
+        sm.ekey[e] = k;
+        slot = (int)h;
+        break;
+      }
+      if (prev == k) {
+        slot = (int)h;
+        break;
+      }
+      h = (h + 1) % NT;
+    }
+  }
+  __syncthreads();
+  int ne = sm.nent;
+  for (int e = tid; e < ne; e += NT) {
+    unsigned long long k = sm.ekey[e];
+    shade_row(P, sg, (uint32_t)(k >> 32), (int)(uint32_t)k, sm.rs[e]);
+  }
+  __syncthreads();
+  if (valid) shade_from_row(P, sg, ax, cy, sm.rs[sm.hent[slot]]);
+  __syncthreads();                       // the next tile reuses the shared memory
+}
+
+
+// one 256-thread block per 16x16 tile
 __global__ void __launch_bounds__(256, 3) k_shade(DrawParams P) {   // 80 registers: 3 blocks per SM
   __shared__ GroupDev sg[64];
-  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < P.ngroups; i += blockDim.x * blockDim.y)
-    sg[i] = P.groups[i];
+  __shared__ ShadeSmem<256> sm;
+  for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
   __syncthreads();
-  int ax = blockIdx.x * blockDim.x + threadIdx.x;
-  int cy = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ax >= P.view.w || cy >= P.view.h) return;
-  uint64_t key = P.keys[(size_t)P.view.w * cy + ax];
-  shade_pixel(P, sg, ax, cy, key);
+  shade_tile<256>(P, sg, blockIdx.x * TILE, blockIdx.y * TILE, sm);
 }
 
 __global__ void k_ids(const uint64_t *__restrict__ keys, int n, int32_t *tri_id, uint8_t *cov) {
