@@ -23,7 +23,7 @@ EXPORTS = [
     "axr_batch_get_frame", "axr_batch_get_ids", "axr_batch_stats", "axr_batch_destroy",
     "axr_batch_set_tuning", "axr_set_tuning", "axr_batch_query", "axr_batch_read_async", "axr_batch_bytes",
     "axr_clear_color", "axr_batch_phase_times", "axr_batch_set_mode", "axr_read_frame_async", "axr_wait_frame",
-    "axr_frame_done", "axr_batch_inject_barrier_stall",
+    "axr_frame_done", "axr_batch_inject_barrier_stall", "axr_read_frame_rgb8_async",
 ]
 
 
@@ -91,6 +91,7 @@ _SIGS = {
     "axr_wait_frame": (i32, [vp, C.c_int64]),
     "axr_frame_done": (i32, [vp, C.c_int64]),
     "axr_batch_inject_barrier_stall": (i32, [vp, i32, C.c_longlong]),
+    "axr_read_frame_rgb8_async": (i32, [vp, f32, vp, C.POINTER(C.c_int64)]),
 }
 
 _lib = None

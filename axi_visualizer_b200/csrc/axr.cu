@@ -773,6 +773,38 @@ int axr_read_frame_async(axr_ctx *c, uint16_t *r, uint16_t *g, uint16_t *b, floa
   return 0;
 }
 
+int axr_read_frame_rgb8_async(axr_ctx *c, float exposure, uint8_t *rgb, int64_t *ticket) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!ticket || !rgb) return fail(AXR_EINVAL, "null argument");
+  if ((rc = settle_next(c))) return rc;
+  size_t n = (size_t)c->w * c->h;
+  if (!c->s_copy) CK(cudaStreamCreateWithFlags(&c->s_copy, cudaStreamNonBlocking));
+  axr_ctx::ReadSlot &sl = c->rd[c->read_seq & 1];
+  if (sl.busy) {
+    CK(cudaEventSynchronize(sl.done));
+    sl.busy = false;
+  }
+  if (!sl.stage) {
+    if (cudaMalloc(&sl.stage, n * 10) != cudaSuccess) return fail(AXR_ENOMEM, "frame staging buffer");
+    CK(cudaEventCreateWithFlags(&sl.staged, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+  }
+  cudaStream_t s = c->stream;
+  launch(c, s, "k_pack_rgb8", [&] {
+    k_pack_rgb8<<<grid_for(c, (long)n, 256, 8), 256, 0, s>>>(c->ro, c->go, c->bo, (int)n, exposure, sl.stage);
+  });
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(sl.staged, s));
+  CK(cudaStreamWaitEvent(c->s_copy, sl.staged, 0));
+  CK(cudaMemcpyAsync(rgb, sl.stage, n * 3, cudaMemcpyDeviceToHost, c->s_copy));
+  CK(cudaEventRecord(sl.done, c->s_copy));
+  sl.busy = true;
+  sl.seq = c->read_seq;
+  *ticket = c->read_seq++;
+  return 0;
+}
+
 int axr_wait_frame(axr_ctx *c, int64_t ticket) {
   int rc = check_ctx(c);
   if (rc) return rc;

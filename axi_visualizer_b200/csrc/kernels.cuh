@@ -121,20 +121,38 @@ __global__ void k_fill_rgb(uint16_t *__restrict__ ro, uint16_t *__restrict__ go,
 }
 
 // Post/gamma.c:38-52
+__device__ __forceinline__ void gamma_px(uint16_t r, uint16_t g, uint16_t b, float e8, int &ro, int &go, int &bo) {
+  float jx = sqrtf(e8 * (float)r) / 1.1f;
+  float jy = sqrtf(e8 * (float)g) / 1.1f;
+  float jz = sqrtf(e8 * (float)b) / 1.1f;
+  float m = fmaxf(jx, fmaxf(jy, jz)) / 255.f;
+  if (m > 1.f) {
+    float sm = sqrtf(m);
+    jx = jx / sm; jy = jy / sm; jz = jz / sm;
+  }
+  ro = f2i(fminf(255.f, jx));
+  go = f2i(fminf(255.f, jy));
+  bo = f2i(fminf(255.f, jz));
+}
+
 __global__ void k_gamma(uint16_t *r, uint16_t *g, uint16_t *b, int n, float exposure) {
   float e8 = 8 * exposure;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float jx = sqrtf(e8 * (float)r[i]) / 1.1f;
-    float jy = sqrtf(e8 * (float)g[i]) / 1.1f;
-    float jz = sqrtf(e8 * (float)b[i]) / 1.1f;
-    float m = fmaxf(jx, fmaxf(jy, jz)) / 255.f;
-    if (m > 1.f) {
-      float sm = sqrtf(m);
-      jx = jx / sm; jy = jy / sm; jz = jz / sm;
-    }
-    r[i] = (uint16_t)f2i(fminf(255.f, jx));
-    g[i] = (uint16_t)f2i(fminf(255.f, jy));
-    b[i] = (uint16_t)f2i(fminf(255.f, jz));
+    int x, y, z;
+    gamma_px(r[i], g[i], b[i], e8, x, y, z);
+    r[i] = (uint16_t)x; g[i] = (uint16_t)y; b[i] = (uint16_t)z;
+  }
+}
+
+// Post/gamma.c's mapping packed as interleaved 8-bit RGB for display (the
+// planes are left as they are): 3 bytes per pixel instead of 6 + 4.
+__global__ void k_pack_rgb8(const uint16_t *__restrict__ r, const uint16_t *__restrict__ g,
+                            const uint16_t *__restrict__ b, int n, float exposure, uint8_t *__restrict__ out) {
+  float e8 = 8 * exposure;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int x, y, z;
+    gamma_px(r[i], g[i], b[i], e8, x, y, z);
+    out[3 * (size_t)i] = (uint8_t)x; out[3 * (size_t)i + 1] = (uint8_t)y; out[3 * (size_t)i + 2] = (uint8_t)z;
   }
 }
 

@@ -59,7 +59,8 @@ class CLDraw:
         if self._pinned:
             import torch
             t = torch.empty(shape, dtype={np.uint16: torch.uint16, np.float32: torch.float32,
-                                          np.int32: torch.int32, np.uint8: torch.uint8}[dtype], pin_memory=True)
+                                          np.int32: torch.int32, np.uint8: torch.uint8}[np.dtype(dtype).type],
+                            pin_memory=True)
             self.__dict__.setdefault("_pins", []).append(t)
             return t.numpy()
         return np.ones(shape, dtype)
@@ -186,6 +187,19 @@ class CLDraw:
         check(self._L.axr_read_frame_async(self._h, *[_p(a) for a in bufs], C.byref(t)), "readFrameAsync")
         self._ring_next ^= 1
         return (t.value, bufs)
+
+    def readFrameRGB8Async(self, ex=1.0):
+        """Starts reading the frame back as display-ready 8-bit RGB (H, W, 3):
+        Post/gamma.c's mapping with exposure `ex`, packed on the device (new;
+        the planes are not changed).  Returns a ticket for waitFrame."""
+        if not hasattr(self, "_ring8"):
+            self._ring8 = [self._host((self.H, self.W, 3), np.uint8) for _ in range(2)]
+            self._ring8_next = 0
+        buf = self._ring8[self._ring8_next]
+        t = C.c_int64()
+        check(self._L.axr_read_frame_rgb8_async(self._h, float(ex), _p(buf), C.byref(t)), "readFrameRGB8Async")
+        self._ring8_next ^= 1
+        return (t.value, buf)
 
     def waitFrame(self, ticket):
         """Blocks until the read `ticket` is on the host; returns (r, g, b, depth)."""

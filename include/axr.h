@@ -103,6 +103,12 @@ int axr_set_vm(axr_ctx *ctx, const float vm[9]);
  * getFrame is synchronous). */
 int axr_read_frame_async(axr_ctx *ctx, uint16_t *r, uint16_t *g, uint16_t *b, float *depth, int64_t *ticket);
 int axr_wait_frame(axr_ctx *ctx, int64_t ticket);
+
+/* The same for a display client: the frame mapped by Post/gamma.c's formula
+ * with `exposure` (as axr_gamma, but the planes stay unchanged) and packed
+ * on the device as interleaved 8-bit RGB into rgb [h][w][3] (3 bytes per
+ * pixel instead of 10).  Same ring, tickets and rules as above.  New. */
+int axr_read_frame_rgb8_async(axr_ctx *ctx, float exposure, uint8_t *rgb, int64_t *ticket);
 int axr_frame_done(axr_ctx *ctx, int64_t ticket);
 
 /* CLDraw.clearZBuffer() (Ops0.py:650-653, clearzb.c): depth := 65535 on the

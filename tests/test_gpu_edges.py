@@ -156,3 +156,26 @@ def test_async_frame_read_equals_get_frame():
         assert R.draw.frameDone(t)
         for a, b in zip(got, want[kk]):
             assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_rgb8_read_back_equals_gamma_of_the_planes():
+    """readFrameRGB8Async packs Post/gamma.c's mapping of the colour planes
+    as interleaved 8-bit RGB on the device: equal to the oracle's gamma of
+    the same planes, for two exposures, and the planes stay unchanged."""
+    from axi_visualizer_b200.ops import SceneRenderer
+    sc = S.scene_small(seed=4, flags=S.MIP | S.SHADOW)
+    view = S.default_view(320, 240, pos=(3, 2, -8))
+    R = SceneRenderer(sc, 320, 240, pinned=True)
+    R.frame(view)
+    planes = [x.copy() for x in R.draw.getFrame()[:3]]
+    for ex in (1.0, 0.37):
+        t = R.draw.readFrameRGB8Async(ex)
+        rgb = R.draw.waitFrame(t).copy()
+        fr = O.Frame(320, 240)
+        fr.ro, fr.go, fr.bo = (p.copy() for p in planes)
+        O.gamma(fr, ex)
+        want = np.stack((fr.ro, fr.go, fr.bo), axis=-1).astype(np.uint8)
+        assert rgb.shape == (240, 320, 3) and np.array_equal(rgb, want)
+    after = R.draw.getFrame()[:3]
+    for a, b in zip(after, planes):
+        assert np.array_equal(a, b)
