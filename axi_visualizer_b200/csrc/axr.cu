@@ -126,6 +126,15 @@ struct axr_ctx {
     bool used = false;
   } stage[8];
   int stage_next = 0;
+  // vertex stage: ev_geo follows the last geometry write on `stream`
+  // (rotate/translate/copyTo), which shadow passes on their own streams wait
+  // for; the light table of vertLight is staged through pinned memory
+  cudaEvent_t ev_geo = nullptr;
+  float *d_lights = nullptr, *h_lights = nullptr;
+  size_t lights_cap = 0;
+  cudaEvent_t ev_lights = nullptr;
+  bool lights_used = false;
+  int light_blocks = 4;                      // resident 256-thread blocks of k_vert_light per SM
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
   int min_chunk = MIN_CHUNK;
@@ -410,9 +419,13 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
       cudaMallocHost(&c->h_ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
       cudaMallocHost(&c->h_ring, sizeof(uint32_t) * CTR_N * 2) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_ctr[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_ctr[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->ev_ctr[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_geo, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_lights, cudaEventDisableTiming) != cudaSuccess) {
     rc = fail(AXR_ENOMEM, "framebuffers for %dx%d", w, h);
   }
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->light_blocks, k_vert_light, 256, 0);
+  if (c->light_blocks < 1) c->light_blocks = 1;
   // initial tile-unit queue (grows after an overflow); AXR_UNIT_QUEUE overrides
   uint32_t units0 = 1u << 22;
   if (const char *e = getenv("AXR_UNIT_QUEUE")) {
@@ -478,6 +491,10 @@ int axr_destroy(axr_ctx *c) {
   }
   for (auto &p : c->tpend) { c->ev_pool.push_back(p.a); c->ev_pool.push_back(p.b); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->ev_geo) cudaEventDestroy(c->ev_geo);
+  if (c->ev_lights) { cudaEventSynchronize(c->ev_lights); cudaEventDestroy(c->ev_lights); }
+  cudaFree(c->d_lights);
+  if (c->h_lights) cudaFreeHost(c->h_lights);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -543,26 +560,145 @@ int axr_set_vert_light(axr_ctx *c, int group, const float *li) {
 }
 
 int axr_vert_light(axr_ctx *c, const uint8_t *mask, int ngroups, const float *dir_int, const float *dir_dir, int ndirs,
-                   float amb) {
+                   const float *point_int, const float *point_pos, int npoints, const float *spot_int,
+                   const float *spot_dir, const float *spot_pos, int nspots, float amb) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (ngroups != (int)c->groups.size() || ndirs < 0 || ndirs > 64 || (ndirs && (!dir_int || !dir_dir)))
+  // the reference passes the counts as char / short / int (Ops.py:561,579,595)
+  if (ngroups != (int)c->groups.size() || ndirs < 0 || ndirs > 127 || npoints < 0 || npoints > 32767 ||
+      nspots < 0 || (ndirs && (!dir_int || !dir_dir)) || (npoints && (!point_int || !point_pos)) ||
+      (nspots && (!spot_int || !spot_dir || !spot_pos)))
     return fail(AXR_EINVAL, "vert_light arguments");
-  float *d = nullptr;
-  if (cudaMalloc(&d, sizeof(float) * 6 * std::max(ndirs, 1)) != cudaSuccess) return fail(AXR_ENOMEM, "light table");
-  cudaMemcpyAsync(d, dir_int, sizeof(float) * 3 * ndirs, cudaMemcpyHostToDevice, c->stream);
-  cudaMemcpyAsync(d + 3 * ndirs, dir_dir, sizeof(float) * 3 * ndirs, cudaMemcpyHostToDevice, c->stream);
+  // table: dir int | dir dir | point int | point pos | spot int | spot dir | spot pos
+  size_t nf = 3 * (2 * (size_t)ndirs + 2 * (size_t)npoints + 3 * (size_t)nspots);
+  if (nf > c->lights_cap) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->lights_used) CK(cudaEventSynchronize(c->ev_lights));
+    cudaFree(c->d_lights);
+    if (c->h_lights) cudaFreeHost(c->h_lights);
+    c->d_lights = c->h_lights = nullptr;
+    c->lights_cap = 0;
+    size_t cap = std::max<size_t>(nf, 1024);
+    if (cudaMalloc(&c->d_lights, cap * 4) != cudaSuccess || cudaMallocHost(&c->h_lights, cap * 4) != cudaSuccess)
+      return fail(AXR_ENOMEM, "light table of %zu floats", nf);
+    c->lights_cap = cap;
+  } else if (c->lights_used) {
+    CK(cudaEventSynchronize(c->ev_lights));   // the copy that read the staging buffer last time
+  }
+  float *h = c->h_lights;
+  const float *src[7] = {dir_int, dir_dir, point_int, point_pos, spot_int, spot_dir, spot_pos};
+  const int cnt[7] = {ndirs, ndirs, npoints, npoints, nspots, nspots, nspots};
+  size_t off[7], at = 0;
+  for (int k = 0; k < 7; k++) {
+    off[k] = at;
+    if (cnt[k]) memcpy(h + at, src[k], sizeof(float) * 3 * cnt[k]);
+    at += 3 * (size_t)cnt[k];
+  }
+  if (nf) CK(cudaMemcpyAsync(c->d_lights, h, nf * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(c->ev_lights, c->stream));
+  c->lights_used = true;
+  VertLights L;
+  const float *d = c->d_lights;
+  L.dint = d + off[0]; L.ddir = d + off[1]; L.pint = d + off[2]; L.ppos = d + off[3];
+  L.sint = d + off[4]; L.sdir = d + off[5]; L.spos = d + off[6];
+  L.nd = ndirs; L.np = npoints; L.ns = nspots; L.amb = amb;
   for (int g = 0; g < ngroups; g++) {
     if (mask && !mask[g]) continue;
-    int nv = c->groups[g].ntris * 3;
+    const Group &G = c->groups[g];
+    int nv = G.ntris * 3;
     if (!nv) continue;
-    k_vert_light<<<grid_for(c, nv, 256, 8), 256, 0, c->stream>>>(c->groups[g].vn, c->groups[g].li, nv, d, d + 3 * ndirs,
-                                                                    ndirs, amb);
+    launch(c, c->stream, "k_vert_light", [&] {
+      k_vert_light<<<grid_for(c, nv, 256, c->light_blocks), 256, 0, c->stream>>>(G.xyz, G.vn, G.li, nv, L);
+    });
   }
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  cudaFree(d);
-  if (e != cudaSuccess) return fail(AXR_ECUDA, "vert_light: %s", cudaGetErrorString(e));
+  CK(cudaGetLastError());
   c->amb = amb;
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// A write of group geometry on the handle's stream: waits for every shadow
+// pass in flight (they read the geometry on their own streams) and, after
+// `body` has queued the write, marks it for the next shadow passes.
+template <class F>
+int geometry_write(axr_ctx *c, F body) {
+  for (auto &sm : c->shadows)
+    if (sm.st) CK(cudaStreamWaitEvent(c->stream, sm.ev_write, 0));
+  int rc = body();
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev_geo, c->stream));
+  return 0;
+}
+
+int vertex_range(axr_ctx *c, int group, int &v0, int &v1) {
+  if (group < 0 || group >= (int)c->groups.size()) return fail(AXR_EINVAL, "group %d", group);
+  int nv = c->groups[group].ntris * 3;
+  if (v1 < 0) v1 = nv;
+  if (v0 < 0 || v0 > v1 || v1 > nv) return fail(AXR_EINVAL, "vertices [%d, %d) outside group %d of %d", v0, v1, group, nv);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int axr_transform(axr_ctx *c, int group, const float *old_rm, const float *rot_mat, const float *origin, int v_start,
+                  int v_end) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!old_rm || !rot_mat || !origin) return fail(AXR_EINVAL, "transform arguments");
+  if ((rc = vertex_range(c, group, v_start, v_end))) return rc;
+  VertXform X;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      X.oldr[3 * i + j] = old_rm[3 * i + j];
+      X.rr[3 * i + j] = rot_mat[3 * j + i];
+    }
+  for (int k = 0; k < 3; k++) X.o[k] = origin[k];
+  if (v_start == v_end) return 0;
+  const Group &G = c->groups[group];
+  return geometry_write(c, [&] {
+    int nq = (v_end + 3) / 4 - v_start / 4;
+    launch(c, c->stream, "k_vert_xform", [&] {
+      k_vert_xform<true><<<grid_for(c, nq, 256, 8), 256, 0, c->stream>>>(G.xyz, G.vn, v_start, v_end, X);
+    });
+    CK(cudaGetLastError());
+    return 0;
+  });
+}
+
+int axr_translate(axr_ctx *c, int group, const float *coords, int v_start, int v_end) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!coords) return fail(AXR_EINVAL, "translate arguments");
+  if ((rc = vertex_range(c, group, v_start, v_end))) return rc;
+  VertXform X = {};
+  for (int k = 0; k < 3; k++) X.o[k] = coords[k];
+  if (v_start == v_end) return 0;
+  const Group &G = c->groups[group];
+  return geometry_write(c, [&] {
+    int nq = (v_end + 3) / 4 - v_start / 4;
+    launch(c, c->stream, "k_vert_translate", [&] {
+      k_vert_xform<false><<<grid_for(c, nq, 256, 8), 256, 0, c->stream>>>(G.xyz, nullptr, v_start, v_end, X);
+    });
+    CK(cudaGetLastError());
+    return 0;
+  });
+}
+
+int axr_get_vertices(axr_ctx *c, int group, float *xyz, float *vn, float *li) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (group < 0 || group >= (int)c->groups.size()) return fail(AXR_EINVAL, "group %d", group);
+  const Group &G = c->groups[group];
+  size_t n = (size_t)G.ntris * 9 * 4;
+  if (xyz) CK(cudaMemcpyAsync(xyz, G.xyz, n, cudaMemcpyDeviceToHost, c->stream));
+  if (vn) CK(cudaMemcpyAsync(vn, G.vn, n, cudaMemcpyDeviceToHost, c->stream));
+  if (li) CK(cudaMemcpyAsync(li, G.li, n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -573,9 +709,13 @@ int axr_copy_to(axr_ctx *c, int group, const float *xyz, const float *vn, int tr
   Group &G = c->groups[group];
   if (tri_start < 0 || ntris < 0 || tri_start + ntris > G.ntris) return fail(AXR_EINVAL, "range out of group");
   size_t off = (size_t)tri_start * 9, n = (size_t)ntris * 9;
-  if (xyz) CK(cudaMemcpyAsync(G.xyz + off, xyz, n * 4, cudaMemcpyHostToDevice, c->stream));
-  if (vn) CK(cudaMemcpyAsync(G.vn + off, vn, n * 4, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  rc = geometry_write(c, [&] {
+    if (xyz) CK(cudaMemcpyAsync(G.xyz + off, xyz, n * 4, cudaMemcpyHostToDevice, c->stream));
+    if (vn) CK(cudaMemcpyAsync(G.vn + off, vn, n * 4, cudaMemcpyHostToDevice, c->stream));
+    return 0;
+  });
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));   // host arrays are borrowed only for the call
   return 0;
 }
 
@@ -957,6 +1097,7 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
     sm.cap = c->cap_list;
   }
   CK(cudaStreamWaitEvent(sm.st, sm.ev_read, 0));
+  CK(cudaStreamWaitEvent(sm.st, c->ev_geo, 0));   // rotate / translate / copyTo queued before
   if ((rc = upload_table(c, sm.tab, tab, std::max(ngroups, 1), sm.st))) return rc;
   ShadowParams S;
   memset(&S, 0, sizeof S);

@@ -156,22 +156,136 @@ __global__ void k_pack_rgb8(const uint16_t *__restrict__ r, const uint16_t *__re
   }
 }
 
-// vert.c:38-87 (directional lights 1..n-1; light 0 is shaded per pixel)
-__global__ void k_vert_light(const float *__restrict__ vn, float *__restrict__ li, int nv,
-                             const float *__restrict__ dints, const float *__restrict__ ddirs, int ndirs,
-                             float amb) {
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-    V3 n = ld3(vn + (size_t)v * 3);
-    V3 light{0.f, 0.f, 0.f};
-    for (int i = 1; i < ndirs; i++) {
-      V3 d{ddirs[3 * i], ddirs[3 * i + 1], ddirs[3 * i + 2]};
-      V3 it{dints[3 * i], dints[3 * i + 1], dints[3 * i + 2]};
-      float s = fmaxf(0.f, dot3(n, d) + 0.5f) * 0.66f;
-      light = add3(light, smul3(s, it));
+// ------------------------------------------------------------ vertex stage
+//
+// Pipe/vert.c over a group's packed vertex arrays (3 floats a vertex).  A
+// thread takes a quad of 4 consecutive vertices -- three aligned 16-byte
+// words of each array (the arrays start 256-byte aligned, so vertex 4k
+// starts a word) -- when the whole quad lies in [v0, v1); the partial quads
+// at both ends go vertex by vertex.  The arithmetic is vert.c's, one IEEE
+// rounding an operation in source order (no contraction).
+
+struct VertXform {
+  float oldr[9];   // rows of oldRM
+  float rr[9];     // rows of rotMat transposed (CLDraw.rotate uploads rotMat.T)
+  float o[3];      // origin (transform) or offset (Ttranslate)
+};
+
+struct VertLights {
+  const float *dint, *ddir;           // directional lights; light 0 is shaded per pixel
+  const float *pint, *ppos;           // point lights
+  const float *sint, *sdir, *spos;    // spot lights
+  int nd, np, ns;
+  float amb;
+};
+
+__device__ __forceinline__ V3 rows3(const float *m, V3 v) {
+  return V3{dot3(v, V3{m[0], m[1], m[2]}), dot3(v, V3{m[3], m[4], m[5]}), dot3(v, V3{m[6], m[7], m[8]})};
+}
+
+// vert.c:3-28 (transform)
+__device__ __forceinline__ void xform_rotate(const VertXform &X, V3 &p, V3 &n) {
+  V3 o{X.o[0], X.o[1], X.o[2]};
+  p = add3(rows3(X.rr, rows3(X.oldr, sub3(p, o))), o);
+  n = rows3(X.rr, rows3(X.oldr, n));
+}
+
+// vert.c:29-36 (Ttranslate)
+__device__ __forceinline__ void xform_translate(const VertXform &X, V3 &p) { p = add3(p, V3{X.o[0], X.o[1], X.o[2]}); }
+
+__device__ __forceinline__ V3 ldg3(const float *p, int i) { return ld3(p + 3 * i); }
+
+__device__ __forceinline__ float fast_length(V3 v) { return sqrtf(dot3(v, v)); }
+
+// vert.c:49-86 (vertL) for one vertex
+__device__ __forceinline__ V3 vert_light_one(const VertLights &L, V3 x, V3 n) {
+  V3 light{0.f, 0.f, 0.f};
+  for (int i = 1; i < L.nd; i++) {
+    float s = fmaxf(0.f, dot3(n, ldg3(L.ddir, i)) + 0.5f) * 0.66f;
+    light = add3(light, smul3(s, ldg3(L.dint, i)));
+  }
+  for (int i = 0; i < L.np; i++) {
+    V3 pl = sub3(x, ldg3(L.ppos, i));
+    if (dot3(n, pl) > 0.f) {
+      float fl = fast_length(pl);
+      float s = dot3(n, fast_normalize(pl)) / (1.f + fl * fl);
+      light = add3(light, smul3(s, ldg3(L.pint, i)));
     }
-    li[(size_t)v * 3 + 0] = fmaxf(light.x, amb);
-    li[(size_t)v * 3 + 1] = fmaxf(light.y, amb);
-    li[(size_t)v * 3 + 2] = fmaxf(light.z, amb);
+  }
+  for (int i = 0; i < L.ns; i++) {
+    V3 pl = sub3(x, ldg3(L.spos, i)), sd = ldg3(L.sdir, i);
+    if (dot3(sd, pl) > 0.f && dot3(n, pl) > 0.f) {
+      V3 u = fast_normalize(pl);
+      float fl = fast_length(pl);
+      float s = dot3(n, u) * dot3(u, sd) / (1.5f + fl * fl);
+      light = add3(light, smul3(s, ldg3(L.sint, i)));
+    }
+  }
+  return V3{fmaxf(light.x, L.amb), fmaxf(light.y, L.amb), fmaxf(light.z, L.amb)};
+}
+
+__device__ __forceinline__ void quad_ld(const float *a, int q, V3 v[4]) {
+  const float4 *w = reinterpret_cast<const float4 *>(a) + 3 * (size_t)q;
+  float4 w0 = w[0], w1 = w[1], w2 = w[2];
+  v[0] = V3{w0.x, w0.y, w0.z}; v[1] = V3{w0.w, w1.x, w1.y};
+  v[2] = V3{w1.z, w1.w, w2.x}; v[3] = V3{w2.y, w2.z, w2.w};
+}
+
+__device__ __forceinline__ void quad_st(float *a, int q, const V3 v[4]) {
+  float4 *w = reinterpret_cast<float4 *>(a) + 3 * (size_t)q;
+  w[0] = make_float4(v[0].x, v[0].y, v[0].z, v[1].x);
+  w[1] = make_float4(v[1].y, v[1].z, v[2].x, v[2].y);
+  w[2] = make_float4(v[2].z, v[3].x, v[3].y, v[3].z);
+}
+
+__device__ __forceinline__ V3 v_ld(const float *a, int v) { return V3{a[3 * (size_t)v], a[3 * (size_t)v + 1], a[3 * (size_t)v + 2]}; }
+__device__ __forceinline__ void v_st(float *a, int v, V3 x) {
+  a[3 * (size_t)v] = x.x; a[3 * (size_t)v + 1] = x.y; a[3 * (size_t)v + 2] = x.z;
+}
+
+// CLDraw.rotate (ROT) / CLDraw.translate over vertices [v0, v1)
+template <bool ROT>
+__global__ void k_vert_xform(float *__restrict__ xyz, float *__restrict__ vn, int v0, int v1, VertXform X) {
+  int q1 = (v1 + 3) >> 2;
+  for (int q = (v0 >> 2) + blockIdx.x * blockDim.x + threadIdx.x; q < q1; q += gridDim.x * blockDim.x) {
+    int a = q << 2;
+    if (a >= v0 && a + 4 <= v1) {
+      V3 p[4], n[4];
+      quad_ld(xyz, q, p);
+      if (ROT) quad_ld(vn, q, n);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (ROT) xform_rotate(X, p[k], n[k]);
+        else xform_translate(X, p[k]);
+      }
+      quad_st(xyz, q, p);
+      if (ROT) quad_st(vn, q, n);
+    } else {
+      for (int v = max(a, v0); v < min(a + 4, v1); v++) {
+        V3 p = v_ld(xyz, v), n;
+        if (ROT) {
+          n = v_ld(vn, v);
+          xform_rotate(X, p, n);
+          v_st(vn, v, n);
+        } else {
+          xform_translate(X, p);
+        }
+        v_st(xyz, v, p);
+      }
+    }
+  }
+}
+
+// CLDraw.vertLight for one group's nv vertices, one vertex a thread (the
+// light loops make it issue-bound, so the launch is one full wave of
+// resident blocks striding over the vertices); positions are read only when
+// point or spot lights exist.
+__global__ void k_vert_light(const float *__restrict__ xyz, const float *__restrict__ vn, float *__restrict__ li,
+                             int nv, VertLights L) {
+  const bool pos = L.np + L.ns > 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    V3 x = pos ? ld3(xyz + 3 * (size_t)v) : V3{0.f, 0.f, 0.f};
+    v_st(li, v, vert_light_one(L, x, ld3(vn + 3 * (size_t)v)));
   }
 }
 

@@ -49,6 +49,10 @@ class CLDraw:
         self._tex_alpha = 0
         self.SHADOWMAP = {}
         self.ambLight = np.float32(0.2)
+        # point and spot lights of vertLight stay set until a call replaces
+        # them (None) or clears them (1), as in the reference
+        self._points = (np.zeros((0, 3), np.float32),) * 2
+        self._spots = (np.zeros((0, 3), np.float32),) * 3
         self._pinned = pinned
         self.hro = self._host((self.H, self.W), np.uint16)
         self.hgo = self._host((self.H, self.W), np.uint16)
@@ -105,20 +109,65 @@ class CLDraw:
         check(self._L.axr_set_vert_light(self._h, int(tn), _p(a)), "setVertLight")
 
     def vertLight(self, mask, dirI, dirD, pointI=None, pointP=None, spotI=None, spotD=None, spotP=None):
-        """Per-vertex lighting from directional lights 1.. (vert.c vertL)."""
-        for extra in (pointI, spotI):
-            if extra is not None and not (isinstance(extra, int) and extra == 1) and len(np.atleast_1d(extra)):
-                raise NotImplementedError("point/spot lights of vertLight are outside this library")
+        """Per-vertex light I of every masked group from directional lights
+        1.., point and spot lights (vert.c vertL; Ops.py:552-612).  pointI /
+        spotI: None keeps the lights of the previous call, 1 clears them,
+        arrays [n][3] replace them."""
+        def lights(arg, rest, cur):
+            if arg is None:
+                return cur
+            if isinstance(arg, (int, np.integer)) and not isinstance(arg, bool) and arg == 1:
+                return tuple(np.zeros((0, 3), np.float32) for _ in cur)
+            arrs = tuple(_f32(np.asarray(x).reshape(-1, 3)) for x in (arg, *rest))
+            if len({a.shape[0] for a in arrs}) != 1:
+                raise ValueError("vertLight: light arrays of different lengths")
+            return arrs
+        self._points = lights(pointI, (pointP,), self._points)
+        self._spots = lights(spotI, (spotD, spotP), self._spots)
         i = _f32(np.asarray(dirI).reshape(-1, 3))
         d = _f32(np.asarray(dirD).reshape(-1, 3))
-        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8)[:len(self.gSize)])
+        if m.size < len(self.gSize):
+            raise ValueError("vertLight: mask shorter than the number of groups")
+        (pi, pp), (si, sd, sp) = self._points, self._spots
         check(self._L.axr_vert_light(self._h, _p(m), len(self.gSize), _p(i), _p(d), i.shape[0],
+                                     _p(pi), _p(pp), pi.shape[0], _p(si), _p(sd), _p(sp), si.shape[0],
                                      float(self.ambLight)), "vertLight")
+
+    def rotate(self, oldRM, rotMat, origin, cStart, cEnd, tn):
+        """Rotates vertices [cStart, cEnd) of group tn (None: to the end) about
+        origin: p -> rotMat^T (oldRM (p - origin)) + origin, normals alike
+        (vert.c transform; Ops.py:481-497)."""
+        old = _f32(np.asarray(oldRM).reshape(3, 3))
+        rot = _f32(np.asarray(rotMat).reshape(3, 3))
+        o = _f32(np.asarray(origin).reshape(3))
+        end = -1 if cEnd is None else int(cEnd)
+        check(self._L.axr_transform(self._h, int(tn), _p(old), _p(rot), _p(o), int(cStart), end), "rotate")
+
+    def transform(self, oldRM, rotMat, origin, cStart, cEnd, tn):
+        """The name VertObject.transform calls (VertObjects.py:238); same as rotate."""
+        self.rotate(oldRM, rotMat, origin, cStart, cEnd, tn)
+
+    def translate(self, coords, cStart, cEnd, tn):
+        """Moves vertices [cStart, cEnd) of group tn by coords (vert.c
+        Ttranslate; Ops.py:499-508)."""
+        o = _f32(np.asarray(coords).reshape(3))
+        end = -1 if cEnd is None else int(cEnd)
+        check(self._L.axr_translate(self._h, int(tn), _p(o), int(cStart), end), "translate")
 
     def copyTo(self, tn, vp, vn, cstart=0):
         p = _f32(np.asarray(vp).reshape(-1, 3))
         n = _f32(np.asarray(vn).reshape(-1, 3))
         check(self._L.axr_copy_to(self._h, int(tn), _p(p), _p(n), int(cstart), p.shape[0] // 3), "copyTo")
+
+    def getVertices(self, tn):
+        """New: group tn's vertex arrays (positions, normals, per-vertex light)
+        as (V, 3) float32 host copies, after the work queued before them.
+        The reference keeps them in device buffers (getBuffers, Ops.py:618-620)."""
+        nv = int(self.gSize[tn])
+        out = [np.empty((nv, 3), np.float32) for _ in range(3)]
+        check(self._L.axr_get_vertices(self._h, int(tn), *[_p(a) for a in out]), "getVertices")
+        return tuple(out)
 
     def addTexAlpha(self, a):
         a = np.asarray(a)
@@ -134,10 +183,12 @@ class CLDraw:
         check(self._L.axr_set_primary_light(self._h, _p(i), _p(d)), "setPrimaryLight")
 
     def setPos(self, vc):
-        check(self._L.axr_set_pos(self._h, _p(_f32(np.asarray(vc).reshape(3)))), "setPos")
+        v = _f32(np.asarray(vc).reshape(3))            # held until the call returns
+        check(self._L.axr_set_pos(self._h, _p(v)), "setPos")
 
     def setVM(self, vM):
-        check(self._L.axr_set_vm(self._h, _p(_f32(np.asarray(vM)[:3, :3].reshape(9)))), "setVM")
+        m = _f32(np.asarray(vM)[:3, :3].reshape(9))
+        check(self._L.axr_set_vm(self._h, _p(m)), "setVM")
 
     # ------------------------------------------------------------ frame
     def clearZBuffer(self):
@@ -326,7 +377,7 @@ class CLDraw:
 
     def __getattr__(self, name):
         if name in ("addTexture", "setReflTex", "setHostSkyTex", "addBoneWeights", "initBoneTransforms",
-                    "setBoneTransform", "boneTransform", "rotate", "translate", "setupWave", "updateWave",
+                    "setBoneTransform", "boneTransform", "setupWave", "updateWave",
                     "highlight", "blur", "drawDirectional", "getGIM", "addOpacityMap", "clearShadowOpMap",
                     "shadowClouds", "shadowCloudsOpacity", "tonemap", "mipShadowMap", "setPSTex", "drawPS"):
             raise NotImplementedError(f"CLDraw.{name} belongs to an effect outside the rasterizer hot path")

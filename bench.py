@@ -372,6 +372,85 @@ def small_section(device, frames=300):
             "launches_per_frame": launches}
 
 
+# ------------------------------------------------------------------ vertex stage
+
+def _rot_y(a):
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+
+
+def vertex_section(R, view, hbm, frames=100, warmup=5):
+    """An animated 1080p frame: both sphere groups (2 x 240,000 triangles)
+    turn about the scene centre (CLDraw.rotate, undoing the previous turn and
+    applying the next), the per-vertex light of every group is recomputed
+    from 2 extra directional, 4 point and 2 spot lights (CLDraw.vertLight),
+    then both cascades and drawAll render.  Frames/s device-timed with CUDA
+    events; the vertex kernels' HBM throughput from their event times, at
+    48 B a rotated vertex (position + normal read and written) and 36 B a
+    lit vertex (position + normal read, light written)."""
+    import torch
+    D = R.draw
+    scene = R.scene
+    spheres = [2, 3]
+    stream = torch.cuda.ExternalStream(D.stream_ptr(), device=torch.cuda.current_device())
+    rng = np.random.default_rng(11)
+    dirI = np.array([(1.6, 1.4, 1.2), (0.5, 0.5, 0.5), (0.1, 0.2, 0.6)])
+    dirD = np.array([(0.3, -0.8, 0.5), (-0.3, 0.8, -0.5), (0.0, 1.0, 0.0)])
+    pointI, pointP = rng.uniform(0, 3, (4, 3)), rng.uniform(-20, 20, (4, 3)) + (0, 8, 0)
+    spotI, spotD, spotP = rng.uniform(0, 3, (2, 3)), np.array([(0, -1, 0), (0.6, -0.8, 0)]), np.array([(0, 15, 0), (-10, 12, -5)])
+    mask = [1] * len(scene.groups)
+    state = {"k": 0}
+
+    def step():
+        k = state["k"]
+        prev, new = _rot_y(0.01 * k), _rot_y(0.01 * (k + 1))
+        for g in spheres:
+            D.rotate(prev, new, (0.0, 0.0, 0.0), 0, None, g)
+        D.vertLight(mask, dirI, dirD, pointI, pointP, spotI, spotD, spotP)
+        R.frame(view)
+        state["k"] = k + 1
+
+    for _ in range(warmup):
+        step()
+    D.sync()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(frames):
+        step()
+    ev[1].record(stream)
+    D.sync()
+    ms = ev[0].elapsed_time(ev[1]) / frames
+    D.setKernelTiming(True)
+    for _ in range(frames):
+        step()
+    kt = D.kernelTimes()
+    D.setKernelTiming(False)
+    # the scene's own geometry and light back on the device
+    for g in spheres:
+        D.copyTo(g, scene.groups[g].xyz, scene.groups[g].vn)
+    D.vertLight(mask, dirI, dirD, 1, None, 1)
+    for g, G in enumerate(scene.groups):
+        D.setVertLight(g, G.li)
+    D.sync()
+    nv_rot = sum(scene.groups[g].ntris * 3 for g in spheres)
+    nv_all = scene.ntris * 3
+    out = {"workload": "c2_animated_1080p_1m_tris", "rotated_vertices": nv_rot, "lit_vertices": nv_all,
+           "lights": {"directional": len(dirI) - 1, "point": len(pointI), "spot": len(spotI)},
+           "frames_per_s": 1000.0 / ms, "ms_per_frame": ms}
+    for name, per_v, nv, calls in (("k_vert_xform", 48, nv_rot // len(spheres), len(spheres)),
+                                   ("k_vert_light", 36, None, None)):
+        if name not in kt:
+            continue
+        tot_ms, n = kt[name]
+        avg_s = tot_ms / n / 1000.0
+        if nv is None:   # one launch per group: bytes of the average group
+            nv = nv_all / (n / frames)
+        gbs = per_v * nv / avg_s / 1e9
+        out[name] = {"avg_us": avg_s * 1e6, "launches_per_frame": n / frames, "bytes_per_vertex": per_v,
+                     "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm}
+    return out
+
+
 # ------------------------------------------------------------------ stress
 
 def stress_section(device, frames=10, log=progress):
@@ -585,6 +664,7 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-stress", action="store_true")
     ap.add_argument("--no-small", action="store_true")
+    ap.add_argument("--no-vertex", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -759,6 +839,11 @@ def main():
     # the added sections are per-GPU measurements: rank 0 runs them (the
     # other replicas are done once the whole-job numbers above are taken)
     extra = rank == 0
+    vertex = None
+    if extra and not args.no_vertex:
+        progress("vertex stage")
+        vertex = vertex_section(R, view, hbm, frames=min(args.steps, 100))
+
     small = None
     if extra and not args.no_small:
         progress("640x480 scene")
@@ -816,6 +901,7 @@ def main():
             "served": served,
             "stress": stress,
             "small": small,
+            "vertex": vertex,
         }
         print(json.dumps(line))
     ranks.close()

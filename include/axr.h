@@ -70,12 +70,39 @@ int axr_add_texture_group(axr_ctx *ctx, const float *xyz, const float *uv, const
  * with I = 0. */
 int axr_set_vert_light(axr_ctx *ctx, int group, const float *li);
 
-/* CLDraw.vertLight(mask, dirI, dirD) for directional lights only: computes
- * I = max(sum_{i>=1} max(0, dot(n, dir_i) + 0.5) * 0.66 * int_i, ambLight)
- * on the device for every group whose mask entry is non-zero
- * (vert.c:38-87; light 0 is the per-pixel primary light). */
+/* CLDraw.vertLight(mask, dirI, dirD, pointI, pointP, spotI, spotD, spotP)
+ * (Ops.py:552-612, vert.c:38-88): for every group whose mask entry is
+ * non-zero, on the device,
+ *   I = max(sum_{i>=1} max(0, dot(n, dir_i) + 0.5) * 0.66 * dint_i
+ *         + sum_points [dot(n, x - p) > 0] dot(n, u) / (1 + |x - p|^2) * pint
+ *         + sum_spots [dot(sdir, x - p) > 0 and dot(n, x - p) > 0]
+ *               dot(n, u) * dot(u, sdir) / (1.5 + |x - p|^2) * sint,  amb)
+ * with u = (x - p) / |x - p| (light 0 is the per-pixel primary light).
+ * Light arrays are [count][3]; at most 127 directional and 32767 point
+ * lights (the reference passes the counts as char and short).  Queued on
+ * the handle's stream; the light arrays are copied before the call returns. */
 int axr_vert_light(axr_ctx *ctx, const uint8_t *mask, int ngroups, const float *dir_int, const float *dir_dir,
-                   int ndirs, float amb);
+                   int ndirs, const float *point_int, const float *point_pos, int npoints, const float *spot_int,
+                   const float *spot_dir, const float *spot_pos, int nspots, float amb);
+
+/* CLDraw.rotate(oldRM, rotMat, origin, cStart, cEnd, tn) (Ops.py:481-497,
+ * vert.c:3-28): vertices [v_start, v_end) of a group (v_end < 0: to the end)
+ * move to rotMat^T . (oldRM . (p - origin)) + origin, and their normals to
+ * rotMat^T . (oldRM . n).  old_rm and rot_mat are row-major 3x3.  Queued on
+ * the handle's stream; shadow passes queued later see the new geometry and
+ * shadow passes in flight finish reading the old one first. */
+int axr_transform(axr_ctx *ctx, int group, const float *old_rm, const float *rot_mat, const float *origin,
+                  int v_start, int v_end);
+
+/* CLDraw.translate(coords, cStart, cEnd, tn) (Ops.py:499-508, vert.c:29-36):
+ * vertices [v_start, v_end) of a group move by coords; ordered as
+ * axr_transform. */
+int axr_translate(axr_ctx *ctx, int group, const float *coords, int v_start, int v_end);
+
+/* New: copies a group's vertex arrays to the host ([3*ntris][3] each; any
+ * pointer may be NULL) after the work queued before it on the handle's
+ * stream.  The reference keeps them in device buffers (Ops.py:618-620). */
+int axr_get_vertices(axr_ctx *ctx, int group, float *xyz, float *vn, float *li);
 
 /* CLDraw.copyTo(tn, vp, vn, cstart) (Ops.py:448-452): overwrite vertices
  * [3*tri_start, 3*(tri_start+ntris)) of a group. */

@@ -7,7 +7,7 @@
  *   - dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z, no fused multiply-add
  *   - min/max/clamp on floats = fminf/fmaxf (NaN -> the other operand)
  *   - float->int truncates toward zero, saturates, NaN -> 0 (f2i)
- *   - fast_normalize(v) = v * (1/sqrtf(dot(v,v)))
+ *   - fast_normalize(v) = v * (1/sqrtf(dot(v,v))), fast_length(v) = sqrtf(dot(v,v))
  *   - convert_ushort = truncate, then saturate to [0, 65535]
  *   - log2 = orc_log2f (correctly rounded, own series evaluation)
  */
@@ -995,5 +995,74 @@ void orc_gamma(uint16_t *r, uint16_t *g, uint16_t *b, int w, int h, float exposu
     r[p] = (uint16_t)f2i(fminf(255.f, jx));
     g[p] = (uint16_t)f2i(fminf(255.f, jy));
     b[p] = (uint16_t)f2i(fminf(255.f, jz));
+  }
+}
+
+
+/* ------------------------------------------------------------------ */
+/* vertex stage                                                        */
+/* ------------------------------------------------------------------ */
+
+static inline f3 f3max(f3 a, float s) { f3 r = {fmaxf(a.x, s), fmaxf(a.y, s), fmaxf(a.z, s)}; return r; }
+static inline float fast_length(f3 v) { return sqrtf(dot3(v, v)); }
+static inline void f3st(float *p, f3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+
+void orc_transform(float *xyz, float *vn, const float old_rm[9], const float rot_mat[9],
+                   const float origin[3], int start, int end) {
+  /* vert.c:3-28 with OldR = rows of oldRM and RR = rows of rotMat^T
+   * (CLDraw.rotate, Ops.py:481-497) */
+  f3 oldr[3], rr[3], o = f3ld(origin);
+  for (int i = 0; i < 3; i++) {
+    oldr[i] = f3ld(old_rm + 3 * i);
+    rr[i].x = rot_mat[i]; rr[i].y = rot_mat[3 + i]; rr[i].z = rot_mat[6 + i];
+  }
+  for (int v = start; v < end; v++) {
+    f3 p = f3sub(f3ld(xyz + 3 * (size_t)v), o);
+    f3 q = {dot3(p, oldr[0]), dot3(p, oldr[1]), dot3(p, oldr[2])};
+    f3 r = {dot3(q, rr[0]), dot3(q, rr[1]), dot3(q, rr[2])};
+    f3st(xyz + 3 * (size_t)v, f3add(r, o));
+    f3 n = f3ld(vn + 3 * (size_t)v);
+    f3 m = {dot3(n, oldr[0]), dot3(n, oldr[1]), dot3(n, oldr[2])};
+    f3 l = {dot3(m, rr[0]), dot3(m, rr[1]), dot3(m, rr[2])};
+    f3st(vn + 3 * (size_t)v, l);
+  }
+}
+
+void orc_translate(float *xyz, const float c[3], int start, int end) {
+  /* vert.c:29-36 */
+  f3 o = f3ld(c);
+  for (int v = start; v < end; v++) f3st(xyz + 3 * (size_t)v, f3add(f3ld(xyz + 3 * (size_t)v), o));
+}
+
+void orc_vert_light(const float *xyz, const float *vn, float *li, int nv,
+                    const float *dir_int, const float *dir_dir, int nd,
+                    const float *pint, const float *ppos, int np,
+                    const float *sint, const float *sdir, const float *spos, int ns, float amb) {
+  /* vert.c:38-88; light 0 is the primary light, shaded per pixel */
+  for (int v = 0; v < nv; v++) {
+    f3 x = f3ld(xyz + 3 * (size_t)v), n = f3ld(vn + 3 * (size_t)v);
+    f3 light = {0.f, 0.f, 0.f};
+    for (int i = 1; i < nd; i++) {   /* vert.c:57-60 */
+      float s = fmaxf(0.f, dot3(n, f3ld(dir_dir + 3 * i)) + 0.5f) * 0.66f;
+      light = f3add(light, f3smul(s, f3ld(dir_int + 3 * i)));
+    }
+    for (int i = 0; i < np; i++) {   /* vert.c:61-66 */
+      f3 pl = f3sub(x, f3ld(ppos + 3 * i));
+      if (dot3(n, pl) > 0.f) {
+        float fl = fast_length(pl);
+        float s = dot3(n, fast_normalize(pl)) / (1.f + fl * fl);
+        light = f3add(light, f3smul(s, f3ld(pint + 3 * i)));
+      }
+    }
+    for (int i = 0; i < ns; i++) {   /* vert.c:67-82 */
+      f3 pl = f3sub(x, f3ld(spos + 3 * i)), sd = f3ld(sdir + 3 * i);
+      if (dot3(sd, pl) > 0.f && dot3(n, pl) > 0.f) {
+        f3 u = fast_normalize(pl);
+        float fl = fast_length(pl);
+        float s = dot3(n, u) * dot3(u, sd) / (1.5f + fl * fl);
+        light = f3add(light, f3smul(s, f3ld(sint + 3 * i)));
+      }
+    }
+    f3st(li + 3 * (size_t)v, f3max(light, amb));   /* vert.c:83-86 */
   }
 }

@@ -113,6 +113,20 @@ long orc_coarse_counts(const orc_group *g, const orc_frame *f, int32_t *tile_cou
 /* Correctly rounded log2 used by the mip selection, exposed for tests. */
 float orc_log2f(float x);
 
+/* Vertex stage (Pipe/vert.c) on packed vertex arrays (3 floats a vertex).
+ * orc_transform: vertices [start, end) move to rot^T-rows . (old . (p - o)) + o
+ * and their normals to rot^T-rows . (old . n) (CLDraw.rotate).
+ * orc_translate: vertices [start, end) move by c (CLDraw.translate).
+ * orc_vert_light: li of nv vertices from directional lights 1..nd-1, np point
+ * and ns spot lights, floored at amb (CLDraw.vertLight). */
+void orc_transform(float *xyz, float *vn, const float old_rm[9], const float rot_mat[9],
+                   const float origin[3], int start, int end);
+void orc_translate(float *xyz, const float c[3], int start, int end);
+void orc_vert_light(const float *xyz, const float *vn, float *li, int nv,
+                    const float *dir_int, const float *dir_dir, int nd,
+                    const float *pint, const float *ppos, int np,
+                    const float *sint, const float *sdir, const float *spos, int ns, float amb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,7 @@ KERNELS = [
     ("ref_drawmin_alpha", "PyOpenCL27C/Shaders/drawminalpha.c"),
     ("ref_clearzb", "PyOpenCL27C/Shaders/clearzb.c"),
     ("ref_gamma", "PyOpenCL27C/Shaders/Post/gamma.c"),
+    ("ref_vert", "PyOpenCL27C/Pipe/vert.c"),
 ]
 
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",

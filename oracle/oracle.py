@@ -73,12 +73,56 @@ def lib():
         L.orc_coarse_counts.argtypes = [C.POINTER(OrcGroup), C.POINTER(OrcFrame), C.c_void_p]
         L.orc_log2f.restype = C.c_float
         L.orc_log2f.argtypes = [C.c_float]
+        L.orc_transform.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_int]
+        L.orc_translate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.orc_vert_light.argtypes = ([C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int]
+                                     + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_int, C.c_float])
         _lib = L
     return _lib
 
 
 def _ptr(a):
+    """Address of an array's data.  The caller keeps the array referenced
+    until the C call returns (a temporary is freed as soon as this returns)."""
     return a.ctypes.data if a is not None else None
+
+
+def _v3(a, n=None):
+    """float32 C-contiguous (k, 3) array (k = 0 for None)."""
+    if a is None:
+        return np.zeros((0, 3), np.float32)
+    return np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1, 3))
+
+
+def _m3(a):
+    return np.ascontiguousarray(np.asarray(a, np.float32).reshape(3, 3))
+
+
+def transform(xyz, vn, old_rm, rot_mat, origin, start=0, end=None):
+    """vert.transform on packed (V, 3) float32 arrays, in place (CLDraw.rotate)."""
+    end = xyz.shape[0] if end is None else end
+    o = np.asarray(origin, np.float32).reshape(3)
+    old, rot = _m3(old_rm), _m3(rot_mat)            # held until the call returns
+    lib().orc_transform(_ptr(xyz), _ptr(vn), _ptr(old), _ptr(rot), _ptr(o), start, end)
+
+
+def translate(xyz, coords, start=0, end=None):
+    """vert.Ttranslate on a packed (V, 3) float32 array, in place."""
+    end = xyz.shape[0] if end is None else end
+    c = np.asarray(coords, np.float32).reshape(3)
+    lib().orc_translate(_ptr(xyz), _ptr(c), start, end)
+
+
+def vert_light(xyz, vn, dir_int, dir_dir, amb, point_int=None, point_pos=None,
+               spot_int=None, spot_dir=None, spot_pos=None):
+    """vert.vertL: the per-vertex light I of (V, 3) positions and normals."""
+    di, dd, pi, pp, si, sd, sp = (_v3(a) for a in (dir_int, dir_dir, point_int, point_pos, spot_int, spot_dir,
+                                                   spot_pos))
+    x, n = np.ascontiguousarray(xyz, np.float32), np.ascontiguousarray(vn, np.float32)
+    li = np.empty_like(n)
+    lib().orc_vert_light(_ptr(x), _ptr(n), _ptr(li), li.shape[0], _ptr(di), _ptr(dd), di.shape[0], _ptr(pi), _ptr(pp), pi.shape[0],
+                         _ptr(si), _ptr(sd), _ptr(sp), si.shape[0], C.c_float(amb))
+    return li
 
 
 class Frame:
@@ -263,6 +307,15 @@ def ref_lib():
         R.ref_gamma.argtypes = [C.c_void_p, C.c_float]
         R.ref_overflow.restype = C.c_int
         R.ref_overflow.argtypes = [C.c_void_p]
+        R.ref_transform.restype = C.c_int
+        R.ref_transform.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3 + [C.c_int, C.c_int]
+        R.ref_translate.restype = C.c_int
+        R.ref_translate.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int]
+        R.ref_vert_light.restype = C.c_int
+        R.ref_vert_light.argtypes = ([C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 2 + [C.c_int]
+                                     + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_int, C.c_float])
+        R.ref_get_geometry.restype = C.c_int
+        R.ref_get_geometry.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3
         _ref = R
     return _ref
 
@@ -285,7 +338,8 @@ class RefDraw:
         pos = np.asarray(view.pos, np.float32)
         vv = np.ascontiguousarray(view.vv, np.float32)
         self.R.ref_set_view(self.h, _ptr(pos), _ptr(vv), view.sscale, view.cax, view.cay)
-        self.R.ref_set_light(self.h, _ptr(np.asarray(scene.lint, np.float32)), _ptr(np.asarray(scene.ldir, np.float32)))
+        self._light = (np.asarray(scene.lint, np.float32), np.asarray(scene.ldir, np.float32))
+        self.R.ref_set_light(self.h, _ptr(self._light[0]), _ptr(self._light[1]))
         self.flags = np.array([g.flags for g in scene.groups], np.int32)
         self.aidx = np.array([g.alpha_index for g in scene.groups], np.int32)
 
@@ -316,8 +370,8 @@ class RefDraw:
         sc = self.scene.shadows[k]
         if clear:
             self.R.ref_add_shadow_map(self.h, k, sc.dim, sc.scale)
-            self.R.ref_place_shadow_map(self.h, k, _ptr(np.asarray(sc.pos, np.float32)),
-                                        _ptr(np.ascontiguousarray(sc.vv, np.float32)))
+            p, vv = np.asarray(sc.pos, np.float32), np.ascontiguousarray(sc.vv, np.float32)
+            self.R.ref_place_shadow_map(self.h, k, _ptr(p), _ptr(vv))
             self.R.ref_clear_shadow_map(self.h, k)
         if cast is None:
             cast = [g.cast for g in self.scene.groups]
@@ -332,3 +386,27 @@ class RefDraw:
 
     def gamma(self, ex=1.0):
         self.R.ref_gamma(self.h, ex)
+
+    # vertex stage (Pipe/vert.c through CLDraw.rotate / translate / vertLight)
+    def rotate(self, old_rm, rot_mat, origin, start, end, tn):
+        o = np.asarray(origin, np.float32).reshape(3)
+        old, rot = _m3(old_rm), _m3(rot_mat)
+        return self.R.ref_transform(self.h, tn, _ptr(old), _ptr(rot), _ptr(o), start, end)
+
+    def translate(self, coords, start, end, tn):
+        c = np.asarray(coords, np.float32).reshape(3)
+        return self.R.ref_translate(self.h, tn, _ptr(c), start, end)
+
+    def vert_light(self, mask, dir_int, dir_dir, amb, point_int=None, point_pos=None,
+                   spot_int=None, spot_dir=None, spot_pos=None):
+        di, dd, pi, pp, si, sd, sp = (_v3(a) for a in (dir_int, dir_dir, point_int, point_pos, spot_int,
+                                                       spot_dir, spot_pos))
+        m = np.asarray(mask, np.uint8)
+        return self.R.ref_vert_light(self.h, _ptr(m), len(m), _ptr(di), _ptr(dd), di.shape[0], _ptr(pi), _ptr(pp),
+                                     pi.shape[0], _ptr(si), _ptr(sd), _ptr(sp), si.shape[0], C.c_float(amb))
+
+    def geometry(self, tn):
+        nv = self.scene.groups[tn].ntris * 3
+        xyz = np.empty((nv, 3), np.float32); vn = np.empty((nv, 3), np.float32); li = np.empty((nv, 3), np.float32)
+        self.R.ref_get_geometry(self.h, tn, _ptr(xyz), _ptr(vn), _ptr(li))
+        return xyz, vn, li

@@ -21,6 +21,7 @@
 namespace cl_shim {
 thread_local int g_group[2];
 thread_local int g_local[2];
+thread_local int g_global[2];
 
 namespace ref_trisetup {
 void setup(float3 *XYZ, float3 *VN, int *TIA, int *TIB, int *TNA, int *TNB, float2 *XY, float *ZZ,
@@ -72,6 +73,13 @@ void clearFrame(float *F, const int wF, const int hF, const int BS, const int le
 namespace ref_gamma {
 void g(ushort *Ro, ushort *Go, ushort *Bo, const float exposure, const int wF, const int hF, const int BS,
        const int stepW, const int stepH);
+}
+namespace ref_vert {
+void transform(float3 *XYZ, float3 *VN, float3 *OldR, float3 *RR, float *O, const int lStart, const int lEnd);
+void Ttranslate(float3 *XYZ, float *O, const int lStart, const int lEnd);
+void vertL(float3 *XYZ, float3 *VN, float3 *I, float3 *LInt, float3 *LDir, float3 *PInt, float3 *PPos,
+           float3 *SInt, float3 *SDir, float3 *SPos, const float ambLight, const char lenD, const short lenP,
+           const int lenS, const int lenV);
 }
 }  // namespace cl_shim
 
@@ -140,6 +148,25 @@ void grid1(int ng, int nthreads, F fn) {
 }
 
 float3 f3(const float *p) { return make_float3(p[0], p[1], p[2]); }
+
+std::vector<float3> f3s(const float *p, int n) {
+  std::vector<float3> v(n > 0 ? n : 1, make_float3(0, 0, 0));   // the reference binds a 4-byte buffer when empty
+  for (int i = 0; i < n; i++) v[i] = f3(p + 3 * (size_t)i);
+  return v;
+}
+
+// 1-D launch of `ng` groups of BS work-items with global ids set
+template <class F>
+void grid1_global(int ng, F fn) {
+  for (int bx = 0; bx < ng; bx++) {
+    g_group[0] = bx; g_group[1] = 0;
+    for (int tx = 0; tx < BS; tx++) {
+      g_local[0] = tx; g_local[1] = 0;
+      g_global[0] = bx * BS + tx; g_global[1] = 0;
+      fn();
+    }
+  }
+}
 
 }  // namespace
 
@@ -434,5 +461,73 @@ void ref_gamma(void *h, float ex) {
 }
 
 int ref_overflow(void *h) { return ((Ctx *)h)->overflow; }
+
+// CLDraw.rotate (Ops.py:481-497): vert.transform over vertices [start, end)
+// of group g, with OldR = oldRM and RR = rotMat transposed.
+int ref_transform(void *h, int g, const float *old_rm, const float *rot_mat, const float *origin, int start, int end) {
+  Ctx *c = (Ctx *)h;
+  if (g < 0 || g >= (int)c->groups.size()) return -1;
+  Group &G = c->groups[g];
+  if (start < 0 || end < start || end > G.V) return -1;
+  float3 oldr[3], rr[3];
+  for (int i = 0; i < 3; i++) {
+    oldr[i] = f3(old_rm + 3 * i);
+    rr[i] = make_float3(rot_mat[i], rot_mat[3 + i], rot_mat[6 + i]);
+  }
+  float o[3] = {origin[0], origin[1], origin[2]};
+  grid1_global((end - start) / BS + 1, [&] {
+    ref_vert::transform(G.xyz.data(), G.vn.data(), oldr, rr, o, start, end);
+  });
+  return 0;
+}
+
+// CLDraw.translate (Ops.py:499-508): vert.Ttranslate over [start, end)
+int ref_translate(void *h, int g, const float *coords, int start, int end) {
+  Ctx *c = (Ctx *)h;
+  if (g < 0 || g >= (int)c->groups.size()) return -1;
+  Group &G = c->groups[g];
+  if (start < 0 || end < start || end > G.V) return -1;
+  float o[3] = {coords[0], coords[1], coords[2]};
+  grid1_global((end - start) / BS + 1, [&] { ref_vert::Ttranslate(G.xyz.data(), o, start, end); });
+  return 0;
+}
+
+// CLDraw.vertLight (Ops.py:552-612): vert.vertL over every masked group
+int ref_vert_light(void *h, const uint8_t *mask, int n, const float *dir_int, const float *dir_dir, int nd,
+                   const float *pint, const float *ppos, int np, const float *sint, const float *sdir,
+                   const float *spos, int ns, float amb) {
+  Ctx *c = (Ctx *)h;
+  if (n != (int)c->groups.size()) return -1;
+  std::vector<float3> di = f3s(dir_int, nd), dd = f3s(dir_dir, nd), pi = f3s(pint, np), pp = f3s(ppos, np),
+                      si = f3s(sint, ns), sd = f3s(sdir, ns), sp = f3s(spos, ns);
+  for (int g = 0; g < n; g++) {
+    if (!mask[g]) continue;
+    Group &G = c->groups[g];
+    int lenV = G.V;
+    grid1(lenV / BS + 1, 1, [&](int, int) {
+      ref_vert::vertL(G.xyz.data(), G.vn.data(), G.li.data(), di.data(), dd.data(), pi.data(), pp.data(), si.data(),
+                      sd.data(), sp.data(), amb, (char)nd, (short)np, ns, lenV);
+    });
+  }
+  return 0;
+}
+
+// the vertex buffers of group g, packed as 3 floats per vertex
+int ref_get_geometry(void *h, int g, float *xyz, float *vn, float *li) {
+  Ctx *c = (Ctx *)h;
+  if (g < 0 || g >= (int)c->groups.size()) return -1;
+  const Group &G = c->groups[g];
+  for (int v = 0; v < G.V; v++) {
+    const float3 *src[3] = {&G.xyz[v], &G.vn[v], &G.li[v]};
+    float *dst[3] = {xyz, vn, li};
+    for (int k = 0; k < 3; k++)
+      if (dst[k]) {
+        dst[k][3 * (size_t)v] = src[k]->x;
+        dst[k][3 * (size_t)v + 1] = src[k]->y;
+        dst[k][3 * (size_t)v + 2] = src[k]->z;
+      }
+  }
+  return 0;
+}
 
 }  // extern "C"

@@ -7,7 +7,8 @@
 // harness sets the ids below before each call.  `__local` variables become
 // thread-local namespace-scope arrays that the harness can preload.
 // Float conventions match the oracle: no contraction (-ffp-contract=off),
-// min/max/clamp = fminf/fmaxf, fast_normalize = v * (1/sqrt(dot(v,v))).
+// min/max/clamp = fminf/fmaxf, fast_normalize = v * (1/sqrt(dot(v,v))),
+// fast_length = sqrt(dot(v,v)).
 #pragma once
 #include <math.h>
 #include <stdint.h>
@@ -21,8 +22,10 @@ typedef unsigned int uint;
 
 extern thread_local int g_group[2];
 extern thread_local int g_local[2];
+extern thread_local int g_global[2];
 inline int get_group_id(int d) { return g_group[d]; }
 inline int get_local_id(int d) { return g_local[d]; }
+inline int get_global_id(int d) { return g_global[d]; }
 #define CLK_GLOBAL_MEM_FENCE 1
 #define CLK_LOCAL_MEM_FENCE 2
 inline void barrier(int) {}
@@ -41,6 +44,8 @@ struct float3 {
     struct { float s0, s1, s2; };
   };
   float pad_;
+  float3() = default;
+  float3(float s) : pad_(0) { x = s; y = s; z = s; }   // OpenCL scalar-to-vector broadcast
 };
 struct int3 {
   union {
@@ -118,6 +123,8 @@ inline float sqrt(float x) { return ::sqrtf(x); }
 inline float3 sqrt(float3 a) { return make_float3(::sqrtf(a.x), ::sqrtf(a.y), ::sqrtf(a.z)); }
 inline int abs(int x) { return x < 0 ? (int)(0u - (unsigned)x) : x; }
 inline float3 fast_normalize(float3 v) { return v * (1.0f / ::sqrtf(dot(v, v))); }
+inline float fast_length(float3 v) { return ::sqrtf(dot(v, v)); }
+inline float3 max(float3 a, float s) { return make_float3(::fmaxf(a.x, s), ::fmaxf(a.y, s), ::fmaxf(a.z, s)); }
 inline int cvt_int(float x) {
   if (x != x) return 0;
   if (x >= 2147483648.0f) return INT_MAX;

@@ -14,6 +14,12 @@ Run in a checkout where the reference is present (it is read, never copied):
    field, and Utils.createMips (PyOpenCL27C/Utils.py:79-93) of an 8x8 RGB
    texture, imported from the reference with a stub for its unused numexpr
    import.
+3. ref_vertex.npz: the vertex stage through the reference's own
+   PyOpenCL27C/Pipe/vert.c kernels (oracle/_ref): a rotation about an origin
+   and a translation of vertex sub-ranges, then per-vertex light from
+   directional, point and spot lights, on a small seeded scene; the inputs
+   (vertex_ops()), the resulting vertex arrays, and digests of the shadow
+   maps and the frame rendered from them.
 """
 import hashlib
 import os
@@ -73,6 +79,66 @@ def frames():
     np.savez_compressed(os.path.join(HERE, "ref_frames.npz"), **out)
 
 
+def rot_mat(a, b, c):
+    """VertObject.rotate (PyOpenCL27C/VertObjects.py:281-294): rotX @ rotZ @ rotY."""
+    ca, sa, cb, sb, cc, sc = np.cos(a), np.sin(a), np.cos(b), np.sin(b), np.cos(c), np.sin(c)
+    rx = np.array([[1, 0, 0], [0, ca, -sa], [0, sa, ca]])
+    ry = np.array([[cb, 0, sb], [0, 1, 0], [-sb, 0, cb]])
+    rz = np.array([[cc, -sc, 0], [sc, cc, 0], [0, 0, 1]])
+    return rx @ rz @ ry
+
+
+def vertex_ops():
+    """Inputs of the vertex-stage fixture: the scene, the operations in
+    order, the lights.  Shared by the generator and the tests."""
+    r1 = rot_mat(0.3, 1.1, -0.4)
+    r2 = rot_mat(-0.7, 0.2, 0.9)
+    ops = [
+        # (kind, group, start vertex, end vertex, args)
+        ("rotate", 1, 37, 5001, (np.eye(3), r1, (1.5, 0.25, -2.0))),
+        ("rotate", 1, 37, 5001, (r1.T, r2, (1.5, 0.25, -2.0))),
+        ("translate", 0, 5, 1530, ((0.75, -0.5, 1.25),)),
+        ("rotate", 2, 0, 240, (np.eye(3), r1, (0.0, 0.0, 0.0))),
+    ]
+    lights = dict(
+        dir_int=np.array([(1.6, 1.4, 1.2), (0.5, 0.5, 0.5), (0.1, 0.2, 0.6)], np.float32),
+        dir_dir=np.array([(0.3, -0.8, 0.5), (-0.3, 0.8, -0.5), (0.0, 1.0, 0.0)], np.float32),
+        point_int=np.array([(3.0, 2.0, 1.0), (0.5, 1.5, 4.0)], np.float32),
+        point_pos=np.array([(2.0, 3.0, -1.0), (-6.0, 1.0, 4.0)], np.float32),
+        spot_int=np.array([(2.0, 2.0, 2.0), (1.0, 0.2, 0.2)], np.float32),
+        spot_dir=np.array([(0.0, -1.0, 0.0), (0.6, -0.8, 0.0)], np.float32),
+        spot_pos=np.array([(0.0, 6.0, 0.0), (-5.0, 4.0, -3.0)], np.float32),
+        amb=0.2, mask=(1, 1, 0))
+    return 3, (192, 144, (3, 4, -14)), ops, lights
+
+
+def vertex():
+    import oracle as O
+    from axi_visualizer_b200 import scenes as S
+    seed, (w, h, pos), ops, L = vertex_ops()
+    sc = S.scene_small(seed=seed, flags=0, with_alpha=True)
+    view = S.default_view(w, h, pos=pos)
+    rd = O.RefDraw(sc, view)
+    for kind, g, a, b, args in ops:
+        rc = rd.rotate(args[0], args[1], args[2], a, b, g) if kind == "rotate" else rd.translate(args[0], a, b, g)
+        assert rc == 0
+    assert rd.vert_light(L["mask"], L["dir_int"], L["dir_dir"], L["amb"], L["point_int"], L["point_pos"],
+                         L["spot_int"], L["spot_dir"], L["spot_pos"]) == 0
+    out = {}
+    for g in range(len(sc.groups)):
+        xyz, vn, li = rd.geometry(g)
+        out.update({f"g{g}_xyz": xyz, f"g{g}_vn": vn, f"g{g}_li": li})
+    for k in range(len(sc.shadows)):
+        rc, m = rd.shadow_map(k)
+        assert rc == 0
+        out[f"shm{k}_sha256"] = np.array(digest(m))
+    rd.clear_zbuffer()
+    assert rd.draw_all() == 0
+    for n, a in zip(("r", "g", "b", "db"), rd.get_frame()):
+        out[f"{n}_sha256"] = np.array(digest(a))
+    np.savez_compressed(os.path.join(HERE, "ref_vertex.npz"), **out)
+
+
 def terrain():
     sys.modules.setdefault("numexpr", types.ModuleType("numexpr"))
     sys.path.insert(0, os.path.join(REF, "PyOpenCL27C"))
@@ -101,4 +167,5 @@ def terrain():
 if __name__ == "__main__":
     frames()
     terrain()
+    vertex()
     print("golden fixtures written to", HERE)
