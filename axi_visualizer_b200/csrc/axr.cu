@@ -339,6 +339,20 @@ int group_table(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, co
     bool on = true;
     if (enabled_mask) on = mask_means_enabled ? enabled_mask[g] != 0 : enabled_mask[g] == 0;
     d.enabled = on ? 1 : 0;
+    if ((d.flags & F_MULTI) && (d.flags & F_ALPHA)) d.flags &= ~F_MULTI;   // the alpha material wins (Ops0.py:521-533)
+    if (d.flags & F_MULTI) {
+      // av_draw_multi.c samples this group's texture and the next three groups' at
+      // this group's side (the reference has no mip or shadow lookup in it)
+      d.flags &= ~(F_MIP | F_SHADOW);
+      if (G.mip_side != 0) return fail(AXR_EINVAL, "group %d: the multi material needs a single-level texture", g);
+      if (g + 3 >= ngroups)
+        return fail(AXR_EINVAL, "group %d: the multi material blends the textures of groups %d..%d, which do not exist",
+                    g, g + 1, g + 3);
+      for (int k = 1; k <= 3; k++)
+        if (c->groups[g + k].ntexels < (long)G.tex_size * G.tex_size)
+          return fail(AXR_EINVAL, "group %d: texture of group %d has fewer than %d x %d texels", g, g + k,
+                      G.tex_size, G.tex_size);
+    }
     if ((d.flags & F_MIP) && G.mip_side == 0)
       return fail(AXR_EINVAL, "group %d: mip flag on a group added without a mip chain", g);
     if (!(d.flags & F_MIP) && G.mip_side != 0)

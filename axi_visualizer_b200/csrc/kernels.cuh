@@ -1145,6 +1145,49 @@ __device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *s
   st.fmip = ms.fmip; st.mip = ms.mip; st.g = g;
 }
 
+// av_draw_multi.c:30-105: the 4-way terrain blend of a F_MULTI group.  Its
+// texture and the next three groups' (Ops0.py:533-545 binds TR[tn+1..tn+3])
+// are sampled at the same bilinear taps; blend weights come from the world
+// height and the normal; no shadow lookup.  The blended texel is converted
+// to u16 before the lighting product, as the source does.
+__device__ __forceinline__ void shade_multi(const DrawParams &P, const GroupDev *G, size_t pix, float t, float tz,
+                                            V2 uvi, const RowState &st) {
+  float omt = 1 - t;
+  Taps q = make_taps(uvi, tz, G[0].tex_size, 0);
+  V3 tx[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) tx[k] = bilerp_rgb(q, G[k].tex);
+  V3 col = mul3(add3(smul3(omt, st.c2.li), smul3(t, st.c1.li)), tz);
+  V3 nrm = fast_normalize(mul3(add3(smul3(omt, st.c2.n), smul3(t, st.c1.n)), tz));
+  V3 ldir{P.light.ldir[0], P.light.ldir[1], P.light.ldir[2]};
+  V3 lint{P.light.lint[0], P.light.lint[1], P.light.lint[2]};
+  V3 dc = smul3(fmaxf(0.f, dot3(nrm, ldir)), lint);
+  V3 cpos = mul3(add3(smul3(omt, st.c2.p), smul3(t, st.c1.p)), tz);
+  float m = (cpos.y - 15.f) / 4.f;
+  m = fminf(fmaxf(m, 0.f), 1.f);
+  float ny = fmaxf(0.f, fabsf(nrm.y) - 0.33f) * 1.5f;
+  m -= 1.5f * (ny * ny - 0.4f);
+  m = fminf(fmaxf(m, 0.f), 1.f);
+  V3 qv = div3(cpos, 3.f);
+  float threshy = 16.f + 2.f * fabsf(qv.x - roundf(qv.x)) + 2.f * fabsf(qv.z - roundf(qv.z));
+  float n = fminf(fmaxf((cpos.y - threshy) / 2.f, 0.f), 4.f);
+  n = n * n * n;
+  n += 1.5f * (ny * ny - 0.4f);
+  n = fminf(fmaxf(n, 0.f), 32.f);
+  float o = fminf(fmaxf((5.f - cpos.y) / 4.f, 0.f), 1.f);
+  if (m + n + o > 1.f) {   // each weight divides by the sum of the updated ones
+    n = n / (n + m + o);
+    m = m / (n + m + o);
+    o = o / (n + m + o);
+  }
+  float w1 = 1 - m - n - o;
+  const float light = 1;
+  P.ro[pix] = u16sat((float)u16sat(m * tx[1].x + n * tx[2].x + o * tx[3].x + w1 * tx[0].x) * (light * dc.x + col.x));
+  P.go[pix] = u16sat((float)u16sat(m * tx[1].y + n * tx[2].y + o * tx[3].y + w1 * tx[0].y) * (light * dc.y + col.y));
+  P.bo[pix] = u16sat((float)u16sat(m * tx[1].z + n * tx[2].z + o * tx[3].z + w1 * tx[0].z) * (light * dc.z + col.z));
+  P.db[pix] = tz;
+}
+
 // Shades pixel ax of row cy from its winner's row state.
 __device__ __forceinline__ void shade_from_row(const DrawParams &P, const GroupDev *sg, int ax, int cy,
                                                const RowState &st) {
@@ -1162,6 +1205,10 @@ __device__ __forceinline__ void shade_from_row(const DrawParams &P, const GroupD
   float tz = 1.0f / ((1 - t) * cz2 + t * cz1);
   float omt = 1 - t;
   V2 uvi = add2(smul2(omt, c2.uv), smul2(t, c1.uv));
+  if (G.flags & F_MULTI) {                 // the group table clears F_MULTI on alpha-tested groups
+    shade_multi(P, &G, (size_t)P.view.w * cy + ax, t, tz, uvi, st);
+    return;
+  }
   float outR, outG, outB;
   if (mip) {
     // av_draw_normmap_mip.c:73-123

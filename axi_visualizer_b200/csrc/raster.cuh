@@ -14,7 +14,8 @@
 
 namespace axr {
 
-enum { F_MIP = 1, F_ALPHA = 2, F_SHADOW = 4, F_CULL = 8 };
+// F_MULTI: av_draw_multi.c's 4-way blend with the next three groups' textures
+enum { F_MIP = 1, F_ALPHA = 2, F_SHADOW = 4, F_CULL = 8, F_MULTI = 16 };
 constexpr int TILE = 16;
 constexpr int SMALL_THRESH = 6;
 constexpr unsigned FULL = 0xffffffffu;

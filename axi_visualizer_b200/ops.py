@@ -406,9 +406,9 @@ class SceneRenderer:
             self.draw.addShadowMap(k, sc.dim, sc.scale, scene.amb)
             self.draw.placeShadowMapBasis(k, sc.pos, sc.vv, scene.amb)
         self.flags = [g.flags for g in scene.groups]
-        self.shaders = [{"alpha": g.alpha_index, **{k: 1 for k, b in (("mip", 1), ("shadow", 4), ("cull", 8))
-                                                     if g.flags & b}} if g.flags & 2 else
-                        " ".join(k for k, b in (("mip", 1), ("shadow", 4), ("cull", 8)) if g.flags & b)
+        names = (("mip", 1), ("shadow", 4), ("cull", 8), ("multi", 16))
+        self.shaders = [{"alpha": g.alpha_index, **{k: 1 for k, b in names if g.flags & b}} if g.flags & 2 else
+                        " ".join(k for k, b in names if g.flags & b)
                         for g in scene.groups]
 
     def shadow_pass(self):

@@ -28,7 +28,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-MIP, ALPHA, SHADOW, CULL = 1, 2, 4, 8
+MIP, ALPHA, SHADOW, CULL, MULTI = 1, 2, 4, 8, 16
 
 
 def flags_from_string(s) -> int:
@@ -46,6 +46,8 @@ def flags_from_string(s) -> int:
         f |= SHADOW
     if "cull" in keys:
         f |= CULL
+    if "multi" in keys:
+        f |= MULTI
     return f
 
 
@@ -388,6 +390,35 @@ def scene_small(seed=3, terrain_n=16, spheres=24, nquads=40, tex=64, alpha_tex=6
     shadows = [ShadowCam.facing(shadow_dim, shadow_dim / 2 / 30.0, (0, 0, 0), SUN),
                ShadowCam.facing(shadow_dim // 2, shadow_dim / 4 / 60.0, (0, 0, 0), SUN)]
     return _finish(groups, alphas, shadows)
+
+
+def scene_multi(seed=9, terrain_n=24, cell=2.0, tex=64, spheres=12, shadow_dim=256):
+    """A terrain in the 4-way blend material (av_draw_multi.c, as
+    PyOpenCL27C/3RandTerrain2.py uses it): heights from 0 to about 25 so the
+    sand (y < 5), rock (y > 15) and snow (y > 16 + ripple) weights and the
+    normal-dependent terms all occur.  Groups 1-3 are single quads whose
+    textures the blend samples (the demo's Rock, Snow and Sand planes);
+    group 4 is icospheres in the trilinear + shadow material."""
+    rng = np.random.default_rng(seed)
+    n = terrain_n
+    i = np.arange(n + 1)
+    hx, hz = np.meshgrid(i, i, indexing="ij")
+    h = 12.5 + 9.0 * np.sin(hx * 0.45 + rng.uniform(0, 6)) * np.cos(hz * 0.35 + rng.uniform(0, 6))
+    h += rng.standard_normal(h.shape) * 1.5
+    xyz, vn, uv = terrain_from_heights(h, cell, (-n * cell / 2, 0.0, -n * cell / 2), 1.0)
+    grass, _ = noise_texture(rng, tex)
+    groups = [_group(xyz, vn, uv, grass, MULTI | CULL, 0.2)]
+    for k in range(3):
+        qx, qn, qu = quads(rng, 1, -4, 4, 1.0, 2.0, ground=3.0 * k)
+        rgb, _ = noise_texture(rng, tex)
+        groups.append(_group(qx, qn, qu, rgb, 0, 0.2))
+    sx, sn, su = icospheres(rng, spheres, 0.5, 2.0, -n * cell / 3, n * cell / 3)
+    sx[:, 1] += 14.0
+    srgb, _ = noise_texture(rng, tex)
+    groups.append(_group(sx, sn, su, srgb, MIP | SHADOW | CULL, 0.2))
+    shadows = [ShadowCam.facing(shadow_dim, shadow_dim / 2 / 30.0, (0, 10, 0), SUN),
+               ShadowCam.facing(shadow_dim // 2, shadow_dim / 4 / 60.0, (0, 10, 0), SUN)]
+    return _finish(groups, [], shadows)
 
 
 def noise_rgb_fast(rng, n):

@@ -246,6 +246,54 @@ static float shadow_light(const shade_ctx *c, f3 p) {
   return light;
 }
 
+/* av_draw_multi.c:30-105: the 4-way terrain blend.  This group's texture and
+ * the next three groups' (Ops0.py:533-545 binds TR[tn+1..tn+3]) are sampled
+ * at the same bilinear taps (side lenT of this group); blend weights m, n, o
+ * come from the world height and the normal; no shadow lookup (light = 1).
+ * The blended texel is converted to u16 before the lighting product, and
+ * the product's implicit conversion to u16 is pinned as convert_ushort's. */
+static void multi_core(const shade_ctx *c, size_t pix, float t, float tz, f2 uvi, const attrs *a1,
+                       const attrs *a2) {
+  const orc_frame *f = c->f;
+  const orc_group *g = c->g;
+  float omt = 1 - t;
+  taps q = make_taps(uvi, tz, g->tex_size, 0);
+  float tr[4], tg[4], tb[4];
+  for (int k = 0; k < 4; k++) {
+    tr[k] = bilerp_u16(&q, g[k].tr);
+    tg[k] = bilerp_u16(&q, g[k].tg);
+    tb[k] = bilerp_u16(&q, g[k].tb);
+  }
+  f3 col = f3mul(f3add(f3smul(omt, a2->li), f3smul(t, a1->li)), tz);
+  f3 norm = fast_normalize(f3mul(f3add(f3smul(omt, a2->n), f3smul(t, a1->n)), tz));
+  f3 lint = {f->lint[0], f->lint[1], f->lint[2]};
+  f3 ldir = {f->ldir[0], f->ldir[1], f->ldir[2]};
+  f3 dirCol = f3smul(fmaxf(0.f, dot3(norm, ldir)), lint);
+  f3 cpos = f3mul(f3add(f3smul(omt, a2->p), f3smul(t, a1->p)), tz);
+  float m = (cpos.y - 15.f) / 4.f;
+  m = fclampf(m, 0.f, 1.f);
+  float ny = fmaxf(0.f, fabsf(norm.y) - 0.33f) * 1.5f;
+  m -= 1.5f * (ny * ny - 0.4f);
+  m = fclampf(m, 0.f, 1.f);
+  f3 qv = f3div(cpos, 3.f);
+  float threshy = 16.f + 2.f * fabsf(qv.x - roundf(qv.x)) + 2.f * fabsf(qv.z - roundf(qv.z));
+  float n = fclampf((cpos.y - threshy) / 2.f, 0.f, 4.f);
+  n = n * n * n;
+  n += 1.5f * (ny * ny - 0.4f);
+  n = fclampf(n, 0.f, 32.f);
+  float o = fclampf((5.f - cpos.y) / 4.f, 0.f, 1.f);
+  if (m + n + o > 1.f) {   /* each weight divides by the sum of the updated ones */
+    n = n / (n + m + o);
+    m = m / (n + m + o);
+    o = o / (n + m + o);
+  }
+  float w1 = 1 - m - n - o;
+  float light = 1;
+  f->ro[pix] = u16sat((float)u16sat(m * tr[1] + n * tr[2] + o * tr[3] + w1 * tr[0]) * (light * dirCol.x + col.x));
+  f->go[pix] = u16sat((float)u16sat(m * tg[1] + n * tg[2] + o * tg[3] + w1 * tg[0]) * (light * dirCol.y + col.y));
+  f->bo[pix] = u16sat((float)u16sat(m * tb[1] + n * tb[2] + o * tb[3] + w1 * tb[0]) * (light * dirCol.z + col.z));
+}
+
 /* One fragment at (cy, ax) with edge interpolants a1 (edge 1) and a2
  * (edge 2).  `zcur` points at the depth sample the test reads (the global
  * depth buffer in the serial model).  Returns 1 if it wrote. */
@@ -270,6 +318,12 @@ static int fragment(const shade_ctx *c, int tri, int cy, int ax, float t, float 
   /* Templates.py:74-91 + AVSL.py:238-239: `depth >= tz` (later wins ties) */
   if (!(f->db[pix] >= tz)) return 0;
   f->db[pix] = tz;
+  if ((flags & ORC_MULTI) && !(flags & ORC_ALPHA)) {
+    multi_core(c, pix, t, tz, uvi, a1, a2);
+    f->tri_id[pix] = c->gid_base + tri;
+    f->cov[pix] = 1;
+    return 1;
+  }
   float outR, outG, outB;
   if (flags & ORC_MIP) {
     /* av_draw_normmap_mip.c:73-123 */
@@ -721,6 +775,7 @@ int orc_draw_all(orc_frame *f, const orc_group *g, int ng, const uint8_t *mask,
     if (mask && mask[tn]) continue;
     if ((g[tn].flags & ORC_ALPHA) && (g[tn].alpha_index < 0 || g[tn].alpha_index >= nalpha)) return -2;
     if ((g[tn].flags & ORC_SHADOW) && nshadow < 1) return -3;
+    if ((g[tn].flags & ORC_MULTI) && !(g[tn].flags & ORC_ALPHA) && tn + 3 >= ng) return -4;
   }
   if (nthreads < 1) nthreads = 1;
   size_t npix = (size_t)f->w * f->h;

@@ -43,6 +43,7 @@ extern "C" {
 #define ORC_ALPHA  2
 #define ORC_SHADOW 4
 #define ORC_CULL   8
+#define ORC_MULTI 16   /* av_draw_multi.c: blend with the next three groups' textures */
 
 typedef struct orc_group {
   int ntris;

@@ -28,7 +28,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libaxr_ref.so")
 
-# (namespace, path inside the reference checkout)
+# (namespace, path inside the reference checkout[, prelude]); a prelude is
+# declared first inside the kernel's namespace
+SAT_STORES = "typedef sat_u16 ushort;"
 KERNELS = [
     ("ref_trisetup", "PyOpenCL27C/Pipe/trisetup.c"),
     ("ref_trisetup_cull", "PyOpenCL27C/Pipe/trisetup_cull.c"),
@@ -42,6 +44,8 @@ KERNELS = [
     ("ref_clearzb", "PyOpenCL27C/Shaders/clearzb.c"),
     ("ref_gamma", "PyOpenCL27C/Shaders/Post/gamma.c"),
     ("ref_vert", "PyOpenCL27C/Pipe/vert.c"),
+    # the 4-way blend stores `convert_ushort(blend) * light` into u16 planes
+    ("ref_drawmulti", "PyOpenCL27C/Shaders/drawmulti.c", SAT_STORES),
 ]
 
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
@@ -51,7 +55,7 @@ _VEC_LIT = re.compile(r"\((float|int|ushort|uchar)([234])\)\s*\(")
 _LOCAL_DECL = re.compile(r"__local\s+(\w+)\s+(\w+)\s*(\[[^\]]*\])?\s*;")
 
 
-def translate(src: str, ns: str) -> str:
+def translate(src: str, ns: str, prelude: str = "") -> str:
     """Mechanical OpenCL C -> C++ rewrite of one kernel file."""
     locals_ = _LOCAL_DECL.findall(src)
     body = _VEC_LIT.sub(lambda m: f"make_{m.group(1)}{m.group(2)}(", src)
@@ -63,7 +67,7 @@ def translate(src: str, ns: str) -> str:
     getters = ""
     for t, n, dim in locals_:
         getters += f"{t} *local_{n}() {{ return {'' if dim else '&'}{n}; }}\n"
-    return (f'#include "ref_shim.h"\nnamespace cl_shim {{ namespace {ns} {{\n'
+    return (f'#include "ref_shim.h"\nnamespace cl_shim {{ namespace {ns} {{\n{prelude}\n'
             f"{body}\n{defs}{getters}}} }}\n")
 
 
@@ -77,10 +81,10 @@ def build(reference: str = DEFAULT_REFERENCE, verbose: bool = False) -> str | No
         return None
     os.makedirs(OUT, exist_ok=True)
     objs = []
-    for ns, rel in KERNELS:
+    for ns, rel, *pre in KERNELS:
         path = os.path.join(reference, rel)
         with open(path) as f:
-            src = translate(f.read(), ns)
+            src = translate(f.read(), ns, pre[0] if pre else "")
         obj = os.path.join(OUT, ns + ".o")
         cmd = ["g++", *CXXFLAGS, "-I", HERE, "-x", "c++", "-c", "-", "-o", obj]
         if verbose:

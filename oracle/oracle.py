@@ -57,8 +57,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(ORACLE_SO):
-            build_oracle()
+        build_oracle()                  # rebuilds only when the source is newer
         L = C.CDLL(ORACLE_SO)
         L.orc_draw_all.restype = C.c_int
         L.orc_draw_all.argtypes = [C.POINTER(OrcFrame), C.POINTER(OrcGroup), C.c_int, C.c_void_p,

@@ -74,6 +74,19 @@ namespace ref_gamma {
 void g(ushort *Ro, ushort *Go, ushort *Bo, const float exposure, const int wF, const int hF, const int BS,
        const int stepW, const int stepH);
 }
+namespace ref_drawmulti {
+void draw(int *TO, int *TN, sat_u16 *Ro, sat_u16 *Go, sat_u16 *Bo, float *F, float2 *P, float *Z, float2 *UV,
+          float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, sat_u16 *TR, sat_u16 *TG, sat_u16 *TB,
+          const int lenT, sat_u16 *TR2, sat_u16 *TG2, sat_u16 *TB2, const int lenT2, sat_u16 *TR3, sat_u16 *TG3,
+          sat_u16 *TB3, const int lenT3, sat_u16 *TR4, sat_u16 *TG4, sat_u16 *TB4, const int lenT4, const int wF,
+          const int hF);
+void drawSmall(int *TO, sat_u16 *Ro, sat_u16 *Go, sat_u16 *Bo, float *F, float2 *P, float *Z, float2 *UV,
+               float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, sat_u16 *TR, sat_u16 *TG,
+               sat_u16 *TB, const int lenT, sat_u16 *TR2, sat_u16 *TG2, sat_u16 *TB2, const int lenT2,
+               sat_u16 *TR3, sat_u16 *TG3, sat_u16 *TB3, const int lenT3, sat_u16 *TR4, sat_u16 *TG4,
+               sat_u16 *TB4, const int lenT4, const int wF, const int hF, const int lenP);
+float *local_ZBuf();
+}
 namespace ref_vert {
 void transform(float3 *XYZ, float3 *VN, float3 *OldR, float3 *RR, float *O, const int lStart, const int lEnd);
 void Ttranslate(float3 *XYZ, float *O, const int lStart, const int lEnd);
@@ -148,6 +161,24 @@ void grid1(int ng, int nthreads, F fn) {
 }
 
 float3 f3(const float *p) { return make_float3(p[0], p[1], p[2]); }
+
+sat_u16 *su(std::vector<ushort> &v) { return reinterpret_cast<sat_u16 *>(v.data()); }
+
+// the 4-way blend material (Ops0.py:533-545, 604-617): this group's texture
+// and the next three groups'
+struct Multi {
+  sat_u16 *t[4][3];
+  int len[4];
+};
+Multi multi_textures(Ctx *c, int tn) {
+  Multi m;
+  for (int k = 0; k < 4; k++) {
+    Group &G = c->groups[tn + k];
+    m.t[k][0] = su(G.tr); m.t[k][1] = su(G.tg); m.t[k][2] = su(G.tb);
+    m.len[k] = G.tex_size;
+  }
+  return m;
+}
 
 std::vector<float3> f3s(const float *p, int n) {
   std::vector<float3> v(n > 0 ? n : 1, make_float3(0, 0, 0));   // the reference binds a 4-byte buffer when empty
@@ -287,9 +318,18 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
     int ns = newSize[tn] / BS + 1;
     if (newSize[tn] <= 0) continue;
     bool alpha = (flags[tn] & 2) != 0;
+    bool multi = !alpha && (flags[tn] & 16) != 0;
+    if (multi && tn + 3 >= ng) return -3;
     bool *TA = alpha ? (bool *)c->alphas[alpha_index[tn]].data() : nullptr;
     grid1(ns, nthreads, [&](int, int) {
-      if (alpha)
+      if (multi) {
+        Multi m = multi_textures(c, tn);
+        ref_drawmulti::drawSmall(G.toa.data(), su(c->ro), su(c->go), su(c->bo), c->db.data(), G.sp.data(),
+                                 G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), c->lint, c->ldir,
+                                 m.t[0][0], m.t[0][1], m.t[0][2], m.len[0], m.t[1][0], m.t[1][1], m.t[1][2], m.len[1],
+                                 m.t[2][0], m.t[2][1], m.t[2][2], m.len[2], m.t[3][0], m.t[3][1], m.t[3][2], m.len[3],
+                                 c->W, c->H, newSize[tn]);
+      } else if (alpha)
         ref_draw_alpha::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(),
                                   G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(),
                                   c->lint, c->ldir, G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, TA, c->W,
@@ -321,10 +361,12 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
       if (c->nbuf[t] > TILE_BUF) c->overflow = 1;
     if (c->overflow) return -2;  // the reference's bins overflow: result undefined
     bool alpha = (flags[tn] & 2) != 0;
+    bool multi = !alpha && (flags[tn] & 16) != 0;
+    if (multi && tn + 3 >= ng) return -3;
     bool *TA = alpha ? (bool *)c->alphas[alpha_index[tn]].data() : nullptr;
     int ntiles = c->WC * c->HC;
     auto tile = [&](int bx) {
-      float *zb = alpha ? ref_draw_alpha::local_ZBuf() : ref_draw::local_ZBuf();
+      float *zb = multi ? ref_drawmulti::local_ZBuf() : alpha ? ref_draw_alpha::local_ZBuf() : ref_draw::local_ZBuf();
       int tileX = bx % c->WC, tileY = bx / c->WC;
       for (int r = 0; r < 16; r++)
         for (int i = 0; i < 16; i++) zb[r * 16 + i] = c->db[(size_t)c->W * (tileY * 16 + r) + tileX * 16 + i];
@@ -333,7 +375,14 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
       for (int tx = 0; tx < BS; tx++) {
         c->nbuf[bx] = nb;
         g_local[0] = tx; g_local[1] = 0;
-        if (alpha)
+        if (multi) {
+          Multi m = multi_textures(c, tn);
+          ref_drawmulti::draw(c->ibuf.data(), c->nbuf.data(), su(c->ro), su(c->go), su(c->bo), c->db.data(),
+                              G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), c->lint,
+                              c->ldir, m.t[0][0], m.t[0][1], m.t[0][2], m.len[0], m.t[1][0], m.t[1][1], m.t[1][2],
+                              m.len[1], m.t[2][0], m.t[2][1], m.t[2][2], m.len[2], m.t[3][0], m.t[3][1], m.t[3][2],
+                              m.len[3], c->W, c->H);
+        } else if (alpha)
           ref_draw_alpha::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
                                c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),
                                G.xyz.data(), c->lint, c->ldir, G.tr.data(), G.tg.data(), G.tb.data(),

@@ -122,6 +122,7 @@ inline float ceil(float x) { return ::ceilf(x); }
 inline float sqrt(float x) { return ::sqrtf(x); }
 inline float3 sqrt(float3 a) { return make_float3(::sqrtf(a.x), ::sqrtf(a.y), ::sqrtf(a.z)); }
 inline int abs(int x) { return x < 0 ? (int)(0u - (unsigned)x) : x; }
+inline float round(float x) { return ::roundf(x); }
 inline float3 fast_normalize(float3 v) { return v * (1.0f / ::sqrtf(dot(v, v))); }
 inline float fast_length(float3 v) { return ::sqrtf(dot(v, v)); }
 inline float3 max(float3 a, float s) { return make_float3(::fmaxf(a.x, s), ::fmaxf(a.y, s), ::fmaxf(a.z, s)); }
@@ -137,6 +138,17 @@ inline ushort convert_ushort(float x) {
   return (ushort)(v < 0 ? 0 : (v > 65535 ? 65535 : v));
 }
 inline ushort convert_ushort_sat(float x) { return convert_ushort(x); }
+
+// A u16 buffer element whose implicit conversion from float (a store such as
+// `Ro[i] = x * y`, undefined out of range in C) is pinned as convert_ushort's
+// truncate-and-saturate.  Kernels whose stores rely on it see `ushort` as this
+// type (build_ref.py gives them a one-line prelude).
+struct sat_u16 {
+  unsigned short v;
+  operator float() const { return (float)v; }
+  sat_u16 &operator=(float x) { v = convert_ushort(x); return *this; }
+};
+static_assert(sizeof(sat_u16) == 2, "sat_u16 aliases a u16 buffer");
 inline float3 convert_float3(ushort3 a) { return make_float3((float)a.x, (float)a.y, (float)a.z); }
 
 }  // namespace cl_shim

@@ -14,6 +14,10 @@ Run in a checkout where the reference is present (it is read, never copied):
    field, and Utils.createMips (PyOpenCL27C/Utils.py:79-93) of an 8x8 RGB
    texture, imported from the reference with a stub for its unused numexpr
    import.
+4. ref_multi.npz: frames of the 4-way blend terrain material rendered by
+   the reference's own PyOpenCL27C/Shaders/drawmulti.c (oracle/_ref) on the
+   seeded scenes of MULTI_CASES (reference-kernel variant: the other groups
+   bilinear at their base level, no shadow lookup); SHA-256 digests.
 3. ref_vertex.npz: the vertex stage through the reference's own
    PyOpenCL27C/Pipe/vert.c kernels (oracle/_ref): a rotation about an origin
    and a translation of vertex sub-ranges, then per-vertex light from
@@ -77,6 +81,27 @@ def frames():
         if not k.endswith("sha256"):
             out[k + "_sha256"] = np.array(digest(out[k]))
     np.savez_compressed(os.path.join(HERE, "ref_frames.npz"), **out)
+
+
+MULTI_CASES = [  # (seed, width, height, camera position, target)
+    (9, 192, 144, (0, 30, -40), (0, 12, 0)),
+    (10, 192, 144, (5, 20, -20), (0, 12, 0)),
+    (9, 160, 128, (-10, 8, -12), (0, 12, 0)),
+]
+
+
+def multi():
+    import oracle as O
+    from axi_visualizer_b200 import scenes as S
+    out = {}
+    for i, (seed, w, h, pos, target) in enumerate(MULTI_CASES):
+        sc = S.reference_kernel_variant(S.scene_multi(seed=seed))
+        rd = O.RefDraw(sc, S.default_view(w, h, pos=pos, target=target))
+        rd.clear_zbuffer()
+        assert rd.draw_all() == 0
+        for n, a in zip(("r", "g", "b", "db"), rd.get_frame()):
+            out[f"m{i}_{n}_sha256"] = np.array(digest(a))
+    np.savez_compressed(os.path.join(HERE, "ref_multi.npz"), **out)
 
 
 def rot_mat(a, b, c):
@@ -168,4 +193,5 @@ if __name__ == "__main__":
     frames()
     terrain()
     vertex()
+    multi()
     print("golden fixtures written to", HERE)

@@ -100,3 +100,40 @@ def test_scene_terrain_matches_reference_vertterrain():
 def test_create_mips_matches_reference():
     z = np.load(os.path.join(GOLD, "ref_terrain.npz"))
     assert np.array_equal(S.create_mips(z["tex"]), z["mips"])
+
+
+# ---------------------------------------------------------------- 4-way blend material
+
+def _multi_cases():
+    sys.path.insert(0, GOLD)
+    import make_golden as MG
+    return MG.MULTI_CASES
+
+
+@pytest.mark.parametrize("i", range(3))
+def test_multi_material_equals_reference_golden(i):
+    """av_draw_multi.c through the reference's own drawmulti.c kernels
+    (tests/golden/ref_multi.npz) against the oracle: bit-exact."""
+    gold = np.load(os.path.join(GOLD, "ref_multi.npz"))
+    seed, w, h, pos, target = _multi_cases()[i]
+    sc = S.reference_kernel_variant(S.scene_multi(seed=seed))
+    fr, _ = O.render(sc, S.default_view(w, h, pos=pos, target=target))
+    for n, a in (("r", fr.ro), ("g", fr.go), ("b", fr.bo), ("db", fr.db)):
+        assert sha(a) == str(gold[f"m{i}_{n}_sha256"]), n
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [9, 11])
+@pytest.mark.parametrize("pos", [(0, 30, -40), (-10, 8, -12), (12, 4, 6)])
+def test_multi_material_equals_reference_kernels_live(seed, pos):
+    sc = S.reference_kernel_variant(S.scene_multi(seed=seed))
+    view = S.default_view(160, 128, pos=pos, target=(0, 12, 0))
+    fr, _ = O.render(sc, view)
+    rd = O.RefDraw(sc, view)
+    rd.clear_zbuffer()
+    assert rd.draw_all() == 0
+    r, g, b, db = rd.get_frame()
+    assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32))
+    assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo)
+    terrain = (fr.tri_id >= 0) & (fr.tri_id < sc.groups[0].ntris)
+    assert terrain.sum() > 1000 or pos == (12, 4, 6)
