@@ -38,6 +38,10 @@ extern "C" {
 #define AXR_ALPHA 2   /* "alpha": bilinear boolean alpha test before depth */
 #define AXR_SHADOW 4  /* "shadow": double-cascade 5-tap shadow lookup */
 #define AXR_CULL 8    /* "cull": back-face rejection (trisetup_cull.c:49-54) */
+#define AXR_MULTI 16  /* "multi": 4-way blend with the next three groups' textures
+                         (av_draw_multi.c; Ops0.py:533-545); needs a single-level
+                         texture and groups g+1..g+3 with >= side^2 texels; no mip or
+                         shadow lookup; ignored on AXR_ALPHA groups */
 
 typedef struct axr_ctx axr_ctx;
 
