@@ -134,6 +134,7 @@ struct axr_ctx {
   size_t lights_cap = 0;
   cudaEvent_t ev_lights = nullptr;
   bool lights_used = false;
+  uint16_t *post[3] = {nullptr, nullptr, nullptr};   // dof's gather target (SSRO/SSGO/SSBO)
   int light_blocks = 4;                      // resident 256-thread blocks of k_vert_light per SM
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
@@ -509,6 +510,7 @@ int axr_destroy(axr_ctx *c) {
   if (c->ev_lights) { cudaEventSynchronize(c->ev_lights); cudaEventDestroy(c->ev_lights); }
   cudaFree(c->d_lights);
   if (c->h_lights) cudaFreeHost(c->h_lights);
+  for (auto p : c->post) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -1020,6 +1022,40 @@ int axr_gamma(axr_ctx *c, float ex) {
   if (rc) return rc;
   long n = (long)c->w * c->h;
   launch(c, c->stream, "k_gamma", [&] { k_gamma<<<grid_for(c, n, 256, 8), 256, 0, c->stream>>>(c->ro, c->go, c->bo, (int)n, ex); });
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_ssao(axr_ctx *c, const float *rnd, int n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!rnd || n < 32) return fail(AXR_EINVAL, "ssao needs a random table of at least 32 floats (got %d)", n);
+  if (c->w < 16 || c->h < 16) return 0;          // no 16 x 16 work-group fits
+  SsaoParams S;
+  memcpy(S.rnd, rnd, sizeof S.rnd);
+  S.sscale = c->sscale;
+  dim3 grid(c->w / 16, c->h / 16);
+  launch(c, c->stream, "k_ssao", [&] { k_ssao<<<grid, 256, 0, c->stream>>>(c->ro, c->go, c->bo, c->db, c->w, c->h, S); });
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_dof(axr_ctx *c, float focus) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (c->w < 16 || c->h < 16) return 0;
+  size_t n = (size_t)c->w * c->h;
+  for (auto &p : c->post)
+    if (!p && cudaMalloc(&p, n * 2) != cudaSuccess) return fail(AXR_ENOMEM, "dof planes for %dx%d", c->w, c->h);
+  dim3 grid(c->w / 16, c->h / 16);
+  launch(c, c->stream, "k_dof", [&] {
+    k_dof<<<grid, 256, 0, c->stream>>>(c->ro, c->go, c->bo, c->db, c->w, c->h, focus, c->post[0], c->post[1],
+                                       c->post[2]);
+  });
+  // Ops.py:993-995 copies the gather back; rows below the covered region keep their colour
+  size_t bytes = (size_t)c->w * (c->h / 16 * 16) * 2;
+  uint16_t *dst[3] = {c->ro, c->go, c->bo};
+  for (int k = 0; k < 3; k++) CK(cudaMemcpyAsync(dst[k], c->post[k], bytes, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaGetLastError());
   return 0;
 }

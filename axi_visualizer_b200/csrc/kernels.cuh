@@ -156,6 +156,124 @@ __global__ void k_pack_rgb8(const uint16_t *__restrict__ r, const uint16_t *__re
   }
 }
 
+// ------------------------------------------------------------ post effects
+//
+// Post/ssao.c and Post/dof.c over the (w/16*16) x (h/16*16) region their
+// 16 x 16 work-groups cover (Ops.py:973-995); one thread a pixel, a block a
+// 16 x 16 tile.  Arithmetic in source order, one IEEE rounding an operation.
+
+struct SsaoParams {
+  float rnd[32];      // the random table (entries 0..31 of the reference's 48)
+  float sscale;
+};
+
+__device__ __forceinline__ V3 cross3(V3 a, V3 b) {
+  return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// ssao.c:6-97 in place on the colour planes; the depth row past the buffer
+// (read on the last row when h is a multiple of 16) reads 65535
+__global__ void __launch_bounds__(256) k_ssao(uint16_t *__restrict__ ro, uint16_t *__restrict__ go,
+                                              uint16_t *__restrict__ bo, const float *__restrict__ F, int w, int h,
+                                              SsaoParams S) {
+  const float radius = 1.f, bias = 0.002f;
+  __shared__ float rnd[32];                  // indexed per lane: staged out of the parameter space
+  if (threadIdx.x < 32) rnd[threadIdx.x] = S.rnd[threadIdx.x];
+  __syncthreads();
+  int cx = blockIdx.x * 16 + (threadIdx.x & 15), cy = blockIdx.y * 16 + (threadIdx.x >> 4);
+  size_t n = (size_t)w * h, pix = (size_t)w * cy + cx;
+  float w2 = (float)(w / 2), h2 = (float)(h / 2), ss = S.sscale;
+  float d = F[pix];
+  V3 pos = smul3(d, V3{((float)cx + 0.5f - w2) / ss, (-((float)cy + 0.5f - h2)) / ss, 1.f});
+  float dx = pix + 1 < n ? F[pix + 1] : 65535.f;
+  float dy = pix + w < n ? F[pix + w] : 65535.f;
+  V3 px = smul3(dx, V3{((float)cx + 0.5f + 1.f - w2) / ss, (-((float)cy + 0.5f - h2)) / ss, 1.f});
+  V3 py = smul3(dy, V3{((float)cx + 0.5f - w2) / ss, (-((float)cy + 0.5f + 1.f - h2)) / ss, 1.f});
+  V3 norm = fast_normalize(cross3(sub3(pos, px), sub3(pos, py)));   // rx * ry = 1
+  float ao = 0.f;
+  int c3 = 13 * ((cx * 3) & 7), c7 = 13 * ((cx * 7) & 7), c5 = 13 * ((cx * 5) & 7);
+  int y7 = 17 * ((cy * 7) & 7), y5 = 17 * ((cy * 5) & 7), y3 = 17 * ((cy * 3) & 7);
+#pragma unroll 4
+  for (int i = 0; i < 16; i++) {
+    V3 sv{rnd[(7 * i + c3 + y7) & 31], rnd[(7 * i + 1 + c7 + y5) & 31], rnd[(7 * i + 2 + c5 + y3) & 31]};
+    sv = sub3(mul3(sv, 2.f), V3{1.f, 1.f, 1.f});
+    sv = fast_normalize(sv);
+    if (dot3(sv, norm) < 0) sv = sub3(sv, mul3(smul3(2.f, norm), dot3(sv, norm)));
+    float rlen = rnd[(7 * i + 3 + c3 + y3) & 31];
+    sv = mul3(sv, rlen * rlen * radius);
+    sv = add3(sv, pos);
+    float sz = sv.z;
+    float sx = (sv.x / sz * ss) + w2;
+    float sy = (-sv.y / sz * ss) + h2;
+    if (sx >= 0 && sx < (float)w && sy >= 0 && sy < (float)h) {
+      float sampd = __ldg(F + (size_t)w * f2i(sy) + f2i(sx));
+      float disct = fminf(fmaxf(2.f - (d - sampd), 0.f), 1.f);
+      ao += disct * ((sampd < sz - bias) ? 1.f : 0.f);
+    }
+  }
+  ao /= 16.f;
+  if (d > 6000) ao = 0;
+  ao = fminf(fmaxf(ao * 2.f, 0.f), 1.f);
+  ro[pix] = u16sat((1 - ao) * (float)ro[pix]);
+  go[pix] = u16sat((1 - ao) * (float)go[pix]);
+  bo[pix] = u16sat((1 - ao) * (float)bo[pix]);
+}
+
+// dof.c:4-69: the circle-of-confusion gather into (r2, g2, b2).  The tile and
+// a 4-pixel halo (the largest radius) are staged in shared memory with each
+// source pixel's own circle of confusion.
+constexpr int DOF_HALO = 4, DOF_SIDE = 16 + 2 * DOF_HALO;
+__global__ void __launch_bounds__(256) k_dof(const uint16_t *__restrict__ ro, const uint16_t *__restrict__ go,
+                                             const uint16_t *__restrict__ bo, const float *__restrict__ F, int w,
+                                             int h, float focus, uint16_t *__restrict__ r2, uint16_t *__restrict__ g2,
+                                             uint16_t *__restrict__ b2) {
+  const float maxcoc = 4.f, aperture = 4.f;
+  __shared__ float ecs[DOF_SIDE * DOF_SIDE];
+  __shared__ ushort4 cs[DOF_SIDE * DOF_SIDE];
+  int x0 = blockIdx.x * 16 - DOF_HALO, y0 = blockIdx.y * 16 - DOF_HALO;
+  for (int k = threadIdx.x; k < DOF_SIDE * DOF_SIDE; k += blockDim.x) {
+    int sx = x0 + k % DOF_SIDE, sy = y0 + k / DOF_SIDE;
+    float e = 0.f;
+    ushort4 c = make_ushort4(0, 0, 0, 0);
+    if (sx >= 0 && sx < w && sy >= 0 && sy < h) {
+      size_t q = (size_t)w * sy + sx;
+      float f = F[q];
+      e = fminf(maxcoc, aperture * fabsf(f - focus) / focus / f);
+      c = make_ushort4(ro[q], go[q], bo[q], 0);
+    }
+    ecs[k] = e;
+    cs[k] = c;
+  }
+  __syncthreads();
+  int ix = blockIdx.x * 16 + (threadIdx.x & 15), iy = blockIdx.y * 16 + (threadIdx.x >> 4);
+  float cx = (float)ix + 0.5f, cy = (float)iy + 0.5f;
+  float d = F[(size_t)w * iy + ix];
+  float coc = aperture * fabsf(d - focus) / focus / d;
+  float dofR = 0, dofG = 0, dofB = 0, nsamples = 0;
+  float radius = fminf(maxcoc, coc);
+  float ylim = ceilf(cy + radius), xlim = ceilf(cx + radius);
+  int sx0 = f2i(floorf(cx - radius));
+  for (int sy = f2i(floorf(cy - radius)); (float)sy < ylim; sy++) {
+    float wy0 = 1.f - fmaxf(cy - radius - (float)sy, 0.f), wy1 = fminf(cy + radius - (float)sy, 1.f);
+    for (int sx = sx0; (float)sx < xlim; sx++) {
+      float cover = (1.f - fmaxf(cx - radius - (float)sx, 0.f)) * wy0;
+      cover *= fminf(cx + radius - (float)sx, 1.f) * wy1;
+      if (sx < 0 || sx >= w || sy < 0 || sy >= h) continue;
+      int k = (sy - y0) * DOF_SIDE + (sx - x0);
+      float ecoc = ecs[k];
+      if (radius > ecoc) cover *= ecoc / radius;
+      ushort4 c = cs[k];
+      dofR += (float)c.x * cover;
+      dofG += (float)c.y * cover;
+      dofB += (float)c.z * cover;
+      nsamples += cover;
+    }
+  }
+  dofR /= nsamples; dofG /= nsamples; dofB /= nsamples;
+  size_t pix = (size_t)w * iy + ix;
+  r2[pix] = u16sat(dofR); g2[pix] = u16sat(dofG); b2[pix] = u16sat(dofB);
+}
+
 // ------------------------------------------------------------ vertex stage
 //
 // Pipe/vert.c over a group's packed vertex arrays (3 floats a vertex).  A

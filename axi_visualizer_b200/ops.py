@@ -8,7 +8,7 @@ a caller can see:
   - errors raise `AxrError` (the reference raises pyopencl errors)
   - `getIDs()` is new: triangle id and coverage of the last drawAll
   - effects outside the rasterizer hot path (sky, particles, reflections,
-    SSR, cubemap re-layout, GI buffers, bones, waves) are not provided:
+    SSR, cubemap re-layout, GI buffers, bones, waves, bloom) are not provided:
     their methods raise NotImplementedError, except setSkyTex, which the
     engine calls unconditionally and which is accepted and ignored.
 """
@@ -273,6 +273,21 @@ class CLDraw:
     def setFrame(self, r=None, g=None, b=None, depth=None):
         arrs = [None if a is None else np.ascontiguousarray(a) for a in (r, g, b, depth)]
         check(self._L.axr_set_frame(self._h, *[_p(a) for a in arrs]), "setFrame")
+
+    def ssao(self, rand=None):
+        """Screen-space ambient occlusion on the frame in place (Post/ssao.c;
+        Ops.py:973-983).  The random table is drawn once, as the reference
+        does (np.random.rand(48)), unless `rand` gives one (>= 32 floats)."""
+        if rand is None:
+            if getattr(self, "_ssao_rand", None) is None:
+                self._ssao_rand = np.random.rand(48).astype(np.float32)
+            rand = self._ssao_rand
+        t = _f32(np.asarray(rand).reshape(-1))
+        check(self._L.axr_ssao(self._h, _p(t), t.size), "ssao")
+
+    def dof(self, focus):
+        """Depth-of-field gather on the frame (Post/dof.c; Ops.py:985-995)."""
+        check(self._L.axr_dof(self._h, float(np.float32(focus))), "dof")
 
     def gamma(self, ex):
         check(self._L.axr_gamma(self._h, float(ex)), "gamma")

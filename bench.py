@@ -451,6 +451,32 @@ def vertex_section(R, view, hbm, frames=100, warmup=5):
     return out
 
 
+def post_section(R, view, hbm, frames=50):
+    """Post effects on the 1080p frame (CLDraw.ssao, CLDraw.dof(8)) after
+    every rendered frame: their kernels' CUDA-event times and HBM throughput
+    at 16 algorithmic bytes a pixel each (depth and colour read, colour
+    written; the gathered neighbours are re-reads that stay in cache)."""
+    D = R.draw
+    rnd = np.random.default_rng(44).random(48).astype(np.float32)
+    for _ in range(3):
+        R.frame(view); D.ssao(rnd); D.dof(8.0)
+    D.sync()
+    D.setKernelTiming(True)
+    for _ in range(frames):
+        R.frame(view); D.ssao(rnd); D.dof(8.0)
+    kt = D.kernelTimes()
+    D.setKernelTiming(False)
+    D.sync()
+    px = view.w * (view.h // 16 * 16)
+    out = {"workload": "c2_post_1080p", "pixels": px}
+    for name in ("k_ssao", "k_dof"):
+        tot_ms, n = kt[name]
+        avg_s = tot_ms / n / 1000.0
+        gbs = 16 * px / avg_s / 1e9
+        out[name] = {"avg_us": avg_s * 1e6, "bytes_per_pixel": 16, "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm}
+    return out
+
+
 # ------------------------------------------------------------------ stress
 
 def stress_section(device, frames=10, log=progress):
@@ -843,6 +869,10 @@ def main():
     if extra and not args.no_vertex:
         progress("vertex stage")
         vertex = vertex_section(R, view, hbm, frames=min(args.steps, 100))
+    post = None
+    if extra and not args.no_vertex:
+        progress("post effects")
+        post = post_section(R, view, hbm, frames=min(args.steps, 50))
 
     small = None
     if extra and not args.no_small:
@@ -902,6 +932,7 @@ def main():
             "stress": stress,
             "small": small,
             "vertex": vertex,
+            "post": post,
         }
         print(json.dumps(line))
     ranks.close()

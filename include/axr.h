@@ -175,6 +175,20 @@ int axr_set_frame(axr_ctx *ctx, const uint16_t *r, const uint16_t *g, const uint
 /* CLDraw.gamma(ex) (Ops0.py:654-660, Post/gamma.c) on the colour planes. */
 int axr_gamma(axr_ctx *ctx, float exposure);
 
+/* CLDraw.ssao() (Ops.py:973-983, Post/ssao.c): screen-space ambient
+ * occlusion in place on the colour planes of the w/16*16 x h/16*16 region,
+ * from the depth buffer and a random table (rnd[0..31] are read; the
+ * reference draws 48 uniform floats once).  A depth read one row past the
+ * buffer (the kernel's neighbour on the last row when h is a multiple of 16)
+ * reads 65535.  Queued on the handle's stream. */
+int axr_ssao(axr_ctx *ctx, const float *rnd, int n);
+
+/* CLDraw.dof(focus) (Ops.py:985-995, Post/dof.c): depth-of-field gather of
+ * the w/16*16 x h/16*16 region (circle of confusion 4|d - focus|/focus/d,
+ * at most 4 pixels) replacing its colour; the rows below the region keep
+ * their colour.  Queued on the handle's stream. */
+int axr_dof(axr_ctx *ctx, float focus);
+
 /* CLDraw.addShadowMap(i, size, scale, ambLight) (Ops.py:1048-1070) */
 int axr_add_shadow_map(axr_ctx *ctx, int i, int size, float scale, float amb_light);
 

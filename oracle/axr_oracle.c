@@ -1121,3 +1121,94 @@ void orc_vert_light(const float *xyz, const float *vn, float *li, int nv,
     f3st(li + 3 * (size_t)v, f3max(light, amb));   /* vert.c:83-86 */
   }
 }
+
+
+/* ------------------------------------------------------------------ */
+/* post effects                                                        */
+/* ------------------------------------------------------------------ */
+
+static inline f3 f3cross(f3 a, f3 b) {
+  f3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  return r;
+}
+
+void orc_ssao(uint16_t *r, uint16_t *g, uint16_t *b, const float *db, int w, int h, float sscale,
+              const float *rnd) {
+  /* ssao.c:6-97 over the (h/16) x (w/16) work-groups of 16 x 16 (Ops.py:973-983) */
+  const float radius = 1.f, bias = 0.002f;
+  size_t n = (size_t)w * h;
+  int w2 = w / 2, h2 = h / 2;
+  for (int cy = 0; cy < h / 16 * 16; cy++)
+    for (int cx = 0; cx < w / 16 * 16; cx++) {
+      size_t pix = (size_t)w * cy + cx;
+      float ao = 0.f;
+      float d = db[pix];
+      f3 pv = {((float)cx + 0.5f - (float)w2) / sscale, (-((float)cy + 0.5f - (float)h2)) / sscale, 1.f};
+      f3 pos = f3smul(d, pv);
+      size_t ix = pix + 1, iy = pix + (size_t)w;
+      float dx = ix < n ? db[ix] : 65535.f;
+      float dy = iy < n ? db[iy] : 65535.f;
+      const int rx = 1, ry = 1;
+      f3 xv = {((float)cx + 0.5f + (float)rx - (float)w2) / sscale, (-((float)cy + 0.5f - (float)h2)) / sscale, 1.f};
+      f3 yv = {((float)cx + 0.5f - (float)w2) / sscale, (-((float)cy + 0.5f + (float)ry - (float)h2)) / sscale, 1.f};
+      f3 px = f3smul(dx, xv), py = f3smul(dy, yv);
+      f3 norm = f3smul((float)(rx * ry), fast_normalize(f3cross(f3sub(pos, px), f3sub(pos, py))));
+      for (int i = 0; i < 16; i++) {
+        f3 sv = {rnd[(7 * i + 13 * ((cx * 3) & 7) + 17 * ((cy * 7) & 7)) & 31],
+                 rnd[(7 * i + 1 + 13 * ((cx * 7) & 7) + 17 * ((cy * 5) & 7)) & 31],
+                 rnd[(7 * i + 2 + 13 * ((cx * 5) & 7) + 17 * ((cy * 3) & 7)) & 31]};
+        sv = f3sub(f3mul(sv, 2.f), (f3){1.f, 1.f, 1.f});
+        sv = fast_normalize(sv);
+        if (dot3(sv, norm) < 0) sv = f3sub(sv, f3mul(f3smul(2.f, norm), dot3(sv, norm)));
+        float rlen = rnd[(7 * i + 3 + 13 * ((cx * 3) & 7) + 17 * ((cy * 3) & 7)) & 31];
+        sv = f3mul(sv, rlen * rlen * radius);
+        sv = f3add(sv, pos);
+        float sz = sv.z;
+        float sx = (sv.x / sz * sscale) + (float)w2;
+        float sy = (-sv.y / sz * sscale) + (float)h2;
+        if (sx >= 0 && sx < (float)w && sy >= 0 && sy < (float)h) {
+          float sampd = db[(size_t)w * f2i(sy) + f2i(sx)];
+          float disct = fclampf(2.f - (d - sampd), 0.f, 1.f);
+          ao += disct * ((sampd < sz - bias) ? 1.f : 0.f);
+        }
+      }
+      ao /= 16.f;
+      if (d > 6000) ao = 0;
+      ao = fclampf(ao * 2.f, 0.f, 1.f);
+      r[pix] = u16sat((1 - ao) * (float)r[pix]);
+      g[pix] = u16sat((1 - ao) * (float)g[pix]);
+      b[pix] = u16sat((1 - ao) * (float)b[pix]);
+    }
+}
+
+void orc_dof(const uint16_t *r, const uint16_t *g, const uint16_t *b, const float *db, int w, int h,
+             float focus, uint16_t *r2, uint16_t *g2, uint16_t *b2) {
+  /* dof.c:4-69 over the (h/16) x (w/16) work-groups of 16 x 16 (Ops.py:985-995) */
+  const float maxcoc = 4.f, aperture = 4.f;
+  for (int iy = 0; iy < h / 16 * 16; iy++)
+    for (int ix = 0; ix < w / 16 * 16; ix++) {
+      float cx = (float)ix + 0.5f, cy = (float)iy + 0.5f;
+      float d = db[(size_t)w * iy + ix];
+      float coc = aperture * fabsf(d - focus) / focus / d;
+      float dofR = 0, dofG = 0, dofB = 0, nsamples = 0;
+      float radius = fminf(maxcoc, coc);
+      for (int sy = f2i(floorf(cy - radius)); (float)sy < ceilf(cy + radius); sy++)
+        for (int sx = f2i(floorf(cx - radius)); (float)sx < ceilf(cx + radius); sx++) {
+          float cover = (1.f - fmaxf(cx - radius - (float)sx, 0.f)) * (1.f - fmaxf(cy - radius - (float)sy, 0.f));
+          cover *= fminf(cx + radius - (float)sx, 1.f) * fminf(cy + radius - (float)sy, 1.f);
+          if (sx < 0 || sx >= w || sy < 0 || sy >= h) continue;
+          float ecoc = db[(size_t)w * sy + sx];
+          ecoc = aperture * fabsf(ecoc - focus) / focus / ecoc;
+          ecoc = fminf(maxcoc, ecoc);
+          if (radius > ecoc) cover *= ecoc / radius;
+          size_t q = (size_t)w * sy + sx;
+          dofR += (float)r[q] * cover;
+          dofG += (float)g[q] * cover;
+          dofB += (float)b[q] * cover;
+          nsamples += cover;
+        }
+      dofR /= nsamples; dofG /= nsamples; dofB /= nsamples;
+      size_t pix = (size_t)w * iy + ix;
+      r2[pix] = u16sat(dofR); g2[pix] = u16sat(dofG); b2[pix] = u16sat(dofB);
+    }
+}

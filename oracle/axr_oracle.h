@@ -114,6 +114,18 @@ long orc_coarse_counts(const orc_group *g, const orc_frame *f, int32_t *tile_cou
 /* Correctly rounded log2 used by the mip selection, exposed for tests. */
 float orc_log2f(float x);
 
+/* Post/ssao.c in place on the colour planes: 16 depth samples per pixel of
+ * the w/16*16 x h/16*16 region around its reconstructed position, from the
+ * random table rnd[32]; a depth read one row past the buffer (the last row
+ * when h is a multiple of 16) reads 65535. */
+void orc_ssao(uint16_t *r, uint16_t *g, uint16_t *b, const float *db, int w, int h, float sscale,
+              const float *rnd);
+
+/* Post/dof.c: depth-of-field gather of the w/16*16 x h/16*16 region into
+ * (r2, g2, b2) (the reference writes SSRO/SSGO/SSBO and copies them back). */
+void orc_dof(const uint16_t *r, const uint16_t *g, const uint16_t *b, const float *db, int w, int h,
+             float focus, uint16_t *r2, uint16_t *g2, uint16_t *b2);
+
 /* Vertex stage (Pipe/vert.c) on packed vertex arrays (3 floats a vertex).
  * orc_transform: vertices [start, end) move to rot^T-rows . (old . (p - o)) + o
  * and their normals to rot^T-rows . (old . n) (CLDraw.rotate).

@@ -44,6 +44,8 @@ KERNELS = [
     ("ref_clearzb", "PyOpenCL27C/Shaders/clearzb.c"),
     ("ref_gamma", "PyOpenCL27C/Shaders/Post/gamma.c"),
     ("ref_vert", "PyOpenCL27C/Pipe/vert.c"),
+    ("ref_ssao", "PyOpenCL27C/Shaders/Post/ssao.c"),
+    ("ref_dof", "PyOpenCL27C/Shaders/Post/dof.c"),
     # the 4-way blend stores `convert_ushort(blend) * light` into u16 planes
     ("ref_drawmulti", "PyOpenCL27C/Shaders/drawmulti.c", SAT_STORES),
 ]

@@ -72,6 +72,8 @@ def lib():
         L.orc_coarse_counts.argtypes = [C.POINTER(OrcGroup), C.POINTER(OrcFrame), C.c_void_p]
         L.orc_log2f.restype = C.c_float
         L.orc_log2f.argtypes = [C.c_float]
+        L.orc_ssao.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_float, C.c_void_p]
+        L.orc_dof.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_float] + [C.c_void_p] * 3
         L.orc_transform.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_int]
         L.orc_translate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.orc_vert_light.argtypes = ([C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int]
@@ -95,6 +97,21 @@ def _v3(a, n=None):
 
 def _m3(a):
     return np.ascontiguousarray(np.asarray(a, np.float32).reshape(3, 3))
+
+
+def ssao(fr, sscale, rnd):
+    """Post/ssao.c on a Frame's colour planes, in place (depth read only)."""
+    t = np.ascontiguousarray(np.asarray(rnd, np.float32).reshape(-1)[:32])
+    lib().orc_ssao(_ptr(fr.ro), _ptr(fr.go), _ptr(fr.bo), _ptr(fr.db), fr.w, fr.h, C.c_float(sscale), _ptr(t))
+
+
+def dof(fr, focus):
+    """Post/dof.c on a Frame: the gathered region replaces the colour planes;
+    pixels outside the (w/16*16) x (h/16*16) region keep their colour."""
+    r2, g2, b2 = fr.ro.copy(), fr.go.copy(), fr.bo.copy()
+    lib().orc_dof(_ptr(fr.ro), _ptr(fr.go), _ptr(fr.bo), _ptr(fr.db), fr.w, fr.h, C.c_float(focus),
+                  _ptr(r2), _ptr(g2), _ptr(b2))
+    fr.ro, fr.go, fr.bo = r2, g2, b2
 
 
 def transform(xyz, vn, old_rm, rot_mat, origin, start=0, end=None):
@@ -313,6 +330,8 @@ def ref_lib():
         R.ref_vert_light.restype = C.c_int
         R.ref_vert_light.argtypes = ([C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 2 + [C.c_int]
                                      + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_int, C.c_float])
+        R.ref_ssao.argtypes = [C.c_void_p, C.c_void_p]
+        R.ref_dof.argtypes = [C.c_void_p, C.c_float]
         R.ref_get_geometry.restype = C.c_int
         R.ref_get_geometry.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3
         _ref = R
@@ -409,3 +428,12 @@ class RefDraw:
         xyz = np.empty((nv, 3), np.float32); vn = np.empty((nv, 3), np.float32); li = np.empty((nv, 3), np.float32)
         self.R.ref_get_geometry(self.h, tn, _ptr(xyz), _ptr(vn), _ptr(li))
         return xyz, vn, li
+
+    # post effects (Post/ssao.c, Post/dof.c)
+    def ssao(self, rnd):
+        t = np.zeros(48, np.float32)
+        t[:32] = np.asarray(rnd, np.float32).reshape(-1)[:32]
+        self.R.ref_ssao(self.h, _ptr(t))
+
+    def dof(self, focus):
+        self.R.ref_dof(self.h, C.c_float(focus))

@@ -87,6 +87,14 @@ void drawSmall(int *TO, sat_u16 *Ro, sat_u16 *Go, sat_u16 *Bo, float *F, float2 
                sat_u16 *TB4, const int lenT4, const int wF, const int hF, const int lenP);
 float *local_ZBuf();
 }
+namespace ref_ssao {
+void ao(ushort *Ro, ushort *Go, ushort *Bo, float *F, const float sScale, float *R, const int wF, const int hF,
+        const int BS);
+}
+namespace ref_dof {
+void dof(ushort *Ro, ushort *Go, ushort *Bo, ushort *R2, ushort *G2, ushort *B2, float *F, const float focus,
+         const int wF, const int hF, const int BS);
+}
 namespace ref_vert {
 void transform(float3 *XYZ, float3 *VN, float3 *OldR, float3 *RR, float *O, const int lStart, const int lEnd);
 void Ttranslate(float3 *XYZ, float *O, const int lStart, const int lEnd);
@@ -577,6 +585,41 @@ int ref_get_geometry(void *h, int g, float *xyz, float *vn, float *li) {
       }
   }
   return 0;
+}
+
+// CLDraw.ssao (Ops.py:973-983): (H/16) x (W/16) work-groups of 16 x 16 over
+// the frame in place.  The kernel reads the depth one row past the buffer on
+// the last row when H is a multiple of 16; that row holds 65535 here.
+void ref_ssao(void *h, const float *rnd) {
+  Ctx *c = (Ctx *)h;
+  std::vector<float> F(c->db);
+  F.resize((size_t)c->W * (c->H + 1), 65535.f);
+  std::vector<float> R(rnd, rnd + 48);
+  const int s = 16;
+  for (int bx = 0; bx < c->H / s; bx++)
+    for (int by = 0; by < c->W / s; by++)
+      for (int tx = 0; tx < s; tx++)
+        for (int ty = 0; ty < s; ty++) {
+          g_group[0] = bx; g_group[1] = by; g_local[0] = tx; g_local[1] = ty;
+          ref_ssao::ao(c->ro.data(), c->go.data(), c->bo.data(), F.data(), c->sscale, R.data(), c->W, c->H, s);
+        }
+}
+
+// CLDraw.dof (Ops.py:985-995): the gather into SSRO/SSGO/SSBO, then copied
+// back to the frame
+void ref_dof(void *h, float focus) {
+  Ctx *c = (Ctx *)h;
+  std::vector<ushort> r2(c->ro), g2(c->go), b2(c->bo);
+  const int s = 16;
+  for (int bx = 0; bx < c->H / s; bx++)
+    for (int by = 0; by < c->W / s; by++)
+      for (int tx = 0; tx < s; tx++)
+        for (int ty = 0; ty < s; ty++) {
+          g_group[0] = bx; g_group[1] = by; g_local[0] = tx; g_local[1] = ty;
+          ref_dof::dof(c->ro.data(), c->go.data(), c->bo.data(), r2.data(), g2.data(), b2.data(), c->db.data(),
+                       focus, c->W, c->H, s);
+        }
+  c->ro = r2; c->go = g2; c->bo = b2;
 }
 
 }  // extern "C"

@@ -123,6 +123,10 @@ inline float sqrt(float x) { return ::sqrtf(x); }
 inline float3 sqrt(float3 a) { return make_float3(::sqrtf(a.x), ::sqrtf(a.y), ::sqrtf(a.z)); }
 inline int abs(int x) { return x < 0 ? (int)(0u - (unsigned)x) : x; }
 inline float round(float x) { return ::roundf(x); }
+inline float3 cross(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+inline float3 operator*(int s, float3 a) { return (float)s * a; }
 inline float3 fast_normalize(float3 v) { return v * (1.0f / ::sqrtf(dot(v, v))); }
 inline float fast_length(float3 v) { return ::sqrtf(dot(v, v)); }
 inline float3 max(float3 a, float s) { return make_float3(::fmaxf(a.x, s), ::fmaxf(a.y, s), ::fmaxf(a.z, s)); }

@@ -18,6 +18,10 @@ Run in a checkout where the reference is present (it is read, never copied):
    the reference's own PyOpenCL27C/Shaders/drawmulti.c (oracle/_ref) on the
    seeded scenes of MULTI_CASES (reference-kernel variant: the other groups
    bilinear at their base level, no shadow lookup); SHA-256 digests.
+5. ref_post.npz: Post/ssao.c and Post/dof.c of the reference (oracle/_ref)
+   applied to the frames of POST_CASES (ssao with the table POST_RAND, then
+   dof at each focus of POST_FOCUS); SHA-256 digests of the colour planes
+   after each step.
 3. ref_vertex.npz: the vertex stage through the reference's own
    PyOpenCL27C/Pipe/vert.c kernels (oracle/_ref): a rotation about an origin
    and a translation of vertex sub-ranges, then per-vertex light from
@@ -102,6 +106,38 @@ def multi():
         for n, a in zip(("r", "g", "b", "db"), rd.get_frame()):
             out[f"m{i}_{n}_sha256"] = np.array(digest(a))
     np.savez_compressed(os.path.join(HERE, "ref_multi.npz"), **out)
+
+
+POST_CASES = [  # (seed, width, height, camera position); 128 and 144 are multiples of 16
+    (3, 160, 128, (0, 8, -30)),
+    (1, 192, 144, (3, 2, -8)),
+    (2, 128, 100, (-20, 3, 5)),
+]
+POST_FOCUS = (2.0, 8.0, 20.0)
+
+
+def post_rand():
+    return np.random.default_rng(44).random(48).astype(np.float32)
+
+
+def post():
+    import oracle as O
+    from axi_visualizer_b200 import scenes as S
+    out = {}
+    rnd = post_rand()
+    for i, (seed, w, h, pos) in enumerate(POST_CASES):
+        sc = S.scene_small(seed=seed, flags=0, with_alpha=True)
+        rd = O.RefDraw(sc, S.default_view(w, h, pos=pos))
+        rd.clear_zbuffer()
+        assert rd.draw_all() == 0
+        rd.ssao(rnd)
+        r, g, b, _ = rd.get_frame()
+        out[f"p{i}_ssao_sha256"] = np.array(digest(np.stack((r, g, b))))
+        for f in POST_FOCUS:
+            rd.dof(f)
+            r, g, b, _ = rd.get_frame()
+            out[f"p{i}_dof{f:g}_sha256"] = np.array(digest(np.stack((r, g, b))))
+    np.savez_compressed(os.path.join(HERE, "ref_post.npz"), **out)
 
 
 def rot_mat(a, b, c):
@@ -194,4 +230,5 @@ if __name__ == "__main__":
     terrain()
     vertex()
     multi()
+    post()
     print("golden fixtures written to", HERE)
