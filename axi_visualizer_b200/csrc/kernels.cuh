@@ -172,13 +172,29 @@ __device__ __forceinline__ V3 cross3(V3 a, V3 b) {
 }
 
 // ssao.c:6-97 in place on the colour planes; the depth row past the buffer
-// (read on the last row when h is a multiple of 16) reads 65535
+// (read on the last row when h is a multiple of 16) reads 65535.  A pixel's
+// 16 sample directions depend on it only through cx mod 8 and cy mod 8, so
+// the block first builds the 64 x 16 normalised directions and length
+// factors (stride 17 float4 per (cx, cy) class: conflict-free reads), with
+// the same arithmetic as the per-pixel loop.  The two quotients by the
+// sample depth share one reciprocal (quot_by_recip: still the IEEE quotient).
 __global__ void __launch_bounds__(256) k_ssao(uint16_t *__restrict__ ro, uint16_t *__restrict__ go,
                                               uint16_t *__restrict__ bo, const float *__restrict__ F, int w, int h,
                                               SsaoParams S) {
   const float radius = 1.f, bias = 0.002f;
   __shared__ float rnd[32];                  // indexed per lane: staged out of the parameter space
+  __shared__ float4 tab[64 * 17];
   if (threadIdx.x < 32) rnd[threadIdx.x] = S.rnd[threadIdx.x];
+  __syncthreads();
+  for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {
+    int i = e & 15, mx = (e >> 4) & 7, my = e >> 7;
+    int c3 = 13 * ((mx * 3) & 7), c7 = 13 * ((mx * 7) & 7), c5 = 13 * ((mx * 5) & 7);
+    int y7 = 17 * ((my * 7) & 7), y5 = 17 * ((my * 5) & 7), y3 = 17 * ((my * 3) & 7);
+    V3 sv{rnd[(7 * i + c3 + y7) & 31], rnd[(7 * i + 1 + c7 + y5) & 31], rnd[(7 * i + 2 + c5 + y3) & 31]};
+    sv = fast_normalize(sub3(mul3(sv, 2.f), V3{1.f, 1.f, 1.f}));
+    float rlen = rnd[(7 * i + 3 + c3 + y3) & 31];
+    tab[(my * 8 + mx) * 17 + i] = make_float4(sv.x, sv.y, sv.z, rlen * rlen * radius);
+  }
   __syncthreads();
   int cx = blockIdx.x * 16 + (threadIdx.x & 15), cy = blockIdx.y * 16 + (threadIdx.x >> 4);
   size_t n = (size_t)w * h, pix = (size_t)w * cy + cx;
@@ -190,21 +206,17 @@ __global__ void __launch_bounds__(256) k_ssao(uint16_t *__restrict__ ro, uint16_
   V3 px = smul3(dx, V3{((float)cx + 0.5f + 1.f - w2) / ss, (-((float)cy + 0.5f - h2)) / ss, 1.f});
   V3 py = smul3(dy, V3{((float)cx + 0.5f - w2) / ss, (-((float)cy + 0.5f + 1.f - h2)) / ss, 1.f});
   V3 norm = fast_normalize(cross3(sub3(pos, px), sub3(pos, py)));   // rx * ry = 1
+  const float4 *T = tab + ((cy & 7) * 8 + (cx & 7)) * 17;
   float ao = 0.f;
-  int c3 = 13 * ((cx * 3) & 7), c7 = 13 * ((cx * 7) & 7), c5 = 13 * ((cx * 5) & 7);
-  int y7 = 17 * ((cy * 7) & 7), y5 = 17 * ((cy * 5) & 7), y3 = 17 * ((cy * 3) & 7);
 #pragma unroll 4
   for (int i = 0; i < 16; i++) {
-    V3 sv{rnd[(7 * i + c3 + y7) & 31], rnd[(7 * i + 1 + c7 + y5) & 31], rnd[(7 * i + 2 + c5 + y3) & 31]};
-    sv = sub3(mul3(sv, 2.f), V3{1.f, 1.f, 1.f});
-    sv = fast_normalize(sv);
+    float4 t = T[i];
+    V3 sv{t.x, t.y, t.z};
     if (dot3(sv, norm) < 0) sv = sub3(sv, mul3(smul3(2.f, norm), dot3(sv, norm)));
-    float rlen = rnd[(7 * i + 3 + c3 + y3) & 31];
-    sv = mul3(sv, rlen * rlen * radius);
-    sv = add3(sv, pos);
-    float sz = sv.z;
-    float sx = (sv.x / sz * ss) + w2;
-    float sy = (-sv.y / sz * ss) + h2;
+    sv = add3(mul3(sv, t.w), pos);
+    float sz = sv.z, y = span_recip(sz);
+    float sx = (quot_by_recip(sv.x, sz, y) * ss) + w2;
+    float sy = (quot_by_recip(-sv.y, sz, y) * ss) + h2;
     if (sx >= 0 && sx < (float)w && sy >= 0 && sy < (float)h) {
       float sampd = __ldg(F + (size_t)w * f2i(sy) + f2i(sx));
       float disct = fminf(fmaxf(2.f - (d - sampd), 0.f), 1.f);
