@@ -135,6 +135,7 @@ struct axr_ctx {
   cudaEvent_t ev_lights = nullptr;
   bool lights_used = false;
   uint16_t *post[3] = {nullptr, nullptr, nullptr};   // dof's gather target (SSRO/SSGO/SSBO)
+  uint16_t *bloom = nullptr;                           // the bloom's 9 half-resolution planes
   int light_blocks = 4;                      // resident 256-thread blocks of k_vert_light per SM
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
@@ -511,6 +512,7 @@ int axr_destroy(axr_ctx *c) {
   cudaFree(c->d_lights);
   if (c->h_lights) cudaFreeHost(c->h_lights);
   for (auto p : c->post) cudaFree(p);
+  cudaFree(c->bloom);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -1056,6 +1058,36 @@ int axr_dof(axr_ctx *c, float focus) {
   size_t bytes = (size_t)c->w * (c->h / 16 * 16) * 2;
   uint16_t *dst[3] = {c->ro, c->go, c->bo};
   for (int k = 0; k < 3; k++) CK(cudaMemcpyAsync(dst[k], c->post[k], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int axr_bloom(axr_ctx *c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  int wf = c->w / 2, hf = c->h / 2;
+  if (hf < 3) return 0;                              // no row of the bright pass
+  size_t plane = (size_t)wf * (hf + 8);
+  if (!c->bloom) {
+    if (cudaMalloc(&c->bloom, plane * 9 * 2) != cudaSuccess) return fail(AXR_ENOMEM, "bloom planes");
+    CK(cudaMemsetAsync(c->bloom, 0, plane * 9 * 2, c->stream));   // rows no pass writes read 0
+  }
+  BloomPlanes B;
+  for (int k = 0; k < 3; k++) {
+    B.br[k] = c->bloom + plane * k;
+    B.hb[k] = c->bloom + plane * (3 + k);
+    B.vb[k] = c->bloom + plane * (6 + k);
+  }
+  int bx = (wf + 127) / 128;
+  launch(c, c->stream, "k_bloom_bright", [&] {
+    k_bloom_bright<<<dim3(bx, hf - 2), 128, 0, c->stream>>>(c->ro, c->go, c->bo, wf, hf, B);
+  });
+  launch(c, c->stream, "k_bloom_blur_h", [&] { k_bloom_blur<true><<<dim3(bx, hf - 1), 128, 0, c->stream>>>(wf, hf, B); });
+  launch(c, c->stream, "k_bloom_blur_v", [&] { k_bloom_blur<false><<<dim3(bx, hf - 1), 128, 0, c->stream>>>(wf, hf, B); });
+  int fx = (2 * wf + 127) / 128;
+  launch(c, c->stream, "k_bloom_add", [&] {
+    k_bloom_add<<<dim3(fx, 2 * hf), 128, 0, c->stream>>>(c->ro, c->go, c->bo, c->w, wf, hf, B);
+  });
   CK(cudaGetLastError());
   return 0;
 }

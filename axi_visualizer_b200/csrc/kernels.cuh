@@ -286,6 +286,89 @@ __global__ void __launch_bounds__(256) k_dof(const uint16_t *__restrict__ ro, co
   r2[pix] = u16sat(dofR); g2[pix] = u16sat(dofG); b2[pix] = u16sat(dofB);
 }
 
+// Post/blur.c + Post/blur2.c (CLDraw.blur): the bloom.  Four passes, each
+// over the whole image before the next (the reference's barrier orders only
+// its work-group; the launch-wide order is the one its phases are written
+// for).  The half-resolution planes are wf x (hf + 8) with wf = w/2,
+// hf = h/2: rows no pass writes, and the 8 rows the vertical blur reads past
+// the image, stay 0.
+struct BloomPlanes {
+  uint16_t *br[3], *hb[3], *vb[3];   // bright pass, horizontal blur, vertical blur
+};
+
+__constant__ float c_bloom_w[9] = {0.00816f, 0.01384f, 0.02207f, 0.03306f, 0.04654f,
+                                   0.06157f, 0.07654f, 0.08941f, 0.09815f};   // taps 9..1
+
+// blur.c:22-34: rows [0, hf - 2) of the bright pass
+__global__ void k_bloom_bright(const uint16_t *__restrict__ ro, const uint16_t *__restrict__ go,
+                               const uint16_t *__restrict__ bo, int wf, int hf, BloomPlanes B) {
+  int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y;
+  if (cx >= wf || cy >= hf - 2) return;
+  int y1 = min(wf * (hf - 1) * 4, wf * cy * 4 + 1);
+  int x1 = min(wf * 2 - 1, cx * 2 + 1);
+  int i0 = wf * cy * 4 + cx * 2, i1 = y1 + cx * 2, i2 = wf * cy * 4 + x1, i3 = y1 + x1;
+  const uint16_t *f[3] = {ro, go, bo};
+  float c[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    c[k] = (float)((int)f[k][i0] / 4 + (int)f[k][i1] / 4 + (int)f[k][i2] / 4 + (int)f[k][i3] / 4);
+  float lum = (float)(0.3626 * (double)c[0] + 0.5152 * (double)c[1] + 0.1222 * (double)c[2]);
+#pragma unroll
+  for (int k = 0; k < 3; k++) B.br[k][(size_t)wf * cy + cx] = u16sat(c[k] * lum / 256.f / 256.f);
+}
+
+// blur.c:38-66 (HORIZONTAL) and blur2.c:22-50 (vertical): the 19-tap blur
+// of rows [0, hf - 1); the vertical lower taps are bounded by the half
+// width, as blur2.c writes it
+template <bool HORIZONTAL>
+__global__ void k_bloom_blur(int wf, int hf, BloomPlanes B) {
+  int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y;
+  if (cx >= wf || cy >= hf - 1) return;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const uint16_t *src = HORIZONTAL ? B.br[k] : B.hb[k];
+    const int pos = HORIZONTAL ? cx : cy;
+    const size_t step = HORIZONTAL ? 1 : (size_t)wf;
+    const uint16_t *c0 = src + (size_t)wf * cy + cx;
+    float a = 0.f;
+#pragma unroll
+    for (int d = 9; d >= 1; d--)
+      if (pos > d - 1) a = a + c_bloom_w[9 - d] * (float)c0[-(ptrdiff_t)(d * step)];
+    a += 0.10125f * (float)c0[0];
+#pragma unroll
+    for (int d = 1; d <= 9; d++)
+      if (pos < wf - d) a = a + c_bloom_w[9 - d] * (float)c0[d * step];
+    a /= 0.9f;
+    (HORIZONTAL ? B.hb[k] : B.vb[k])[(size_t)wf * cy + cx] = u16sat(a);
+  }
+}
+
+// blur2.c:54-79: the vertical blur upsampled bilinearly and added to the
+// frame's rows [0, 2 hf) and columns [0, 2 wf)
+__global__ void k_bloom_add(uint16_t *__restrict__ ro, uint16_t *__restrict__ go, uint16_t *__restrict__ bo, int w,
+                            int wf, int hf, BloomPlanes B) {
+  int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y;
+  if (cx >= 2 * wf || cy >= 2 * hf) return;
+  const int lenT = wf;
+  float texr1 = (float)cx / 2.f;
+  int tex1 = f2i(texr1);
+  texr1 -= (float)tex1;
+  float texr2 = (float)cy / 2.f;
+  int tex2 = f2i(texr2);
+  texr2 -= (float)tex2;
+  int t1n = min(tex1 + 1, lenT - 1), t2n = min(tex2 + 1, hf - 2);
+  int tex = tex1 + lenT * tex2, tex10 = t1n + lenT * tex2, tex01 = tex1 + lenT * t2n, tex11 = t1n + lenT * t2n;
+  float texi1 = 1 - texr1, texi2 = 1 - texr2;
+  uint16_t *f[3] = {ro, go, bo};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const uint16_t *T = B.vb[k];
+    uint16_t *p = f[k] + (size_t)w * cy + cx;
+    *p = u16sat((float)*p + (texi1 * texi2 * (float)T[tex] + texr1 * texi2 * (float)T[tex10] +
+                             texi1 * texr2 * (float)T[tex01] + texr1 * texr2 * (float)T[tex11]));
+  }
+}
+
 // ------------------------------------------------------------ vertex stage
 //
 // Pipe/vert.c over a group's packed vertex arrays (3 floats a vertex).  A

@@ -8,7 +8,7 @@ a caller can see:
   - errors raise `AxrError` (the reference raises pyopencl errors)
   - `getIDs()` is new: triangle id and coverage of the last drawAll
   - effects outside the rasterizer hot path (sky, particles, reflections,
-    SSR, cubemap re-layout, GI buffers, bones, waves, bloom) are not provided:
+    SSR, cubemap re-layout, GI buffers, bones, waves) are not provided:
     their methods raise NotImplementedError, except setSkyTex, which the
     engine calls unconditionally and which is accepted and ignored.
 """
@@ -289,6 +289,10 @@ class CLDraw:
         """Depth-of-field gather on the frame (Post/dof.c; Ops.py:985-995)."""
         check(self._L.axr_dof(self._h, float(np.float32(focus))), "dof")
 
+    def blur(self):
+        """The bloom on the frame in place (Post/blur.c + blur2.c; Ops.py:1009-1020)."""
+        check(self._L.axr_bloom(self._h), "blur")
+
     def gamma(self, ex):
         check(self._L.axr_gamma(self._h, float(ex)), "gamma")
 
@@ -393,7 +397,7 @@ class CLDraw:
     def __getattr__(self, name):
         if name in ("addTexture", "setReflTex", "setHostSkyTex", "addBoneWeights", "initBoneTransforms",
                     "setBoneTransform", "boneTransform", "setupWave", "updateWave",
-                    "highlight", "blur", "drawDirectional", "getGIM", "addOpacityMap", "clearShadowOpMap",
+                    "highlight", "drawDirectional", "getGIM", "addOpacityMap", "clearShadowOpMap",
                     "shadowClouds", "shadowCloudsOpacity", "tonemap", "mipShadowMap", "setPSTex", "drawPS"):
             raise NotImplementedError(f"CLDraw.{name} belongs to an effect outside the rasterizer hot path")
         raise AttributeError(name)

@@ -452,18 +452,25 @@ def vertex_section(R, view, hbm, frames=100, warmup=5):
 
 
 def post_section(R, view, hbm, frames=50):
-    """Post effects on the 1080p frame (CLDraw.ssao, CLDraw.dof(8)) after
-    every rendered frame: their kernels' CUDA-event times and HBM throughput
-    at 16 algorithmic bytes a pixel each (depth and colour read, colour
-    written; the gathered neighbours are re-reads that stay in cache)."""
+    """Post effects on the 1080p frame (CLDraw.ssao, CLDraw.dof(8),
+    CLDraw.blur) after every rendered frame: their kernels' CUDA-event times
+    and HBM throughput.  ssao and dof: 16 algorithmic bytes a pixel each
+    (depth and colour read, colour written; the gathered neighbours are
+    re-reads that stay in cache).  The bloom's four passes: 6 + 6 + 6 bytes
+    a half-resolution pixel and 12 a full-resolution one (colour read and
+    written by the final add)."""
     D = R.draw
     rnd = np.random.default_rng(44).random(48).astype(np.float32)
+
+    def step():
+        R.frame(view); D.ssao(rnd); D.dof(8.0); D.blur()
+
     for _ in range(3):
-        R.frame(view); D.ssao(rnd); D.dof(8.0)
+        step()
     D.sync()
     D.setKernelTiming(True)
     for _ in range(frames):
-        R.frame(view); D.ssao(rnd); D.dof(8.0)
+        step()
     kt = D.kernelTimes()
     D.setKernelTiming(False)
     D.sync()
@@ -474,6 +481,13 @@ def post_section(R, view, hbm, frames=50):
         avg_s = tot_ms / n / 1000.0
         gbs = 16 * px / avg_s / 1e9
         out[name] = {"avg_us": avg_s * 1e6, "bytes_per_pixel": 16, "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm}
+    names = ("k_bloom_bright", "k_bloom_blur_h", "k_bloom_blur_v", "k_bloom_add")
+    if all(k in kt for k in names):
+        half = (view.w // 2) * (view.h // 2)
+        us = sum(1000 * kt[k][0] / kt[k][1] for k in names)
+        b = 18 * half + 12 * view.w * view.h
+        out["bloom"] = {"avg_us": us, "passes_us": {k: 1000 * kt[k][0] / kt[k][1] for k in names},
+                        "algorithmic_bytes": b, "achieved_gbs": b / us / 1e3, "frac_of_hbm": b / us / 1e3 / hbm}
     return out
 
 

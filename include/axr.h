@@ -189,6 +189,14 @@ int axr_ssao(axr_ctx *ctx, const float *rnd, int n);
  * their colour.  Queued on the handle's stream. */
 int axr_dof(axr_ctx *ctx, float focus);
 
+/* CLDraw.blur() (Ops.py:1009-1020, Post/blur.c + Post/blur2.c): the bloom,
+ * in place on the colour planes.  A half-resolution bright pass, a 19-tap
+ * horizontal and a 19-tap vertical blur, then the bilinear upsample added
+ * to the frame; each pass covers the whole image before the next.  Rows of
+ * the half-resolution planes that no pass writes, and the 8 rows the
+ * vertical blur reads past them, read 0.  Queued on the handle's stream. */
+int axr_bloom(axr_ctx *ctx);
+
 /* CLDraw.addShadowMap(i, size, scale, ambLight) (Ops.py:1048-1070) */
 int axr_add_shadow_map(axr_ctx *ctx, int i, int size, float scale, float amb_light);
 

@@ -1212,3 +1212,84 @@ void orc_dof(const uint16_t *r, const uint16_t *g, const uint16_t *b, const floa
       r2[pix] = u16sat(dofR); g2[pix] = u16sat(dofG); b2[pix] = u16sat(dofB);
     }
 }
+
+static const float BLOOM_W[9] = {0.00816f, 0.01384f, 0.02207f, 0.03306f, 0.04654f,
+                                 0.06157f, 0.07654f, 0.08941f, 0.09815f};   /* taps 9..1 */
+
+void orc_bloom(uint16_t *r, uint16_t *g, uint16_t *b, int w, int h) {
+  int wf = w / 2, hf = h / 2;
+  size_t hn = (size_t)wf * (hf + 8);               /* 8 zero rows past the end */
+  uint16_t *br[3], *hb[3], *vb[3];
+  uint16_t *fr[3] = {r, g, b};
+  for (int k = 0; k < 3; k++) {
+    br[k] = (uint16_t *)calloc(hn, 2);
+    hb[k] = (uint16_t *)calloc(hn, 2);
+    vb[k] = (uint16_t *)calloc(hn, 2);
+  }
+  /* blur.c:22-34: bright pass at half resolution (the 4 taps of row 2cy at
+   * columns 2cx, 2cx+1, 2cx+1, 2cx+2 as the source indexes them) */
+  for (int cy = 0; cy < hf - 2; cy++)
+    for (int cx = 0; cx < wf; cx++) {
+      int y1 = imin(wf * (hf - 1) * 4, wf * cy * 4 + 1);
+      int x1 = imin(wf * 2 - 1, cx * 2 + 1);
+      float c[3];
+      for (int k = 0; k < 3; k++) {
+        const uint16_t *f = fr[k];
+        c[k] = (float)(f[wf * cy * 4 + cx * 2] / 4 + f[y1 + cx * 2] / 4 + f[wf * cy * 4 + x1] / 4 + f[y1 + x1] / 4);
+      }
+      float lum = (float)(0.3626 * (double)c[0] + 0.5152 * (double)c[1] + 0.1222 * (double)c[2]);
+      for (int k = 0; k < 3; k++) br[k][(size_t)wf * cy + cx] = u16sat(c[k] * lum / 256.f / 256.f);
+    }
+  /* blur.c:38-66: horizontal 19-tap blur of the bright pass */
+  for (int cy = 0; cy < hf - 1; cy++)
+    for (int cx = 0; cx < wf; cx++)
+      for (int k = 0; k < 3; k++) {
+        const uint16_t *row = br[k] + (size_t)wf * cy;
+        float a = 0.f;
+        for (int d = 9; d >= 1; d--)
+          if (cx > d - 1) a = a + BLOOM_W[9 - d] * (float)row[cx - d];
+        a += 0.10125f * (float)row[cx];
+        for (int d = 1; d <= 9; d++)
+          if (cx < wf - d) a = a + BLOOM_W[9 - d] * (float)row[cx + d];
+        a /= 0.9f;
+        hb[k][(size_t)wf * cy + cx] = u16sat(a);
+      }
+  /* blur2.c:22-50: vertical 19-tap blur; the lower taps are bounded by the
+   * half width, as the source writes it, so rows past the buffer read 0 */
+  for (int cy = 0; cy < hf - 1; cy++)
+    for (int cx = 0; cx < wf; cx++)
+      for (int k = 0; k < 3; k++) {
+        const uint16_t *col = hb[k] + cx;
+        float a = 0.f;
+        for (int d = 9; d >= 1; d--)
+          if (cy > d - 1) a = a + BLOOM_W[9 - d] * (float)col[(size_t)wf * (cy - d)];
+        a += 0.10125f * (float)col[(size_t)wf * cy];
+        for (int d = 1; d <= 9; d++)
+          if (cy < wf - d) a = a + BLOOM_W[9 - d] * (float)(cy + d < hf + 8 ? col[(size_t)wf * (cy + d)] : 0);
+        a /= 0.9f;
+        vb[k][(size_t)wf * cy + cx] = u16sat(a);
+      }
+  /* blur2.c:54-79: bilinear upsample added to the full-resolution frame */
+  int W2 = wf * 2, H2 = hf * 2, lenT = wf;
+  for (int cy = 0; cy < H2; cy++)
+    for (int cx = 0; cx < W2; cx++) {
+      float texr1 = (float)cx / 2.f;
+      int tex1 = f2i(texr1);
+      texr1 -= (float)tex1;
+      float texr2 = (float)cy / 2.f;
+      int tex2 = f2i(texr2);
+      texr2 -= (float)tex2;
+      int tex = tex1 + lenT * tex2;
+      int tex10 = imin(tex1 + 1, lenT - 1) + lenT * tex2;
+      int tex01 = tex1 + lenT * imin(tex2 + 1, H2 / 2 - 2);
+      int tex11 = imin(tex1 + 1, lenT - 1) + lenT * imin(tex2 + 1, H2 / 2 - 2);
+      float texi1 = 1 - texr1, texi2 = 1 - texr2;
+      for (int k = 0; k < 3; k++) {
+        const uint16_t *T = vb[k];
+        uint16_t *f = fr[k] + (size_t)w * cy + cx;
+        *f = u16sat((float)*f + (texi1 * texi2 * (float)T[tex] + texr1 * texi2 * (float)T[tex10] +
+                                 texi1 * texr2 * (float)T[tex01] + texr1 * texr2 * (float)T[tex11]));
+      }
+    }
+  for (int k = 0; k < 3; k++) { free(br[k]); free(hb[k]); free(vb[k]); }
+}

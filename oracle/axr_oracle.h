@@ -126,6 +126,14 @@ void orc_ssao(uint16_t *r, uint16_t *g, uint16_t *b, const float *db, int w, int
 void orc_dof(const uint16_t *r, const uint16_t *g, const uint16_t *b, const float *db, int w, int h,
              float focus, uint16_t *r2, uint16_t *g2, uint16_t *b2);
 
+/* Post/blur.c + Post/blur2.c (CLDraw.blur, Ops.py:1009-1020): the bloom,
+ * in place on the colour planes.  Each kernel's phases run one after the
+ * other over the whole image (the reference's barrier orders only one
+ * work-group; the intended order is the global one).  Half-resolution rows
+ * that no phase writes, and the rows the vertical blur reads past its
+ * buffer, read 0. */
+void orc_bloom(uint16_t *r, uint16_t *g, uint16_t *b, int w, int h);
+
 /* Vertex stage (Pipe/vert.c) on packed vertex arrays (3 floats a vertex).
  * orc_transform: vertices [start, end) move to rot^T-rows . (old . (p - o)) + o
  * and their normals to rot^T-rows . (old . n) (CLDraw.rotate).

@@ -46,12 +46,14 @@ KERNELS = [
     ("ref_vert", "PyOpenCL27C/Pipe/vert.c"),
     ("ref_ssao", "PyOpenCL27C/Shaders/Post/ssao.c"),
     ("ref_dof", "PyOpenCL27C/Shaders/Post/dof.c"),
+    ("ref_blur", "PyOpenCL27C/Shaders/Post/blur.c"),
+    ("ref_blur2", "PyOpenCL27C/Shaders/Post/blur2.c"),
     # the 4-way blend stores `convert_ushort(blend) * light` into u16 planes
     ("ref_drawmulti", "PyOpenCL27C/Shaders/drawmulti.c", SAT_STORES),
 ]
 
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
-            "-fopenmp", "-w", "-DBLOCK_SIZE=128"]
+            "-fopenmp", "-pthread", "-w", "-DBLOCK_SIZE=128"]
 
 _VEC_LIT = re.compile(r"\((float|int|ushort|uchar)([234])\)\s*\(")
 _LOCAL_DECL = re.compile(r"__local\s+(\w+)\s+(\w+)\s*(\[[^\]]*\])?\s*;")
@@ -96,7 +98,7 @@ def build(reference: str = DEFAULT_REFERENCE, verbose: bool = False) -> str | No
     harness = os.path.join(HERE, "ref_harness.cpp")
     hobj = os.path.join(OUT, "ref_harness.o")
     subprocess.run(["g++", *CXXFLAGS, "-I", HERE, "-c", harness, "-o", hobj], check=True)
-    subprocess.run(["g++", "-shared", "-fopenmp", "-o", LIB, hobj, *objs], check=True)
+    subprocess.run(["g++", "-shared", "-fopenmp", "-pthread", "-o", LIB, hobj, *objs], check=True)
     return LIB
 
 

@@ -74,6 +74,7 @@ def lib():
         L.orc_log2f.argtypes = [C.c_float]
         L.orc_ssao.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_float, C.c_void_p]
         L.orc_dof.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_float] + [C.c_void_p] * 3
+        L.orc_bloom.argtypes = [C.c_void_p] * 3 + [C.c_int, C.c_int]
         L.orc_transform.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_int]
         L.orc_translate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.orc_vert_light.argtypes = ([C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 2 + [C.c_int]
@@ -112,6 +113,11 @@ def dof(fr, focus):
     lib().orc_dof(_ptr(fr.ro), _ptr(fr.go), _ptr(fr.bo), _ptr(fr.db), fr.w, fr.h, C.c_float(focus),
                   _ptr(r2), _ptr(g2), _ptr(b2))
     fr.ro, fr.go, fr.bo = r2, g2, b2
+
+
+def bloom(fr):
+    """Post/blur.c + Post/blur2.c (CLDraw.blur) on a Frame's colour planes, in place."""
+    lib().orc_bloom(_ptr(fr.ro), _ptr(fr.go), _ptr(fr.bo), fr.w, fr.h)
 
 
 def transform(xyz, vn, old_rm, rot_mat, origin, start=0, end=None):
@@ -331,6 +337,7 @@ def ref_lib():
         R.ref_vert_light.argtypes = ([C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 2 + [C.c_int]
                                      + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 3 + [C.c_int, C.c_float])
         R.ref_ssao.argtypes = [C.c_void_p, C.c_void_p]
+        R.ref_bloom.argtypes = [C.c_void_p]
         R.ref_dof.argtypes = [C.c_void_p, C.c_float]
         R.ref_get_geometry.restype = C.c_int
         R.ref_get_geometry.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3
@@ -437,3 +444,6 @@ class RefDraw:
 
     def dof(self, focus):
         self.R.ref_dof(self.h, C.c_float(focus))
+
+    def bloom(self):
+        self.R.ref_bloom(self.h)

@@ -14,6 +14,9 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <vector>
 #include <omp.h>
 #include "ref_shim.h"
@@ -22,6 +25,7 @@ namespace cl_shim {
 thread_local int g_group[2];
 thread_local int g_local[2];
 thread_local int g_global[2];
+thread_local void (*g_barrier)() = nullptr;
 
 namespace ref_trisetup {
 void setup(float3 *XYZ, float3 *VN, int *TIA, int *TIB, int *TNA, int *TNB, float2 *XY, float *ZZ,
@@ -94,6 +98,14 @@ void ao(ushort *Ro, ushort *Go, ushort *Bo, float *F, const float sScale, float 
 namespace ref_dof {
 void dof(ushort *Ro, ushort *Go, ushort *Bo, ushort *R2, ushort *G2, ushort *B2, float *F, const float focus,
          const int wF, const int hF, const int BS);
+}
+namespace ref_blur {
+void blurH(ushort *r2, ushort *g2, ushort *b2, ushort *Rt, ushort *Gt, ushort *Bt, ushort *Ro, ushort *Go, ushort *Bo,
+           int wF, int hF, const int BS, int stepW, float stepH);
+}
+namespace ref_blur2 {
+void blurV(ushort *Ro, ushort *Go, ushort *Bo, ushort *Rt, ushort *Gt, ushort *Bt, ushort *r2, ushort *g2, ushort *b2,
+           int wF, int hF, const int BS, int stepW, float stepH);
 }
 namespace ref_vert {
 void transform(float3 *XYZ, float3 *VN, float3 *OldR, float3 *RR, float *O, const int lStart, const int lEnd);
@@ -169,6 +181,49 @@ void grid1(int ng, int nthreads, F fn) {
 }
 
 float3 f3(const float *p) { return make_float3(p[0], p[1], p[2]); }
+
+// a barrier across the threads of one launch (one thread per work-item)
+struct LaunchBarrier {
+  std::mutex m;
+  std::condition_variable cv;
+  int n = 0, waiting = 0;
+  long gen = 0;
+  void wait() {
+    std::unique_lock<std::mutex> lk(m);
+    long g = gen;
+    if (++waiting == n) {
+      waiting = 0;
+      gen++;
+      cv.notify_all();
+    } else {
+      cv.wait(lk, [&] { return gen != g; });
+    }
+  }
+};
+LaunchBarrier *g_launch_barrier = nullptr;
+void launch_barrier_wait() { g_launch_barrier->wait(); }
+
+// runs fn(bx, by, tx, ty) for every work-item of an (sx x sy) x (tx x ty)
+// launch, one thread each, with barrier() ordering the whole launch
+template <class F>
+void launch_threads(int gx, int gy, int lx, int ly, F fn) {
+  LaunchBarrier b;
+  b.n = gx * gy * lx * ly;
+  g_launch_barrier = &b;
+  std::vector<std::thread> th;
+  for (int by = 0; by < gy; by++)
+    for (int bx = 0; bx < gx; bx++)
+      for (int ty = 0; ty < ly; ty++)
+        for (int tx = 0; tx < lx; tx++)
+          th.emplace_back([=] {
+            g_group[0] = bx; g_group[1] = by; g_local[0] = tx; g_local[1] = ty;
+            g_barrier = launch_barrier_wait;
+            fn();
+            g_barrier = nullptr;
+          });
+  for (auto &t : th) t.join();
+  g_launch_barrier = nullptr;
+}
 
 sat_u16 *su(std::vector<ushort> &v) { return reinterpret_cast<sat_u16 *>(v.data()); }
 
@@ -620,6 +675,27 @@ void ref_dof(void *h, float focus) {
                        focus, c->W, c->H, s);
         }
   c->ro = r2; c->go = g2; c->bo = b2;
+}
+
+// CLDraw.blur (Ops.py:1009-1020): blurH then blurV, 4 x 4 work-groups of
+// 4 x 4, stepW 16, stepH ceil(H/16); each launch runs one thread per
+// work-item so that its barrier orders the whole launch.  The half-size
+// buffers start at 0 and carry 8 zero rows past their end (blurV reads
+// that far below its last row).
+void ref_bloom(void *h) {
+  Ctx *c = (Ctx *)h;
+  size_t hn = (size_t)(c->W / 2) * (c->H / 2 + 8);
+  std::vector<ushort> r2(hn, 0), g2(hn, 0), b2(hn, 0), r3(hn, 0), g3(hn, 0), b3(hn, 0);
+  const int s = 4, t = 4;
+  float stepH = ceilf((float)c->H / (float)(s * t));
+  launch_threads(s, s, t, t, [&] {
+    ref_blur::blurH(c->ro.data(), c->go.data(), c->bo.data(), r2.data(), g2.data(), b2.data(), r3.data(), g3.data(),
+                    b3.data(), c->W, c->H, t, s * t, stepH);
+  });
+  launch_threads(s, s, t, t, [&] {
+    ref_blur2::blurV(r2.data(), g2.data(), b2.data(), r3.data(), g3.data(), b3.data(), c->ro.data(), c->go.data(),
+                     c->bo.data(), c->W, c->H, t, s * t, stepH);
+  });
 }
 
 }  // extern "C"

@@ -28,7 +28,11 @@ inline int get_local_id(int d) { return g_local[d]; }
 inline int get_global_id(int d) { return g_global[d]; }
 #define CLK_GLOBAL_MEM_FENCE 1
 #define CLK_LOCAL_MEM_FENCE 2
-inline void barrier(int) {}
+// Kernels run one work-item at a time need no barrier.  Kernels whose
+// barrier is meant to order the whole launch run one thread per work-item,
+// and the harness points g_barrier at a barrier across all of them.
+extern thread_local void (*g_barrier)();
+inline void barrier(int) { if (g_barrier) g_barrier(); }
 inline int atomic_inc(volatile int *p) { return __atomic_fetch_add((int *)p, 1, __ATOMIC_RELAXED); }
 
 struct int3;

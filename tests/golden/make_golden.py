@@ -18,10 +18,11 @@ Run in a checkout where the reference is present (it is read, never copied):
    the reference's own PyOpenCL27C/Shaders/drawmulti.c (oracle/_ref) on the
    seeded scenes of MULTI_CASES (reference-kernel variant: the other groups
    bilinear at their base level, no shadow lookup); SHA-256 digests.
-5. ref_post.npz: Post/ssao.c and Post/dof.c of the reference (oracle/_ref)
-   applied to the frames of POST_CASES (ssao with the table POST_RAND, then
-   dof at each focus of POST_FOCUS); SHA-256 digests of the colour planes
-   after each step.
+5. ref_post.npz: Post/ssao.c, Post/dof.c and the bloom of Post/blur.c +
+   blur2.c of the reference (oracle/_ref) applied to the frames of
+   POST_CASES (ssao with the table post_rand(), dof at each focus of
+   POST_FOCUS, then the bloom); SHA-256 digests of the colour planes after
+   each step.
 3. ref_vertex.npz: the vertex stage through the reference's own
    PyOpenCL27C/Pipe/vert.c kernels (oracle/_ref): a rotation about an origin
    and a translation of vertex sub-ranges, then per-vertex light from
@@ -137,6 +138,9 @@ def post():
             rd.dof(f)
             r, g, b, _ = rd.get_frame()
             out[f"p{i}_dof{f:g}_sha256"] = np.array(digest(np.stack((r, g, b))))
+        rd.bloom()
+        r, g, b, _ = rd.get_frame()
+        out[f"p{i}_bloom_sha256"] = np.array(digest(np.stack((r, g, b))))
     np.savez_compressed(os.path.join(HERE, "ref_post.npz"), **out)
 
 

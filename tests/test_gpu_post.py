@@ -1,5 +1,6 @@
-"""CLDraw.ssao / CLDraw.dof on the device (k_ssao, k_dof through the C ABI)
-against the oracle on the same frame: bit-exact colour planes.  The frame is
+"""CLDraw.ssao / dof / blur on the device (k_ssao, k_dof and the k_bloom_*
+passes through the C ABI) against the oracle on the same frame: bit-exact
+colour planes.  The frame is
 set from the oracle's own render, so the comparison is of the post effects
 alone; depth is left untouched by both."""
 import numpy as np
@@ -11,7 +12,7 @@ from axi_visualizer_b200 import scenes as S
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("size", [(160, 128), (192, 100), (320, 240)])
+@pytest.mark.parametrize("size", [(160, 128), (192, 101), (320, 240)])
 @pytest.mark.parametrize("seed", [1, 3])
 def test_ssao_dof_match_oracle(size, seed):
     from axi_visualizer_b200.ops import SceneRenderer
@@ -34,6 +35,11 @@ def test_ssao_dof_match_oracle(size, seed):
         O.dof(fr, f)
         r, g, b, _ = [x.copy() for x in d.getFrame()]
         assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo), f"dof {f}"
+    for rep in range(2):                       # the bloom twice: its planes keep no state between calls
+        d.blur()
+        O.bloom(fr)
+        r, g, b, _ = [x.copy() for x in d.getFrame()]
+        assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo), f"bloom {rep}"
 
 
 def test_ssao_default_table_and_errors():

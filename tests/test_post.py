@@ -1,4 +1,5 @@
-"""Post/ssao.c and Post/dof.c in the oracle, pinned to the reference: golden
+"""Post/ssao.c, Post/dof.c and the bloom (Post/blur.c + blur2.c) in the
+oracle, pinned to the reference: golden
 digests made by the reference's own kernels (tests/golden/ref_post.npz) and,
 where oracle/_ref is built, the kernels run live.  Bit-exact."""
 import hashlib
@@ -36,6 +37,8 @@ def test_post_effects_equal_reference_golden(i):
     for f in MG.POST_FOCUS:
         O.dof(fr, f)
         assert sha(np.stack((fr.ro, fr.go, fr.bo))) == str(gold[f"p{i}_dof{f:g}_sha256"]), f
+    O.bloom(fr)
+    assert sha(np.stack((fr.ro, fr.go, fr.bo))) == str(gold[f"p{i}_bloom_sha256"])
 
 
 @needs_ref
@@ -59,6 +62,12 @@ def test_post_effects_equal_reference_kernels_live(seed, size):
         O.dof(fr, f)
         r, g, b, _ = rd.get_frame()
         assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo), f
+    before = fr.ro.copy()
+    rd.bloom()
+    O.bloom(fr)
+    r, g, b, _ = rd.get_frame()
+    assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo), "bloom"
+    assert (fr.ro != before).mean() > 0.3
 
 
 def test_dof_leaves_rows_below_the_region():
