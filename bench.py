@@ -157,9 +157,45 @@ def cpu_oracle_baseline(scene, view, budget_s=12.0):
         el = time.perf_counter() - t0
         if el >= budget_s or n >= 20:
             break
-    return {"value": n / el, "unit": "frames/s", "cores": nthreads, "kind": "port",
-            "sample": f"{n} full frames (2 shadow cascades + 1920x1080 drawAll, 1,044,288 triangles) "
-                      f"on the C oracle with OpenMP, {el:.1f} s"}
+    out = {"value": n / el, "unit": "frames/s", "cores": nthreads, "kind": "port",
+           "sample": f"{n} full frames (2 shadow cascades + 1920x1080 drawAll, 1,044,288 triangles) "
+                     f"on the C oracle with OpenMP, {el:.1f} s"}
+    out["stages"] = cpu_stage_baseline(O, scene, view)
+    return out
+
+
+def cpu_stage_baseline(O, scene, view):
+    """The reference's own kernels for the vertex stage and the post effects
+    (Pipe/vert.c, Post/ssao.c, dof.c, blur.c + blur2.c, compiled for the CPU
+    in oracle/_ref and run work-item by work-item on one core; the bloom's
+    256 work-items run as threads over all cores) on the same
+    work the vertex and post sections time on the GPU: one rotation of the
+    two sphere groups, one vertLight of both with the same light set, and
+    ssao, dof(8) and the bloom of one 1080p frame.  Milliseconds per call."""
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref is not built"}
+    from axi_visualizer_b200 import scenes as S
+    spheres = S.Scene([scene.groups[2], scene.groups[3]], [], scene.lint, scene.ldir, scene.amb, scene.shadows,
+                      scene.bias)
+    rd = O.RefDraw(spheres, view)
+    out = {"kind": "reference", "cores": 1, "bloom_cores": os.cpu_count() or 1}   # the bloom: a thread a work-item
+    t0 = time.perf_counter()
+    rd.rotate(_rot_y(0.0), _rot_y(0.01), (0.0, 0.0, 0.0), 0, spheres.groups[0].ntris * 3, 0)
+    rd.rotate(_rot_y(0.0), _rot_y(0.01), (0.0, 0.0, 0.0), 0, spheres.groups[1].ntris * 3, 1)
+    out["rotate_two_sphere_groups_ms"] = 1000 * (time.perf_counter() - t0)
+    L = VERTEX_LIGHTS
+    t0 = time.perf_counter()
+    rd.vert_light([1, 1], L["dirI"], L["dirD"], scene.amb, L["pointI"], L["pointP"], L["spotI"], L["spotD"],
+                  L["spotP"])
+    out["vert_light_two_sphere_groups_ms"] = 1000 * (time.perf_counter() - t0)
+    fr, _ = O.render(scene, view, nthreads=os.cpu_count() or 1)
+    rd.set_frame(fr.ro, fr.go, fr.bo, fr.db)
+    rnd = np.random.default_rng(44).random(48).astype(np.float32)
+    for name, fn in (("ssao_ms", lambda: rd.ssao(rnd)), ("dof_ms", lambda: rd.dof(8.0)), ("bloom_ms", rd.bloom)):
+        t0 = time.perf_counter()
+        fn()
+        out[name] = 1000 * (time.perf_counter() - t0)
+    return out
 
 
 REF_BUDGET_S = 120.0     # wall time the reference arm's warm-up + timed steps aim at
@@ -379,6 +415,18 @@ def _rot_y(a):
     return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
 
 
+def _vertex_lights():
+    rng = np.random.default_rng(11)
+    return {"dirI": np.array([(1.6, 1.4, 1.2), (0.5, 0.5, 0.5), (0.1, 0.2, 0.6)]),
+            "dirD": np.array([(0.3, -0.8, 0.5), (-0.3, 0.8, -0.5), (0.0, 1.0, 0.0)]),
+            "pointI": rng.uniform(0, 3, (4, 3)), "pointP": rng.uniform(-20, 20, (4, 3)) + (0, 8, 0),
+            "spotI": rng.uniform(0, 3, (2, 3)), "spotD": np.array([(0, -1, 0), (0.6, -0.8, 0)]),
+            "spotP": np.array([(0, 15, 0), (-10, 12, -5)])}
+
+
+VERTEX_LIGHTS = _vertex_lights()
+
+
 def vertex_section(R, view, hbm, frames=100, warmup=5):
     """An animated 1080p frame: both sphere groups (2 x 240,000 triangles)
     turn about the scene centre (CLDraw.rotate, undoing the previous turn and
@@ -393,11 +441,9 @@ def vertex_section(R, view, hbm, frames=100, warmup=5):
     scene = R.scene
     spheres = [2, 3]
     stream = torch.cuda.ExternalStream(D.stream_ptr(), device=torch.cuda.current_device())
-    rng = np.random.default_rng(11)
-    dirI = np.array([(1.6, 1.4, 1.2), (0.5, 0.5, 0.5), (0.1, 0.2, 0.6)])
-    dirD = np.array([(0.3, -0.8, 0.5), (-0.3, 0.8, -0.5), (0.0, 1.0, 0.0)])
-    pointI, pointP = rng.uniform(0, 3, (4, 3)), rng.uniform(-20, 20, (4, 3)) + (0, 8, 0)
-    spotI, spotD, spotP = rng.uniform(0, 3, (2, 3)), np.array([(0, -1, 0), (0.6, -0.8, 0)]), np.array([(0, 15, 0), (-10, 12, -5)])
+    L = VERTEX_LIGHTS
+    dirI, dirD, pointI, pointP = L["dirI"], L["dirD"], L["pointI"], L["pointP"]
+    spotI, spotD, spotP = L["spotI"], L["spotD"], L["spotP"]
     mask = [1] * len(scene.groups)
     state = {"k": 0}
 

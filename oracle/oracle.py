@@ -447,3 +447,10 @@ class RefDraw:
 
     def bloom(self):
         self.R.ref_bloom(self.h)
+
+    def set_frame(self, r, g, b, db):
+        """Replaces the colour planes and the depth buffer."""
+        arrs = [np.ascontiguousarray(a) for a in (r, g, b)]
+        d = np.ascontiguousarray(db, np.float32)
+        self.R.ref_set_frame(self.h, *[_ptr(a) for a in arrs])
+        self.R.ref_set_depth(self.h, _ptr(d))
