@@ -1,8 +1,7 @@
 """CLDraw.ssao / dof / blur on the device (k_ssao, k_dof and the k_bloom_*
 passes through the C ABI) against the oracle on the same frame: bit-exact
-colour planes.  The frame is
-set from the oracle's own render, so the comparison is of the post effects
-alone; depth is left untouched by both."""
+colour planes.  The frame is set from the oracle's own render, so the
+comparison is of the post effects alone; depth is left untouched by both."""
 import numpy as np
 import pytest
 

@@ -159,3 +159,53 @@ def test_vertex_stage_errors():
     # nothing was changed by the refused calls
     xyz, vn, _ = d.getVertices(0)
     assert same(xyz, sc.groups[0].xyz) and same(vn, sc.groups[0].vn)
+
+
+def test_copy_to_between_queued_shadow_passes():
+    """shadowMap, copyTo, shadowMap: the second pass sees the copied
+    geometry, and the first pass's map is the one of the old geometry."""
+    sc = S.scene_small(seed=4)
+    R = renderer(sc, 64, 48)
+    d = R.draw
+    cast = [g.cast for g in sc.groups]
+    ref0 = O.new_shadow_map(sc.shadows[0].dim)
+    O.shadow_map(sc, 0, ref0)
+    G = sc.groups[1]
+    moved = G.xyz.copy()
+    moved[:, 1] += 1.5
+    d.clearShadowMap(0)
+    d.shadowMap(0, cast, R.shaders, sc.bias)
+    d.copyTo(1, moved, G.vn, 0)
+    d.clearShadowMap(1)
+    d.shadowMap(1, cast, R.shaders, sc.bias)
+    G.xyz[...] = moved
+    ref1 = O.new_shadow_map(sc.shadows[1].dim)
+    O.shadow_map(sc, 1, ref1)
+    assert np.array_equal(d.getSHM(0).view(np.uint32), ref0.view(np.uint32))
+    assert np.array_equal(d.getSHM(1).view(np.uint32), ref1.view(np.uint32))
+
+
+def test_batched_render_after_rotation_equals_plain():
+    """A rotation queued before a batched render: the batch (its captured
+    graph) draws the rotated geometry, the same as the plain path."""
+    from axi_visualizer_b200.batch import Batch, scene_batch_views
+    sc = S.scene_small(seed=6)
+    view = S.default_view(128, 96, pos=(3, 6, -16))
+    R = renderer(sc, 128, 96)
+    d = R.draw
+    B = Batch(d, scene_batch_views(sc, view))
+    flags, aidx = [g.flags for g in sc.groups], [g.alpha_index for g in sc.groups]
+    B.render(flags, aidx)                           # the graph is captured before the rotation
+    d.rotate(np.eye(3), MG.rot_mat(0.1, 0.7, 0.0), (0, 0, 0), 0, None, 1)
+    B.render(flags, aidx)
+    nd = len(sc.shadows)
+    br, bg, bb, bdb = [x.copy() for x in B.frame(nd)]
+    R.frame(view)
+    r, g, b, db = d.getFrame()
+    assert np.array_equal(bdb.view(np.uint32), db.view(np.uint32))
+    assert np.array_equal(br, r) and np.array_equal(bg, g) and np.array_equal(bb, b)
+    G = sc.groups[1]
+    O.transform(G.xyz, G.vn, np.eye(3), MG.rot_mat(0.1, 0.7, 0.0), (0, 0, 0), 0, G.ntris * 3)
+    fr, smaps = O.render(sc, view)
+    got = [x.copy() for x in d.getFrame()] + list(d.getIDs()) + [[d.getSHM(k) for k in range(nd)]]
+    check_frame(fr, smaps, got)
