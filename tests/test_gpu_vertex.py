@@ -187,25 +187,40 @@ def test_copy_to_between_queued_shadow_passes():
 
 def test_batched_render_after_rotation_equals_plain():
     """A rotation queued before a batched render: the batch (its captured
-    graph) draws the rotated geometry, the same as the plain path."""
-    from axi_visualizer_b200.batch import Batch, scene_batch_views
+    graph) draws the rotated geometry, the same as the plain path and the
+    oracle.  The batched main view is cleared to the plain frame's initial
+    colour (1, 1, 1): an uncleared view keeps, where nothing covers it now,
+    what its previous render drew there."""
+    from axi_visualizer_b200.batch import Batch, depth, shaded
     sc = S.scene_small(seed=6)
     view = S.default_view(128, 96, pos=(3, 6, -16))
     R = renderer(sc, 128, 96)
     d = R.draw
-    B = Batch(d, scene_batch_views(sc, view))
+    descs = [depth(c, sc.bias) for c in sc.shadows] + [shaded(view, [0, 1], clear=(1, 1, 1))]
+    B = Batch(d, descs)
     flags, aidx = [g.flags for g in sc.groups], [g.alpha_index for g in sc.groups]
     B.render(flags, aidx)                           # the graph is captured before the rotation
     d.rotate(np.eye(3), MG.rot_mat(0.1, 0.7, 0.0), (0, 0, 0), 0, None, 1)
     B.render(flags, aidx)
     nd = len(sc.shadows)
+    bmaps = [B.frame(k).copy() for k in range(nd)]
     br, bg, bb, bdb = [x.copy() for x in B.frame(nd)]
+    bid = B.ids(nd)[0].copy()
     R.frame(view)
-    r, g, b, db = d.getFrame()
-    assert np.array_equal(bdb.view(np.uint32), db.view(np.uint32))
-    assert np.array_equal(br, r) and np.array_equal(bg, g) and np.array_equal(bb, b)
     G = sc.groups[1]
     O.transform(G.xyz, G.vn, np.eye(3), MG.rot_mat(0.1, 0.7, 0.0), (0, 0, 0), 0, G.ntris * 3)
     fr, smaps = O.render(sc, view)
     got = [x.copy() for x in d.getFrame()] + list(d.getIDs()) + [[d.getSHM(k) for k in range(nd)]]
-    check_frame(fr, smaps, got)
+    check_frame(fr, smaps, got)                     # the plain path
+    r, g, b, db = got[:4]
+    for k in range(nd):
+        assert np.array_equal(bmaps[k].view(np.uint32), smaps[k].view(np.uint32)), f"batched cascade {k}"
+    assert np.array_equal(bdb.view(np.uint32), db.view(np.uint32))
+    assert np.array_equal(bid, got[4])
+    diff = (br != r) | (bg != g) | (bb != b)
+    ys, xs = np.nonzero(diff)
+    assert not diff.any(), (f"{diff.sum()} px differ, e.g. {list(zip(ys[:5], xs[:5]))}: batched "
+                            f"{[int(br[y, x]) for y, x in zip(ys[:5], xs[:5])]} plain "
+                            f"{[int(r[y, x]) for y, x in zip(ys[:5], xs[:5])]} oracle "
+                            f"{[int(fr.ro[y, x]) for y, x in zip(ys[:5], xs[:5])]} ids "
+                            f"{[int(got[4][y, x]) for y, x in zip(ys[:5], xs[:5])]}")
