@@ -1244,7 +1244,45 @@ struct RowState {
   int mip, g;
 };
 
-__device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *sg, uint32_t ord, int cy, RowState &st) {
+// Replays `steps` rows of the two edge chains (add: downwards, else upwards)
+// and stores them in st: edge 0 the first chain (cx1, cz1, c1), edge 1 the
+// second (cx2, cz2, c2), edge 2 both.  The chains are independent sequences
+// of rounded additions, so two threads can each replay one of them and the
+// results are those of one thread replaying both.
+__device__ __forceinline__ void replay_edges(int edge, int steps, bool add, float cx1, float cx2, float cz1, float cz2,
+                                             Attr<true> c1, Attr<true> c2, float s1, float s2, float sz1, float sz2,
+                                             const Attr<true> &sa1, const Attr<true> &sa2, RowState &st) {
+  if (edge == 2) {
+    if (add) {
+      for (int r = 0; r < steps; r++) {
+        cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2; c1 = a_add(c1, sa1); c2 = a_add(c2, sa2);
+      }
+    } else {
+      for (int r = 0; r < steps; r++) {
+        cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2; c1 = a_sub(c1, sa1); c2 = a_sub(c2, sa2);
+      }
+    }
+    st.cx1 = cx1; st.cx2 = cx2; st.cz1 = cz1; st.cz2 = cz2;
+    st.c1 = c1; st.c2 = c2;
+    return;
+  }
+  const bool e2 = edge != 0;
+  float cx = e2 ? cx2 : cx1, cz = e2 ? cz2 : cz1, s = e2 ? s2 : s1, sz = e2 ? sz2 : sz1;
+  Attr<true> c = e2 ? c2 : c1;
+  const Attr<true> &sa = e2 ? sa2 : sa1;
+  if (add) {
+    for (int r = 0; r < steps; r++) { cx += s; cz += sz; c = a_add(c, sa); }
+  } else {
+    for (int r = 0; r < steps; r++) { cx -= s; cz -= sz; c = a_sub(c, sa); }
+  }
+  if (e2) { st.cx2 = cx; st.cz2 = cz; st.c2 = c; }
+  else { st.cx1 = cx; st.cz1 = cz; st.c1 = c; }
+}
+
+// The row state of winner `ord` on row cy: the edge chain(s) `edge` selects
+// (see replay_edges) and, for edge 0 or 2, the mip level and group.
+__device__ __forceinline__ void shade_row_edge(const DrawParams &P, const GroupDev *sg, uint32_t ord, int cy, int edge,
+                                               RowState &st) {
   uint32_t o = ord - 1;
   int phase = (int)(o >> 31);
   uint32_t gtri = (o >> 1) & 0x3fffffffu;
@@ -1300,15 +1338,7 @@ __device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *s
       n = y3 - cy;
     }
     if (s1 < s2) { swap_(s1, s2); swap_(sz1, sz2); swap_(sa1, sa2); }
-    if (half == 0) {
-      for (int r = 0; r < n; r++) {
-        cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2; c1 = a_add(c1, sa1); c2 = a_add(c2, sa2);
-      }
-    } else {
-      for (int r = 0; r < n; r++) {
-        cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2; c1 = a_sub(c1, sa1); c2 = a_sub(c2, sa2);
-      }
-    }
+    replay_edges(edge, n, half == 0, cx1, cx2, cz1, cz2, c1, c2, s1, s2, sz1, sz2, sa1, sa2, st);
   } else {
     // tiled path: float vertices, per-tile restart (Templates.py:93-182)
     if (y[0] > y[1]) { swap_(y[0], y[1]); swap_(x[0], x[1]); swap_(z[0], z[1]); swap_(a[0], a[1]); }
@@ -1335,9 +1365,7 @@ __device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *s
       float dy = (float)cy0 - y1;
       cx1 = x1 + dy * s1; cx2 = x1 + dy * s2; cz1 = z1 + dy * sz1; cz2 = z1 + dy * sz2;
       c1 = a_add(a[0], a_smul(dy, sa1)); c2 = a_add(a[0], a_smul(dy, sa2));
-      for (int r = cy0; r < cy; r++) {
-        cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2; c1 = a_add(c1, sa1); c2 = a_add(c2, sa2);
-      }
+      replay_edges(edge, cy - cy0, true, cx1, cx2, cz1, cz2, c1, c2, s1, s2, sz1, sz2, sa1, sa2, st);
     } else {
       float d = 1.0f / (y3 - y2);
       s1 = (x3 - x2) * d; s2 = (x3 - x4) * d;
@@ -1348,14 +1376,14 @@ __device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *s
       float dy = (float)cy0 - y3;
       cx1 = x3 + dy * s1; cx2 = x3 + dy * s2; cz1 = z3 + dy * sz1; cz2 = z3 + dy * sz2;
       c1 = a_add(a[2], a_smul(dy, sa1)); c2 = a_add(a[2], a_smul(dy, sa2));
-      for (int r = cy0; r > cy; r--) {
-        cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2; c1 = a_sub(c1, sa1); c2 = a_sub(c2, sa2);
-      }
+      replay_edges(edge, cy0 - cy, false, cx1, cx2, cz1, cz2, c1, c2, s1, s2, sz1, sz2, sa1, sa2, st);
     }
   }
-  st.cx1 = cx1; st.cx2 = cx2; st.cz1 = cz1; st.cz2 = cz2;
-  st.c1 = c1; st.c2 = c2;
-  st.fmip = ms.fmip; st.mip = ms.mip; st.g = g;
+  if (edge != 1) { st.fmip = ms.fmip; st.mip = ms.mip; st.g = g; }
+}
+
+__device__ __forceinline__ void shade_row(const DrawParams &P, const GroupDev *sg, uint32_t ord, int cy, RowState &st) {
+  shade_row_edge(P, sg, ord, cy, 2, st);
 }
 
 // av_draw_multi.c:30-105: the 4-way terrain blend of a F_MULTI group.  Its
@@ -1478,9 +1506,10 @@ struct ShadeSmem {
 
 // Shades the 16 x (NT/16) pixels at (x0, y0): the block finds the distinct
 // (winner, row) pairs among its pixels (a bounded open-addressing table in
-// shared memory), one thread per pair sets up the triangle and replays its
-// row, then every pixel shades from its pair's row state.  The arithmetic is
-// shade_pixel's, done once per pair instead of once per pixel.
+// shared memory), two threads per pair set up the triangle and replay its
+// row (one edge chain each), then every pixel shades from its pair's row
+// state.  The arithmetic is shade_pixel's, done once per pair instead of once
+// per pixel.
 template <int NT>
 __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *sg, int x0, int y0, ShadeSmem<NT> &sm) {
   const unsigned long long EMPTY = ~0ull;
@@ -1514,9 +1543,9 @@ __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *
   }
   __syncthreads();
   int ne = sm.nent;
-  for (int e = tid; e < ne; e += NT) {
-    unsigned long long k = sm.ekey[e];
-    shade_row(P, sg, (uint32_t)(k >> 32), (int)(uint32_t)k, sm.rs[e]);
+  for (int j = tid; j < 2 * ne; j += NT) {   // two threads a pair, one edge chain each
+    unsigned long long k = sm.ekey[j >> 1];
+    shade_row_edge(P, sg, (uint32_t)(k >> 32), (int)(uint32_t)k, j & 1, sm.rs[j >> 1]);
   }
   __syncthreads();
   if (valid) shade_from_row(P, sg, ax, cy, sm.rs[sm.hent[slot]]);
