@@ -94,6 +94,7 @@ struct axr_ctx {
   float *db = nullptr;
   uint64_t *keys = nullptr;
   uint32_t *small_list = nullptr, *large_list = nullptr, *items = nullptr;
+  float2 *mipc = nullptr;                    // per-triangle mip level of the last drawAll's setup
   uint32_t cap_list = 0;
   uint2 *units = nullptr;
   uint32_t cap_units = 0;
@@ -159,11 +160,14 @@ int ensure_lists(axr_ctx *c) {
   if (need > MAX_LIST) return fail(AXR_EINVAL, "more than %u triangles", MAX_LIST);
   uint32_t cap = (uint32_t)std::max<uint64_t>(need, std::min<uint64_t>(2ull * c->cap_list, MAX_LIST));
   cudaStreamSynchronize(c->stream);
-  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items);
+  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items); cudaFree(c->mipc);
   c->small_list = c->large_list = c->items = nullptr;
+  c->mipc = nullptr;
+  c->cap_list = 0;
   if (cudaMalloc(&c->small_list, sizeof(uint32_t) * cap) != cudaSuccess ||
       cudaMalloc(&c->large_list, sizeof(uint32_t) * cap) != cudaSuccess ||
-      cudaMalloc(&c->items, sizeof(uint32_t) * cap * MAX_CHUNKS) != cudaSuccess)
+      cudaMalloc(&c->items, sizeof(uint32_t) * cap * MAX_CHUNKS) != cudaSuccess ||
+      cudaMalloc(&c->mipc, sizeof(float2) * cap) != cudaSuccess)
     return fail(AXR_ENOMEM, "triangle lists of %u entries", cap);
   c->cap_list = cap;
   return 0;
@@ -488,7 +492,7 @@ int axr_destroy(axr_ctx *c) {
   if (c->ev_coarse) cudaEventDestroy(c->ev_coarse);
   if (c->ev_alpha) cudaEventDestroy(c->ev_alpha);
   cudaFree(c->ro); cudaFree(c->go); cudaFree(c->bo); cudaFree(c->db); cudaFree(c->keys);
-  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items); cudaFree(c->units);
+  cudaFree(c->small_list); cudaFree(c->large_list); cudaFree(c->items); cudaFree(c->units); cudaFree(c->mipc);
   cudaFree(c->ctr); cudaFree(c->d_groups);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
   if (c->h_ring) cudaFreeHost(c->h_ring);
@@ -836,6 +840,7 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   P.units = c->units; P.ctr = c->ctr;
   P.cap_list = c->cap_list; P.cap_units = c->cap_units;
   P.min_chunk = c->min_chunk;
+  P.mipc = c->mipc;
   long npix = (long)c->w * c->h;
   cudaStream_t s = c->stream;
   int64_t nk = 0;

@@ -42,6 +42,8 @@ struct DrawParams {
   uint32_t *ctr;         // see CTR_*
   uint32_t cap_list, cap_units;
   int min_chunk;         // rows per small-triangle work item (at least; tuning knob)
+  float2 *mipc;          // per triangle of a mip group: (mip fraction, mip level), written by
+                         // the setup, read by the shade; null: the shade computes them
 };
 
 enum {
@@ -521,6 +523,19 @@ __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev 
         cls = project_persp(G, t - G.tri_base, P.view, sx, sy, sz);
         alpha = (G.flags & F_ALPHA) != 0;
         iy0 = f2i(sy[0]); iy1 = f2i(sy[1]); iy2 = f2i(sy[2]);
+        if (P.mipc && cls == 2 && (G.flags & F_MIP)) {
+          // a large triangle's mip level, once here instead of once per
+          // shaded (winner, row) pair; it does not depend on the vertex order
+          Attr<false> a[3];
+          int ix[3], iy[3];
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            a[k] = a_load<false>(G, t - G.tri_base, k, sz[k]);
+            ix[k] = f2i(sx[k]); iy[k] = f2i(sy[k]);
+          }
+          MipSel m = mip_setup<false>(a, sz, cls == 1, ix, iy, sx, sy, G.tex_size, G.mip_bias);
+          P.mipc[t] = make_float2(m.fmip, (float)m.mip);
+        }
       }
     }
     unsigned ms = __ballot_sync(FULL, cls == 1 && !alpha), ma = __ballot_sync(FULL, cls == 1 && alpha);
@@ -1350,7 +1365,15 @@ __device__ __forceinline__ void shade_row_edge(const DrawParams &P, const GroupD
     float x4 = x1 + yd * (x3 - x1);
     float z4 = z1 + yd * (z3 - z1);
     Attr<true> a4 = a_add(a[0], a_smul(yd, a_sub(a[2], a[0])));
-    if (mip) ms = mip_setup<true>(a, z, false, nullptr, nullptr, x, y, G.tex_size, G.mip_bias);
+    if (mip) {
+      if (P.mipc) {
+        mip_attr_roundtrip<true>(a, z);
+        float2 mc = P.mipc[gtri];
+        ms.fmip = mc.x; ms.mip = (int)mc.y;
+      } else {
+        ms = mip_setup<true>(a, z, false, nullptr, nullptr, x, y, G.tex_size, G.mip_bias);
+      }
+    }
     int tileY = cy / TILE;
     float yMin = (float)tileY * 16.f, yMax = ((float)tileY + 1.f) * 16.f - 1.f;
     float s1, s2, sz1, sz2;

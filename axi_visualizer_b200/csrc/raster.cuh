@@ -343,6 +343,22 @@ __device__ __forceinline__ MipSel mip_setup(Attr<FULL> a[3], const float z[3], b
   return m;
 }
 
+// The attribute round trip mip_setup makes (uv and position divided by the
+// vertex z, then multiplied back), for callers that have the mip level
+// already: the interpolants must be these values, bit for bit.
+template <bool FULL>
+__device__ __forceinline__ void mip_attr_roundtrip(Attr<FULL> a[3], const float z[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    V2 uv = div2(a[k].uv, z[k]);
+    a[k].uv = mul2(uv, z[k]);
+    if (FULL) {
+      V3 p = div3(a[k].p, z[k]);
+      a[k].p = mul3(p, z[k]);
+    }
+  }
+}
+
 // bilinear taps of av_draw_base.c:29-42 at side `len`, texel offset `start`
 struct Taps {
   int tex, tex10, tex01, tex11;
