@@ -76,3 +76,25 @@ def test_errors_without_gpu_are_reported():
     rc = L.axr_create(64, 64, 0, ctypes.byref(h))
     assert rc != 0 and L.axr_last_error()
     assert L.axr_create(60, 64, 0, ctypes.byref(h)) == -1     # width not a multiple of 16
+
+
+def test_entry_points_refuse_a_null_handle():
+    """Without a handle every entry point returns an error code and leaves a
+    message, before any CUDA call (so this runs without a GPU)."""
+    from axi_visualizer_b200 import _lib
+    L = _lib.lib()
+    f3 = (ctypes.c_float * 9)()
+    calls = [
+        ("axr_transform", (None, 0, f3, f3, f3, 0, -1)),
+        ("axr_translate", (None, 0, f3, 0, -1)),
+        ("axr_vert_light", (None, None, 0, None, None, 0, None, None, 0, None, None, None, 0, 0.2)),
+        ("axr_get_vertices", (None, 0, None, None, None)),
+        ("axr_ssao", (None, f3, 9)),
+        ("axr_dof", (None, 8.0)),
+        ("axr_bloom", (None,)),
+        ("axr_gamma", (None, 1.0)),
+    ]
+    for name, args in calls:
+        rc = getattr(L, name)(*args)
+        assert rc < 0, name
+        assert b"null handle" in L.axr_last_error(), name
