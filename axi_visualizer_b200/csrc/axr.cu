@@ -1511,7 +1511,7 @@ int batch_enqueue(axr_batch *b) {
     kb_tiled<false><<<sms * 8, 128, 0, s>>>(B);
     CK(cudaStreamWaitEvent(s, b->ev_join, 0));
     kb_fallback<<<sms * 4, 128, 0, s>>>(B);
-    kb_shade<<<sms * 3, 256, 0, s>>>(B);
+    kb_shade<<<sms * 4, 256, 0, s>>>(B);
     CK(cudaGetLastError());
   }
   for (size_t k = 0; k < nv; k++)

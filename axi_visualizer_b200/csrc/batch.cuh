@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(128) kb_fallback(BatchParams B) {
   }
 }
 
-__global__ void __launch_bounds__(256, 3) kb_shade(BatchParams B) {
+__global__ void __launch_bounds__(256, 4) kb_shade(BatchParams B) {
   __shared__ GroupDev sgd[BATCH_TABLE];
   __shared__ ShadeSmem<256> sm;
   for (int i = threadIdx.x; i < B.ngroups; i += blockDim.x) sgd[i] = B.groups_draw[i];

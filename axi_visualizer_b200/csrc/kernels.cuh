@@ -1577,7 +1577,7 @@ __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *
 
 
 // one 256-thread block per 16x16 tile
-__global__ void __launch_bounds__(256, 3) k_shade(DrawParams P) {   // 80 registers: 3 blocks per SM
+__global__ void __launch_bounds__(256, 4) k_shade(DrawParams P) {   // 64 registers: 4 blocks per SM
   __shared__ GroupDev sg[64];
   __shared__ ShadeSmem<256> sm;
   for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
