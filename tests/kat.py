@@ -116,3 +116,113 @@ def case_scenes(w=96, h=72):
 
 def masks(name, ngroups):
     return [0, 1] + [0] * (ngroups - 2) if name == "masked_empty" else None
+
+
+# shadow-map border taps (av_alpha_max.c:53-84: a cascade counts its five
+# taps only when the centre tap lies in [2, 2 wS - 2) on both axes)
+BORDER_T0 = 20000            # the receivers' constant texel
+BORDER_CASCADES = [((0.0, 0.0, 0.0), 22.1), ((1.5, 1.0, 0.0), 22.1)]   # (centre, texels per unit), 64^2 each
+BORDER_DEPTH = 10.0          # receiver plane z; the cascades sit at z = -20 looking down +z
+BORDER_SMALL_DEPTH = 9.9     # the small receivers, just in front of the plane
+BORDER_SMALL_OFFSET = (0.3, 0.2)   # the small receivers' vertices sit this far past whole pixels
+
+
+def shadow_border_scene(w=96, h=72):
+    """A receiver plane at z = 10 facing the camera and lit head-on, a caster
+    behind the camera (rejected by the view, drawn into the maps) over the
+    half-plane x + y < 0, and two 64^2 cascades looking down +z that each
+    end inside the view: cascade 0 holds |x|, |y| <= 1.45 around the axis,
+    cascade 1 the same around (1.5, 1.0).  Where cascade 0's centre tap
+    falls on its two outer rows or columns, the caster lies under it and
+    cascade 1 does not reach, so the count there must be 0.  The texture is
+    constant and the vertex light 0: a pixel's red value is
+    T0 * light * 1.6 with light = (s * amb + 5 - s) / 5, from which the
+    shadow count s reads back.
+
+    Receivers: two large triangles at z = 10 (the tiled path, rows
+    < 16 * (h // 16)) and, at z = 9.9 in front of them, 8 x 8-pixel small
+    ones over the bottom 16 rows (the only receivers of rows 64-71) and over
+    the left half of rows 40-55, where the shadow and cascade 0's border
+    reach them too."""
+    rng = np.random.default_rng(12)
+    z = BORDER_DEPTH
+    T = lambda pts: tri(w, h, pts)
+    big = [T([(-30.0, -20.0, z), (130.0, 10.0, z), (10.0, 110.0, z)]),
+           T([(130.0, -20.0, z), (130.0, 110.0, z), (-30.0, 110.0, z)])]
+    small = []
+    zs = BORDER_SMALL_DEPTH
+    cells = [(cx, cy) for cy in range(h - 16, h, 8) for cx in range(0, w, 8)]
+    cells += [(cx, cy) for cy in range(h - 32, h - 16, 8) for cx in range(0, w // 2, 8)]
+    for cx, cy in cells:
+        x0, y0 = cx + BORDER_SMALL_OFFSET[0], cy + BORDER_SMALL_OFFSET[1]
+        small.append(T([(x0, y0, zs), (x0 + 8, y0, zs), (x0, y0 + 8, zs)]))
+        small.append(T([(x0 + 8, y0, zs), (x0 + 8, y0 + 8, zs), (x0, y0 + 8, zs)]))
+    caster = [[(-5.0, 5.0, -5.0), (5.0, -5.0, -5.0), (-5.0, -5.0, -5.0)]]
+    plane = np.full(16 * 16, BORDER_T0, np.uint16)
+
+    def group(tris, flags, normal):
+        xyz = np.asarray(tris, np.float32).reshape(-1, 3)
+        n = xyz.shape[0]
+        vn = np.tile(np.asarray(normal, np.float32), (n, 1))
+        uv = rng.random((n, 2)).astype(np.float32)
+        return S.Group(xyz, uv, vn, np.zeros((n, 3), np.float32), (plane, plane.copy(), plane.copy()), 16, flags)
+
+    groups = [group(big, S.SHADOW, (0, 0, -1)), group(small, S.SHADOW, (0, 0, -1)), group(caster, 0, (0, 0, 1))]
+    cams = [S.ShadowCam.facing(64, s, c, (0.0, 0.0), dist=20.0) for c, s in BORDER_CASCADES]
+    return S.Scene(groups, [], np.asarray(S.LIGHT_INTS[0], np.float32), np.array([0, 0, -1], np.float32), 0.2, cams)
+
+
+def border_counts(sc, maps, tri_id, w, h):
+    """The shadow count av_alpha_max.c gives each pixel of the receiver plane
+    of shadow_border_scene, from the maps, with `clear` False where a tap
+    coordinate lies within 0.02 texels of an integer (where the float
+    rounding of the interpolated position decides); and the mask of pixels
+    whose cascade-0 centre tap is outside [2, 62) on a map texel that the
+    caster covers while cascade 1 is out of reach (count 0 by the border
+    rule alone).
+
+    A pixel's world position is the point of its receiver under the
+    pixel's corner, except that on the small receivers it is the point under
+    the corner plus BORDER_SMALL_OFFSET: the small path truncates vertex
+    screen positions (Templates.py:230-231) while the interpolated position
+    runs between the true vertices."""
+    ys, xs = np.mgrid[0:h, 0:w].astype(np.float64)
+    n0 = sc.groups[0].ntris
+    small = (tri_id >= n0) & (tri_id < n0 + sc.groups[1].ntris)
+    xs = xs + np.where(small, BORDER_SMALL_OFFSET[0], 0.0)
+    ys = ys + np.where(small, BORDER_SMALL_OFFSET[1], 0.0)
+    Z = np.where(small, BORDER_SMALL_DEPTH, BORDER_DEPTH)
+    X = (xs - w // 2) * Z / SCALE
+    Y = (ys - h // 2) * Z / SCALE
+    total = np.zeros((h, w), np.int64)
+    clear = np.ones((h, w), bool)
+    exposed = np.ones((h, w), bool)
+    for k, cam in enumerate(sc.shadows):
+        m = maps[k]
+        ws = cam.dim // 2
+        depth = Z - float(cam.pos[2])
+        fx = -(X - float(cam.pos[0])) * cam.scale
+        fy = (Y - float(cam.pos[1])) * cam.scale
+        for f in (fx, fy):
+            frac = np.abs(f - np.round(f))
+            clear &= frac > 0.02
+        sx = np.trunc(fx).astype(np.int64) + ws
+        sy = np.trunc(fy).astype(np.int64) + ws
+        inside = (sx >= 2) & (sx < 2 * ws - 2) & (sy >= 2) & (sy < 2 * ws - 2)
+        cnt = np.zeros((h, w), np.int64)
+        for dy, dx in ((0, 0), (2, 0), (-2, 0), (0, 2), (0, -2)):
+            ty = np.clip(sy + dy, 0, 2 * ws - 1)
+            tx = np.clip(sx + dx, 0, 2 * ws - 1)
+            cnt += inside & (m[ty, tx] < depth)
+        total += cnt
+        onmap = (sx >= 0) & (sx < 2 * ws) & (sy >= 0) & (sy < 2 * ws)
+        under = onmap & (m[np.clip(sy, 0, 2 * ws - 1), np.clip(sx, 0, 2 * ws - 1)] < depth)
+        exposed &= (~inside & under) if k == 0 else ~inside
+    return np.minimum(total, 5), clear, exposed
+
+
+def decode_shadow_count(red, amb=0.2):
+    """The shadow count s of shadow_border_scene's receivers from the red
+    plane (T0 * light * LInt.x, light = (s * amb + 5 - s) * 0.2)."""
+    light = red.astype(np.float64) / (BORDER_T0 * float(S.LIGHT_INTS[0][0]))
+    return np.rint((1.0 - light) / ((1.0 - amb) * 0.2)).astype(np.int64)

@@ -64,5 +64,68 @@ def test_kat_expectations():
     fr, _ = oracle_frame(SCENES["masked_empty"], VIEW, kat.masks("masked_empty", 3))
     ids = np.unique(fr.tri_id[fr.tri_id >= 0])
     assert ids.size and ids.min() >= SCENES["masked_empty"].groups[0].ntris + SCENES["masked_empty"].groups[1].ntris
-    # rows at and below 16 * floor(h/16) are reached by small triangles only
-    assert VIEW.h % 16 != 0 or True
+    # rows at and below 16 * floor(h/16) are reached by small triangles only:
+    # the large triangle of tile_borders covers the whole view but gives way
+    # there to the small ones or to nothing
+    sc = SCENES["tile_borders"]
+    fr, _ = oracle_frame(sc, VIEW)
+    top = 16 * (VIEW.h // 16)
+    assert top < VIEW.h
+    assert (fr.tri_id[:top] == 3).sum() > 0
+    assert not (fr.tri_id[top:] == 3).any()
+    assert (fr.tri_id[top:] >= 0).any()
+
+
+def border_frame():
+    sc = kat.shadow_border_scene(VIEW.w, VIEW.h)
+    maps = []
+    for k, s in enumerate(sc.shadows):
+        m = O.new_shadow_map(s.dim)
+        O.shadow_map(sc, k, m)
+        maps.append(m)
+    fr = O.Frame(VIEW.w, VIEW.h)
+    O.clear_depth(fr.db)
+    O.draw_all(sc, VIEW, fr, maps)
+    return sc, fr, maps
+
+
+def test_shadow_border_taps():
+    """Shadow lookups at a cascade's border (av_alpha_max.c:53-84) on the
+    oracle.  The count read back from each pixel clear of tap rounding is the
+    one the rule gives from the maps.  Where cascade 0's centre tap falls on
+    its two outer rows or columns, over texels the caster covers, with
+    cascade 1 out of reach, the count is 0, on the tiled and the small path."""
+    sc, fr, maps = border_frame()
+    cov = fr.cov.astype(bool)
+    s = kat.decode_shadow_count(fr.ro)
+    want, clear, exposed = kat.border_counts(sc, maps, fr.tri_id, VIEW.w, VIEW.h)
+    sel = cov & clear
+    assert sel.sum() > 0.75 * cov.sum()
+    assert np.array_equal(s[sel], want[sel])
+    assert set(np.unique(s[cov]).tolist()) >= {0, 2, 3, 5}
+    n0 = sc.groups[0].ntris
+    small = (fr.tri_id >= n0) & (fr.tri_id < n0 + sc.groups[1].ntris)
+    for path in (small, ~small):
+        ex = sel & exposed & path
+        assert ex.sum() >= 20
+        assert not s[ex].any()
+        assert (s[sel & path] == 5).any()
+    # the caster is behind the camera: the view drops it, the maps hold it
+    assert not (fr.tri_id >= n0 + sc.groups[1].ntris).any()
+    assert all((m < 16.0).sum() > 0 for m in maps)
+
+
+@needs_ref
+def test_shadow_border_maps_and_depth_equal_reference():
+    """The border scene's cascades through drawmin.c, and its depth through
+    the reference's draw kernels (which do not read the maps): bit-exact."""
+    sc, fr, maps = border_frame()
+    rd = O.RefDraw(sc, VIEW)
+    for k in range(len(sc.shadows)):
+        rc, m = rd.shadow_map(k)
+        assert rc == 0
+        assert np.array_equal(m.view(np.uint32), maps[k].view(np.uint32)), k
+    rd.clear_zbuffer()
+    assert rd.draw_all() == 0
+    db = rd.get_frame()[3]
+    assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32))

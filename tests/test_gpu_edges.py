@@ -58,6 +58,29 @@ def test_kat_cuda_equals_oracle(name):
     assert_same(fr, smaps, got)
 
 
+def test_shadow_border_taps_cuda_equals_oracle():
+    """Shadow lookups on and past a cascade's outer texels (kat's border
+    scene): maps, coverage, ids and depth bit-exact, colour at the parity
+    bar, and the shadow count read back from every covered pixel equal to
+    the oracle's, on the tiled and the small path."""
+    from test_gpu_parity import check_frame
+    sc = kat.shadow_border_scene(VIEW.w, VIEW.h)
+    smaps = []
+    for k, s in enumerate(sc.shadows):
+        m = O.new_shadow_map(s.dim)
+        O.shadow_map(sc, k, m)
+        smaps.append(m)
+    fr = O.Frame(VIEW.w, VIEW.h)
+    O.clear_depth(fr.db)
+    O.draw_all(sc, VIEW, fr, smaps)
+    got, _ = cuda_frame(sc, VIEW)
+    check_frame(fr, smaps, got)
+    cov = fr.cov.astype(bool)
+    s_cuda, s_orc = kat.decode_shadow_count(got[0]), kat.decode_shadow_count(fr.ro)
+    assert np.array_equal(s_cuda[cov], s_orc[cov])
+    assert (s_orc[cov] == 5).any() and (s_orc[cov] == 0).any()
+
+
 def test_unit_queue_overflow_falls_back_then_grows(monkeypatch):
     monkeypatch.setenv("AXR_UNIT_QUEUE", "16")
     sc = S.scene_small(seed=1, flags=S.MIP | S.SHADOW)
