@@ -7,6 +7,7 @@
 // texture planes (mip chain smallest level first); work queues sized by the
 // triangle count (small/large lists) and a grow-only tile-unit queue.
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -74,6 +75,8 @@ struct Shadow {
 
 constexpr int MAX_GROUPS = 64;
 constexpr int MAX_SHADOWS = 16;
+// 3 * ntris + 3 stays an int: the vertex kernels round v_end up to a quad
+constexpr int MAX_GROUP_TRIS = (INT_MAX - 3) / 3;
 
 }  // namespace
 
@@ -534,6 +537,8 @@ int axr_add_texture_group(axr_ctx *c, const float *xyz, const float *uv, const f
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!xyz || !uv || !vn || !r || !g || !b || ntris < 0) return fail(AXR_EINVAL, "null input or negative count");
+  // vertex ranges (transform, translate, vertLight) are int vertex indices
+  if (ntris > MAX_GROUP_TRIS) return fail(AXR_EINVAL, "a group holds at most %d triangles", MAX_GROUP_TRIS);
   if ((int)c->groups.size() >= MAX_GROUPS) return fail(AXR_EINVAL, "at most %d groups", MAX_GROUPS);
   if ((long)c->total_tris + ntris >= (1L << 30) - 1) return fail(AXR_EINVAL, "more than 2^30 triangles");
   Group G;
@@ -729,7 +734,7 @@ int axr_copy_to(axr_ctx *c, int group, const float *xyz, const float *vn, int tr
   if (rc) return rc;
   if (group < 0 || group >= (int)c->groups.size()) return fail(AXR_EINVAL, "group %d", group);
   Group &G = c->groups[group];
-  if (tri_start < 0 || ntris < 0 || tri_start + ntris > G.ntris) return fail(AXR_EINVAL, "range out of group");
+  if (tri_start < 0 || ntris < 0 || (long)tri_start + ntris > G.ntris) return fail(AXR_EINVAL, "range out of group");
   size_t off = (size_t)tri_start * 9, n = (size_t)ntris * 9;
   rc = geometry_write(c, [&] {
     if (xyz) CK(cudaMemcpyAsync(G.xyz + off, xyz, n * 4, cudaMemcpyHostToDevice, c->stream));
@@ -1367,7 +1372,7 @@ int batch_check_views(axr_ctx *c, const axr_view_desc *v, int n) {
         return fail(AXR_EINVAL, "view %d: background colour outside [0, 65535]", k);
     int ng = (int)c->groups.size();
     if (v[k].group_count < 0 || v[k].group_first < 0 ||
-        (v[k].group_count > 0 && v[k].group_first + v[k].group_count > ng) ||
+        (v[k].group_count > 0 && (long)v[k].group_first + v[k].group_count > ng) ||
         (v[k].group_count == 0 && v[k].group_first != 0))
       return fail(AXR_EINVAL, "view %d: group range [%d, +%d) outside the handle's %d groups", k, v[k].group_first,
                   v[k].group_count, ng);

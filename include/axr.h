@@ -64,7 +64,10 @@ int axr_set_scale_cull(axr_ctx *ctx, float sscale, float cax, float cay);
  * vn [3*ntris][3]; texture planes r, g, b of `ntexels` uint16 each (one
  * side*side level, or the full mip chain smallest level first when
  * mip_side > 0, Utils.createMips).  tex_size is the reference's texSize:
- * side, or log2(side) for mip.  Returns the group id in *out_id. */
+ * side, or log2(side) for mip.  Returns the group id in *out_id.  A group
+ * holds at most 715,827,881 triangles, so that its vertex indices fit the
+ * int vertex ranges of axr_transform / axr_translate / axr_vert_light; a
+ * handle holds fewer than 2^30 - 1 in all. */
 int axr_add_texture_group(axr_ctx *ctx, const float *xyz, const float *uv, const float *vn, int ntris,
                           const uint16_t *r, const uint16_t *g, const uint16_t *b, long ntexels,
                           int mip_side, int *out_id);

@@ -124,6 +124,11 @@ def test_api_errors_raise():
     with pytest.raises(AxrError):
         R.draw.addTextureGroup(np.zeros((4, 3)), np.zeros((4, 2)), np.zeros((4, 3)),
                                np.zeros(16), np.zeros(16), np.zeros(16))   # not 3 vertices per triangle
+    # ranges whose int sum overflows are refused, not wrapped
+    assert R.draw._L.axr_copy_to(R.draw._h, 0, None, None, 2**30, 2**31 - 1) != 0
+    from axi_visualizer_b200.batch import Batch, shaded
+    with pytest.raises(AxrError):
+        Batch(R.draw, [shaded(S.default_view(64, 48), [], groups=(2**31 - 2, 5))])
     R.draw.drawAll(R.shaders)                        # the handle still works
     R.draw.sync()
 
