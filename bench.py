@@ -160,6 +160,11 @@ def cpu_oracle_baseline(scene, view, budget_s=12.0):
     out = {"value": n / el, "unit": "frames/s", "cores": nthreads, "kind": "port",
            "sample": f"{n} full frames (2 shadow cascades + 1920x1080 drawAll, 1,044,288 triangles) "
                      f"on the C oracle with OpenMP, {el:.1f} s"}
+    t0 = time.perf_counter()
+    O.render(scene, view, nthreads=1)
+    el1 = time.perf_counter() - t0
+    out["one_core"] = {"value": 1.0 / el1, "unit": "frames/s", "cores": 1,
+                       "sample": f"1 full frame of the same workload on one thread, {el1:.1f} s"}
     out["stages"] = cpu_stage_baseline(O, scene, view)
     return out
 
