@@ -78,7 +78,7 @@ def tune(batch, flags, aidx=None, cast=None, ntris=0, reps=5, gpu="", use_cache=
             batch.set_mode(mode)
             batch.set_tuning(bps, ch)
         except Exception:
-            continue              # beyond the occupancy limit of this build
+            continue              # more blocks per SM than the compiled kernel can keep resident
         ms = _time_renders(batch, flags, aidx, cast, reps)
         results.append({"mode": mode, "blocks_per_sm": bps, "min_chunk": ch, "ms": ms})
         if log:
