@@ -8,9 +8,12 @@ a caller can see:
   - errors raise `AxrError` (the reference raises pyopencl errors)
   - `getIDs()` is new: triangle id and coverage of the last drawAll
   - effects outside the rasterizer hot path (sky, particles, reflections,
-    SSR, cubemap re-layout, GI buffers, bones, waves) are not provided:
-    their methods raise NotImplementedError, except setSkyTex, which the
-    engine calls unconditionally and which is accepted and ignored.
+    SSR, cubemap re-layout, GI buffers, bones, waves, voxel light, normal
+    and roughness maps), the post kernels the snapshot does not ship
+    (tonemap, exposure, blurTest) and the OpenCL buffer plumbing
+    (getBuffers, getShadow, getArgs) are not provided: their methods raise
+    NotImplementedError, except setSkyTex, which the engine calls
+    unconditionally and which is accepted and ignored.
 """
 from __future__ import annotations
 
@@ -29,6 +32,14 @@ SKY_COLOR = tuple(int(x) for x in (np.array([60, 110, 255.0]) ** 2 / 3).astype(n
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def _pad4(v):
+    """(V, 3) -> (V // 3, 3, 4) float32 with a zero fourth component
+    (the reference's align34 layout, Ops.py:124-125)."""
+    out = np.zeros((v.shape[0], 4), np.float32)
+    out[:, :3] = v
+    return out.reshape(-1, 3, 4)
 
 
 def _f32(a):
@@ -168,6 +179,16 @@ class CLDraw:
         out = [np.empty((nv, 3), np.float32) for _ in range(3)]
         check(self._L.axr_get_vertices(self._h, int(tn), *[_p(a) for a in out]), "getVertices")
         return tuple(out)
+
+    def getVertPoints(self, tn):
+        """Group tn's positions in the reference's device layout
+        (Ops.py:290-293): (T, 3, 4) float32, one float4 per vertex whose
+        fourth component is align34's padding, 0."""
+        return _pad4(self.getVertices(tn)[0])
+
+    def getVertNorms(self, tn):
+        """Group tn's normals in the same layout (Ops.py:294-297)."""
+        return _pad4(self.getVertices(tn)[1])
 
     def addTexAlpha(self, a):
         a = np.asarray(a)
@@ -398,8 +419,15 @@ class CLDraw:
         if name in ("addTexture", "setReflTex", "setHostSkyTex", "addBoneWeights", "initBoneTransforms",
                     "setBoneTransform", "boneTransform", "setupWave", "updateWave",
                     "highlight", "drawDirectional", "getGIM", "addOpacityMap", "clearShadowOpMap",
-                    "shadowClouds", "shadowCloudsOpacity", "tonemap", "mipShadowMap", "setPSTex", "drawPS"):
+                    "shadowClouds", "shadowCloudsOpacity", "tonemap", "mipShadowMap", "setPSTex", "drawPS",
+                    "addNrmMap", "addRghMap", "getBoneWeights", "initBoneOrigin", "invbt", "genVoxels",
+                    "getVoxels", "voxCopy", "voxLight", "voxTerrain"):
             raise NotImplementedError(f"CLDraw.{name} belongs to an effect outside the rasterizer hot path")
+        if name in ("exposure", "blurTest"):
+            raise NotImplementedError(f"CLDraw.{name} runs a kernel file the reference snapshot does not ship")
+        if name in ("getBuffers", "getShadow", "getArgs"):
+            raise NotImplementedError(f"CLDraw.{name} hands out OpenCL buffers; this library keeps its buffers "
+                                      "on the device behind the C ABI")
         raise AttributeError(name)
 
 

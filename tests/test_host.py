@@ -45,6 +45,54 @@ def test_cldraw_material_args_without_gpu():
         CLDraw._material_args(Fake(), ["mip"])
 
 
+# every method of the reference's CLDraw (PyOpenCL27C/Ops.py:127-1230)
+REFERENCE_CLDRAW_METHODS = """
+__init__ addBoneWeights addNrmMap addOpacityMap addRghMap addShadowMap addTexAlpha addTexture addTextureGroup
+blur blurTest boneTransform clearShadowMap clearShadowOpMap clearZBuffer copyTo dof drawAll drawDirectional
+exposure gamma genVoxels getArgs getBoneWeights getBuffers getFrame getGIM getSHM getShadow getVertNorms
+getVertPoints getVoxels highlight initBoneOrigin initBoneTransforms invbt mipShadowMap placeShadowMap rotate
+setBoneTransform setHostSkyTex setPos setPrimaryLight setReflTex setScaleCull setSkyTex setVM setupWave
+shadowMap ssao tonemap translate updateWave vertLight voxCopy voxLight voxTerrain
+""".split()
+
+
+def test_every_reference_cldraw_method_is_provided_or_refused():
+    """A caller of the reference class finds each method: implemented, or
+    raising NotImplementedError with the reason (no AttributeError)."""
+    from axi_visualizer_b200.ops import CLDraw
+    d = CLDraw.__new__(CLDraw)          # no handle: only attribute lookup is exercised
+    provided, refused = [], []
+    for name in REFERENCE_CLDRAW_METHODS:
+        if name in CLDraw.__dict__:
+            assert callable(CLDraw.__dict__[name]), name
+            provided.append(name)
+            continue
+        with pytest.raises(NotImplementedError):
+            getattr(d, name)
+        refused.append(name)
+    assert {"drawAll", "shadowMap", "getFrame", "vertLight", "rotate", "getVertPoints"} <= set(provided)
+    assert "voxLight" in refused and "getBuffers" in refused
+    with pytest.raises(AttributeError):
+        getattr(d, "noSuchMethod")
+
+
+def test_vertex_getters_use_the_padded_layout():
+    """getVertPoints / getVertNorms return the reference's align34 layout
+    (Ops.py:124-125, 290-297): (T, 3, 4) float32 with a zero fourth
+    component."""
+    from axi_visualizer_b200.ops import CLDraw, _pad4
+    v = np.arange(18, dtype=np.float32).reshape(6, 3)
+    out = _pad4(v)
+    assert out.shape == (2, 3, 4) and out.dtype == np.float32
+    assert np.array_equal(out[..., :3].reshape(-1, 3), v) and not out[..., 3].any()
+
+    class Fake:
+        def getVertices(self, tn):
+            return v + tn, -v, np.zeros_like(v)
+    assert np.array_equal(CLDraw.getVertPoints(Fake(), 1)[..., :3].reshape(-1, 3), v + 1)
+    assert np.array_equal(CLDraw.getVertNorms(Fake(), 0)[..., :3].reshape(-1, 3), -v)
+
+
 def test_mip_chain_layout():
     rgb = np.random.default_rng(0).integers(0, 8000, (16, 16, 3))
     planes, num = S.texture_planes(rgb.astype(np.uint16), True)
