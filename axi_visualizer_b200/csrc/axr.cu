@@ -6,6 +6,8 @@
 // light I as packed float triplets/pairs, 3 vertices per triangle) and the
 // texture planes (mip chain smallest level first); work queues sized by the
 // triangle count (small/large lists) and a grow-only tile-unit queue.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <limits.h>
 #include <stdarg.h>
@@ -1917,8 +1919,15 @@ constexpr uint32_t NOALLOC_WORDS = NOALLOC_MAX_TRIS + CTR_N;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_WORDS];
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
-uint32_t *g_noalloc_ptr[NOALLOC_MAX_DEVICES];       // device address of the array, per device
+struct NoallocSlot {
+  unsigned long long ctx_id;   // the context the address was resolved in
+  uint32_t *ptr;               // device address of the array there
+};
+NoallocSlot g_noalloc[NOALLOC_MAX_DEVICES];
 std::mutex g_noalloc_mu;
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+PFN_cuCtxGetId_v12000 g_ctx_id = nullptr;
+bool g_ctx_fns_looked_up = false;
 
 // One caster group, passed by value (no device-side table).
 __global__ void __launch_bounds__(256) k_shadow_setup_noalloc(GroupDev G, ShadowParams S) {
@@ -1945,20 +1954,60 @@ __global__ void __launch_bounds__(128, ALPHA ? 6 : 8) k_shadow_raster_noalloc(Gr
   shadow_warp_loop<ALPHA>(S, sg, qs[w], lane, ALPHA ? CTR_SH_LIST_A : CTR_SH_LIST, ALPHA ? CTR_SH_WORK_A : CTR_SH_WORK);
 }
 
-// Resolves the device address of g_noalloc_scratch for the current device
-// (once per device; the host-side name is only a stand-in for it).
+// The process-unique id of the context current on this thread (binding the
+// device's primary context first if none is), through the driver's
+// cuCtxGetCurrent / cuCtxGetId, which only read host state.  Returns false
+// when the driver does not provide them.
+bool current_ctx_id(int dev, unsigned long long *id) {
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_ctx_fns_looked_up) {
+      g_ctx_fns_looked_up = true;
+      void *f1 = nullptr, *f2 = nullptr;
+      cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+      cudaError_t e1 = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1);
+      cudaError_t e2 = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2);
+      if (e1 == cudaSuccess && e2 == cudaSuccess && q1 == cudaDriverEntryPointSuccess &&
+          q2 == cudaDriverEntryPointSuccess && f1 && f2) {
+        g_ctx_current = (PFN_cuCtxGetCurrent_v4000)f1;
+        g_ctx_id = (PFN_cuCtxGetId_v12000)f2;
+      }
+      if (e1 != cudaSuccess || e2 != cudaSuccess) cudaGetLastError();   // the failed lookup's error is not the caller's
+    }
+  }
+  if (!g_ctx_current || !g_ctx_id) return false;
+  CUcontext ctx = nullptr;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS) return false;
+  if (!ctx) {
+    if (cudaSetDevice(dev) != cudaSuccess || g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  }
+  return g_ctx_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Resolves the device address of g_noalloc_scratch in the current context
+// (the host-side name is only a stand-in for it).  The address is cached per
+// device together with the context's id and looked up again only when the
+// context changes: after cudaDeviceReset the runtime loads the module into a
+// new context, where the array may sit elsewhere.  Without the driver's
+// context id it is looked up on every call.
 int noalloc_scratch(uint32_t **out) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(AXR_EINVAL, "device %d beyond %d", dev, NOALLOC_MAX_DEVICES);
+  unsigned long long id = 0;
+  bool have_id = current_ctx_id(dev, &id);
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return fail(AXR_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = (uint32_t *)p;
+  NoallocSlot &sl = g_noalloc[dev];
+  if (have_id && sl.ptr && sl.ctx_id == id) {
+    *out = sl.ptr;
+    return 0;
   }
-  *out = g_noalloc_ptr[dev];
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) return fail(AXR_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+  sl.ptr = have_id ? (uint32_t *)p : nullptr;   // without a context id a cached copy cannot be checked
+  sl.ctx_id = id;
+  *out = (uint32_t *)p;
   return 0;
 }
 
