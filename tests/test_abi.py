@@ -23,6 +23,23 @@ def test_header_lists_match_binding():
     assert sorted(EXPORTS) == declared()
 
 
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c++", "-std=c++11")])
+def test_header_is_plain_c_and_cpp(lang, std, tmp_path):
+    """The boundary header compiles warning-free as pedantic C99 and as
+    C++11, with no CUDA or torch headers on the include path."""
+    cc = "gcc" if lang == "c" else "g++"
+    try:
+        subprocess.run([cc, "--version"], capture_output=True, check=True)
+    except (OSError, subprocess.CalledProcessError):
+        pytest.skip(f"{cc} not available")
+    src = tmp_path / "use_axr.c"
+    src.write_text('#include "axr.h"\nint main(void) { return 0; }\n')
+    r = subprocess.run([cc, "-x", lang, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                        os.path.dirname(HEADER), "-c", str(src), "-o", str(tmp_path / "use_axr.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_library_loads_and_exports_all_symbols():
     if not os.path.exists(LIB):
         from axi_visualizer_b200 import build
