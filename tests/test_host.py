@@ -19,6 +19,20 @@ def test_named_scene_sizes():
     assert sc.alphas[0][1] == 1024 and 0.55 < sc.alphas[0][0].mean() < 0.65
 
 
+def test_frame_bytes_formula():
+    """The roofline's per-frame algorithmic bytes for the 1080p scene:
+    132 T + sum over cascades (36 T_cast + 24 T_alpha_cast) + 10 W H +
+    4 sum S^2, about 269 MB (texture and shadow-map reads excluded)."""
+    import bench
+    sc = S.scene_c2()
+    T = sc.ntris
+    assert all(g.cast for g in sc.groups)
+    want = 132 * T + 2 * (36 * T + 24 * 40000) + 10 * 1920 * 1080 + 4 * 2 * 2048 * 2048
+    assert (bench.W, bench.H) == (1920, 1080)
+    assert bench.frame_bytes(sc) == want
+    assert 268e6 < want < 270e6
+
+
 def test_camera_bases_orthonormal():
     for a, b in ((0.3, 0.2), (1.7 * math.pi, 0.52), (-2.0, -0.7)):
         for m in (S.camera_basis(a, b), S.view_mat(a, b)):
