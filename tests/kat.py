@@ -226,3 +226,39 @@ def decode_shadow_count(red, amb=0.2):
     plane (T0 * light * LInt.x, light = (s * amb + 5 - s) * 0.2)."""
     light = red.astype(np.float64) / (BORDER_T0 * float(S.LIGHT_INTS[0][0]))
     return np.rint((1.0 - light) / ((1.0 - amb) * 0.2)).astype(np.int64)
+
+
+# trilinear mip selection (av_draw_normmap_mip.c:37-45): the per-triangle
+# level fmip = clamp(|log2 dt| / 2 + mipBias, 0, numMip - 1) from the
+# largest |dUV| / (edge length in pixels)^2 over the three edges
+MIP_SIDE = 16                # levels of side 1, 2, 4, 8, 16 (numMip = 4), smallest first
+MIP_LEVEL_VALUE = 1000       # level k holds MIP_LEVEL_VALUE * (k + 1) in every texel
+
+
+def mip_scene(w=192, h=144):
+    """One triangle per group, each a case of the level selection, at depth
+    5 and apart on screen: (screen vertices, uvs, mipBias).  Every level of
+    the texture is a constant, the vertex light is 1 and the normals face
+    away from the light, so a pixel's red value is
+    MIP_LEVEL_VALUE * (1 + fmip): the level blend reads back as fmip.
+      0 tiled path, mid-range level (dt = 2^-5: fmip 2.5)
+      1 tiled path, dt tiny: clamped to numMip - 1
+      2 small path, mipBias -10: clamped to 0
+      3 small path, dt > 1 (a 6-pixel triangle spanning 100 texture units)
+      4 small path, fractional vertices (edge lengths from the truncated ones)
+    """
+    cases = [([(4.0, 4.0), (120.0, 4.0), (4.0, 70.0)], [(0, 0), (242.0, 0), (0, 100.0)], 0.0),
+             ([(70.0, 140.0), (190.0, 140.0), (190.0, 76.0)], [(0, 0), (0.01, 0), (0, 0.01)], 0.0),
+             ([(130.25, 10.25), (160.25, 10.25), (130.25, 40.25)], [(0, 0), (3.0, 0), (0, 3.0)], -10.0),
+             ([(10.25, 100.25), (16.25, 100.25), (10.25, 106.25)], [(0, 0), (100.0, 0), (0, 100.0)], 0.0),
+             ([(30.7, 90.2), (60.4, 91.9), (35.5, 120.8)], [(0, 0), (150.0, 1.0), (10.0, 20.0)], 0.3)]
+    nmip = int(np.log2(MIP_SIDE))
+    chain = np.concatenate([np.full(4 ** k, MIP_LEVEL_VALUE * (k + 1), np.uint16) for k in range(nmip + 1)])
+    groups = []
+    for pts, uv, bias in cases:
+        xyz = np.asarray(tri(w, h, [(x, y, 5.0) for x, y in pts]), np.float32)
+        groups.append(S.Group(xyz, np.asarray(uv, np.float32), np.tile(np.float32([0, 0, 1]), (3, 1)),
+                              np.ones((3, 3), np.float32), (chain, chain.copy(), chain.copy()), nmip, S.MIP,
+                              mip_bias=bias))
+    sc = S.Scene(groups, [], np.asarray(S.LIGHT_INTS[0], np.float32), np.array([0, 0, -1], np.float32), 0.2, [])
+    return sc, view(w, h), cases

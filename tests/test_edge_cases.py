@@ -129,3 +129,51 @@ def test_shadow_border_maps_and_depth_equal_reference():
     assert rd.draw_all() == 0
     db = rd.get_frame()[3]
     assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32))
+
+
+def expected_fmip(pts, uv, bias, nmip):
+    """av_draw_normmap_mip.c:37-45 evaluated in float64: the largest
+    |dUV| / (edge length in pixels)^2 over the three edges, then
+    clamp(|log2 dt| / 2 + mipBias, 0, numMip - 1).  Small triangles (integer
+    bounding box under 96 pixels, trisetup.c) use their truncated vertices,
+    as the small path does (Templates.py:230-231); large ones the float
+    vertices of the tiled path."""
+    p = np.asarray(pts, np.float64)
+    small = max(np.ptp(np.trunc(p), axis=0)) < 96
+    if small:
+        p = np.trunc(p)
+    u = np.asarray(uv, np.float64)
+    dt = 0.0
+    for i, j in ((0, 1), (0, 2), (1, 2)):
+        d2 = float(((p[j] - p[i]) ** 2).sum())
+        dt = max(dt, *np.abs((u[j] - u[i]) / d2))
+    return min(max(abs(np.log2(dt)) / 2 + bias, 0.0), nmip - 1.0), small
+
+
+def test_trilinear_level_selection():
+    """The per-triangle mip level on the oracle against the formula, read
+    back from constant-per-level textures: a mid-range level and the upper
+    clamp on the tiled path; the lower clamp, dt > 1 and truncated vertices
+    on the small path."""
+    sc, view, cases = kat.mip_scene()
+    fr = O.Frame(view.w, view.h)
+    O.clear_depth(fr.db)
+    O.draw_all(sc, view, fr, [])
+    nmip = int(np.log2(kat.MIP_SIDE))
+    paths = []
+    for k, (pts, uv, bias) in enumerate(cases):
+        px = fr.tri_id == k
+        assert px.sum() >= 20, k
+        got = fr.ro[px].astype(np.float64) / kat.MIP_LEVEL_VALUE - 1.0
+        want, small = expected_fmip(pts, uv, bias, nmip)
+        paths.append(small)
+        assert np.abs(got - want).max() <= 2e-3, (k, float(got.min()), float(got.max()), want)
+    assert paths == [False, False, True, True, True]
+    # the clamps are reached, and case 4 tells truncated edges from float ones
+    assert expected_fmip(*cases[1], nmip)[0] == nmip - 1 and expected_fmip(*cases[2], nmip)[0] == 0.0
+    pts, uv, bias = cases[4]
+    p, u = np.asarray(pts), np.asarray(uv, np.float64)
+    dt_float = max(max(np.abs((u[j] - u[i]) / ((p[j] - p[i]) ** 2).sum())) for i, j in ((0, 1), (0, 2), (1, 2)))
+    float_level = abs(np.log2(dt_float)) / 2 + bias
+    got4 = fr.ro[fr.tri_id == 4].astype(np.float64) / kat.MIP_LEVEL_VALUE - 1.0
+    assert np.abs(got4 - float_level).min() > 5e-3
