@@ -14,8 +14,8 @@ LIB_PATH = os.path.join(HERE, "libaxr.so")
 # every symbol include/axr.h declares (tests check the exports against this)
 EXPORTS = [
     "axr_last_error", "axr_create", "axr_destroy", "axr_set_scale_cull", "axr_add_texture_group",
-    "axr_set_vert_light", "axr_vert_light", "axr_transform", "axr_translate", "axr_get_vertices", "axr_copy_to",
-    "axr_ssao", "axr_dof", "axr_bloom", "axr_add_tex_alpha", "axr_set_primary_light",
+    "axr_set_vert_light", "axr_vert_light", "axr_transform", "axr_translate", "axr_set_mip_bias", "axr_get_vertices",
+    "axr_copy_to", "axr_ssao", "axr_dof", "axr_bloom", "axr_add_tex_alpha", "axr_set_primary_light",
     "axr_set_pos", "axr_set_vm", "axr_clear_zbuffer", "axr_draw_all", "axr_get_frame", "axr_get_ids",
     "axr_set_frame", "axr_gamma", "axr_add_shadow_map", "axr_place_shadow_map", "axr_clear_shadow_map",
     "axr_shadow_map", "axr_get_shadow_map", "axr_sync", "axr_get_stream", "axr_frame_device_ptrs",
@@ -50,6 +50,7 @@ _SIGS = {
     "axr_transform": (i32, [vp, i32, vp, vp, vp, i32, i32]),
     "axr_translate": (i32, [vp, i32, vp, i32, i32]),
     "axr_get_vertices": (i32, [vp, i32, vp, vp, vp]),
+    "axr_set_mip_bias": (i32, [vp, i32, f32]),
     "axr_ssao": (i32, [vp, vp, i32]),
     "axr_dof": (i32, [vp, f32]),
     "axr_bloom": (i32, [vp]),

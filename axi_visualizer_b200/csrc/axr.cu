@@ -50,6 +50,7 @@ struct Group {
   ushort4 *tex = nullptr;     // interleaved (R, G, B, 0) texels
   int ntris = 0, tri_base = 0, tex_size = 0, mip_side = 0;
   long ntexels = 0;
+  float mip_bias = 0.f;       // mipBias of the trilinear level selection (axr_set_mip_bias)
 };
 
 struct Alpha {
@@ -346,7 +347,7 @@ int group_table(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, co
     d.tex = G.tex;
     d.ntris = G.ntris; d.tri_base = G.tri_base; d.tex_size = G.tex_size;
     d.flags = flags ? flags[g] : 0;
-    d.mip_bias = 0.f;
+    d.mip_bias = G.mip_bias;
     bool on = true;
     if (enabled_mask) on = mask_means_enabled ? enabled_mask[g] != 0 : enabled_mask[g] == 0;
     d.enabled = on ? 1 : 0;
@@ -716,6 +717,15 @@ int axr_translate(axr_ctx *c, int group, const float *coords, int v_start, int v
     CK(cudaGetLastError());
     return 0;
   });
+}
+
+int axr_set_mip_bias(axr_ctx *c, int group, float bias) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (group < 0 || group >= (int)c->groups.size()) return fail(AXR_EINVAL, "group %d", group);
+  if (!(bias == bias) || bias > 1e30f || bias < -1e30f) return fail(AXR_EINVAL, "mip bias is not a finite number");
+  c->groups[group].mip_bias = bias;
+  return 0;
 }
 
 int axr_get_vertices(axr_ctx *c, int group, float *xyz, float *vn, float *li) {

@@ -57,6 +57,7 @@ class CLDraw:
         self._h = h_
         self.gSize = []           # vertex counts per group (reference name)
         self.texSize = []
+        self._mip_bias = []       # mipBias per group, as the library holds it
         self._tex_alpha = 0
         self.SHADOWMAP = {}
         self.ambLight = np.float32(0.2)
@@ -112,7 +113,16 @@ class CLDraw:
                                             rr.size, int(mip) if mip else 0, C.byref(out)), "addTextureGroup")
         self.gSize.append(np.int32(p.shape[0]))
         self.texSize.append(np.int32(np.log2(mip)) if mip else np.int32(int(round(rr.size ** 0.5))))
+        self._mip_bias.append(np.float32(0.0))
         return out.value
+
+    def setMipBias(self, tn, bias):
+        """Sets group tn's mipBias (av_draw_normmap_mip.c:43), kept for every
+        later drawAll and batch render.  New: the reference passes it per
+        draw as a dict material's "mip" value, which drawAll also accepts."""
+        b = np.float32(bias)
+        check(self._L.axr_set_mip_bias(self._h, int(tn), C.c_float(b)), "setMipBias")
+        self._mip_bias[int(tn)] = b
 
     def setVertLight(self, tn, li):
         """Uploads the per-vertex light `I` of group tn (what vertLight computes)."""
@@ -235,8 +245,18 @@ class CLDraw:
                 aidx[i] = int(s["alpha"])
         return flags, aidx
 
+    @staticmethod
+    def _dict_mip_biases(shaders, n):
+        """{group: mipBias} for the dict materials that carry a "mip" value:
+        the reference reads it as np.float32(material["mip"]) (Ops.py:687)."""
+        items = shaders.items() if isinstance(shaders, dict) else enumerate(shaders)
+        return {int(i): np.float32(s["mip"]) for i, s in items if isinstance(s, dict) and "mip" in s and int(i) < n}
+
     def drawAll(self, shaders, mask=None, shadowIds=(0, 1), useOpacitySM=False):
         flags, aidx = self._material_args(shaders)
+        for i, b in self._dict_mip_biases(shaders, len(self.gSize)).items():
+            if b != self._mip_bias[i]:
+                self.setMipBias(i, b)
         m = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
         ids = [int(i) for i in shadowIds if int(i) in self.SHADOWMAP][:2]
         sid = np.asarray(ids + [0, 0], np.int32)[:2]
@@ -454,7 +474,12 @@ class SceneRenderer:
             self.draw.placeShadowMapBasis(k, sc.pos, sc.vv, scene.amb)
         self.flags = [g.flags for g in scene.groups]
         names = (("mip", 1), ("shadow", 4), ("cull", 8), ("multi", 16))
-        self.shaders = [{"alpha": g.alpha_index, **{k: 1 for k, b in names if g.flags & b}} if g.flags & 2 else
+        for k, g in enumerate(scene.groups):
+            if g.mip_bias:
+                self.draw.setMipBias(k, g.mip_bias)
+        # a dict material's "mip" value is its mipBias (Ops.py:687)
+        self.shaders = [{"alpha": g.alpha_index, **{k: (np.float32(g.mip_bias) if k == "mip" else 1)
+                                                     for k, b in names if g.flags & b}} if g.flags & 2 else
                         " ".join(k for k, b in names if g.flags & b)
                         for g in scene.groups]
 

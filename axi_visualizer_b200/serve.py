@@ -362,10 +362,11 @@ class Server:
 # ---------------------------------------------------------------------------
 
 def _shader(g, alpha_base):
-    """CLDraw shader description of a scenes.Group (alpha index made global)."""
+    """CLDraw shader description of a scenes.Group (alpha index made global;
+    a dict material's "mip" value is its mipBias, Ops.py:687)."""
     names = [k for k, b in (("mip", 1), ("shadow", 4), ("cull", 8)) if g.flags & b]
     if g.flags & 2:
-        return {"alpha": alpha_base + g.alpha_index, **{k: 1 for k in names}}
+        return {"alpha": alpha_base + g.alpha_index, **{k: (np.float32(g.mip_bias) if k == "mip" else 1) for k in names}}
     return " ".join(names)
 
 
@@ -389,6 +390,8 @@ def load_scenes(draw, scenes):
             r, gg, b = g.tex
             draw.addTextureGroup(g.xyz, g.uv, g.vn, r, gg, b, mip=(1 << g.tex_size) if g.flags & 1 else False)
             draw.setVertLight(group, g.li)
+            if g.mip_bias:
+                draw.setMipBias(group, g.mip_bias)
             shaders.append(_shader(g, alpha_base))
             group += 1
         for m, side in sc.alphas:

@@ -106,6 +106,14 @@ int axr_transform(axr_ctx *ctx, int group, const float *old_rm, const float *rot
  * axr_transform. */
 int axr_translate(axr_ctx *ctx, int group, const float *coords, int v_start, int v_end);
 
+/* The mipBias of a group's trilinear level selection
+ * (av_draw_normmap_mip.c:20,43: fmip = clamp(|log2 dt| / 2 + mipBias, 0,
+ * numMip - 1)), which the reference passes per draw as the value of a dict
+ * material's "mip" entry (Ops.py:687).  It stays with the group for every
+ * later drawAll and batch render; 0 until set.  A bias that is not a finite
+ * number is refused. */
+int axr_set_mip_bias(axr_ctx *ctx, int group, float bias);
+
 /* New: copies a group's vertex arrays to the host ([3*ntris][3] each; any
  * pointer may be NULL) after the work queued before it on the handle's
  * stream.  The reference keeps them in device buffers (Ops.py:618-620). */

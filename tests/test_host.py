@@ -59,6 +59,46 @@ def test_cldraw_material_args_without_gpu():
         CLDraw._material_args(Fake(), ["mip"])
 
 
+def test_dict_material_mip_value_is_the_mip_bias():
+    """drawAll reads a dict material's "mip" value as the group's mipBias,
+    as the reference does (np.float32(material["mip"]), Ops.py:687), and
+    tells the library only when a group's bias changes; string materials
+    leave the bias as it is."""
+    from axi_visualizer_b200.ops import CLDraw
+    calls = []
+
+    class FakeLib:
+        def axr_draw_all(self, *a):
+            calls.append(("draw",))
+            return 0
+
+        def axr_set_mip_bias(self, h, tn, b):
+            calls.append(("bias", tn, float(b.value)))
+            return 0
+
+    class Fake:
+        gSize = [3, 3, 3, 3]
+        SHADOWMAP = {}
+        _h = None
+        _L = FakeLib()
+        _mip_bias = [np.float32(0)] * 4
+        _material_args = CLDraw._material_args
+        _dict_mip_biases = staticmethod(CLDraw._dict_mip_biases)
+        setMipBias = CLDraw.setMipBias
+
+    f = Fake()
+    shaders = ["mip shadow", {"alpha": 0, "mip": 0.5}, {"alpha": 1, "mip": True}, {"alpha": 0}]
+    CLDraw.drawAll(f, shaders, shadowIds=[])
+    assert calls == [("bias", 1, 0.5), ("bias", 2, 1.0), ("draw",)]
+    assert [float(b) for b in f._mip_bias] == [0.0, 0.5, 1.0, 0.0]
+    calls.clear()
+    CLDraw.drawAll(f, shaders, shadowIds=[])          # unchanged: no library call
+    assert calls == [("draw",)]
+    calls.clear()
+    CLDraw.drawAll(f, {1: {"alpha": 0, "mip": 0.0}, 0: "mip"}, shadowIds=[])
+    assert calls == [("bias", 1, 0.0), ("draw",)]
+
+
 # every method of the reference's CLDraw (PyOpenCL27C/Ops.py:127-1230)
 REFERENCE_CLDRAW_METHODS = """
 __init__ addBoneWeights addNrmMap addOpacityMap addRghMap addShadowMap addTexAlpha addTexture addTextureGroup
