@@ -99,6 +99,51 @@ def test_dict_material_mip_value_is_the_mip_bias():
     assert calls == [("bias", 1, 0.0), ("draw",)]
 
 
+def test_scene_renderer_hands_every_group_field_to_the_draw(monkeypatch):
+    """SceneRenderer passes each field of a scene group that the oracle
+    reads (positions, uvs, normals, vertex light, texture planes and mip
+    chain, flags, alpha index, mipBias) and each cascade to the draw
+    runtime.  Recorded through a stand-in CLDraw, without a GPU."""
+    import kat
+    from axi_visualizer_b200 import ops
+    log = []
+
+    class Rec:
+        def __init__(self, *a, **k):
+            pass
+
+        def __getattr__(self, name):
+            return lambda *a, **k: log.append((name, a, k))
+
+    real = ops.CLDraw
+    monkeypatch.setattr(ops, "CLDraw", Rec)
+    sc, view, cases = kat.mip_scene()
+    sc.groups[1].flags |= S.ALPHA
+    sc.alphas = [(np.ones(kat.MIP_SIDE ** 2, np.uint8), kat.MIP_SIDE)]
+    sc.shadows = [S.ShadowCam.facing(64, 3.0, (0, 0, 6), (0.0, 0.0), dist=20.0)]
+    R = ops.SceneRenderer(sc, view.w, view.h)
+    adds = [a for n, a, k in log if n == "addTextureGroup"]
+    mips = [k.get("mip") for n, a, k in log if n == "addTextureGroup"]
+    assert len(adds) == len(sc.groups)
+    for g, a, mip in zip(sc.groups, adds, mips):
+        for got, want in zip(a, (g.xyz, g.uv, g.vn) + tuple(g.tex)):
+            assert np.array_equal(got, want)
+        assert mip == 1 << g.tex_size
+    lis = {a[0]: a[1] for n, a, k in log if n == "setVertLight"}
+    assert all(np.array_equal(lis[i], g.li) for i, g in enumerate(sc.groups))
+    biases = {a[0]: float(a[1]) for n, a, k in log if n == "setMipBias"}
+    assert biases == {i: float(g.mip_bias) for i, g in enumerate(sc.groups) if g.mip_bias}
+    assert [n for n, a, k in log].count("addTexAlpha") == 1
+    assert [a[:2] for n, a, k in log if n == "addShadowMap"] == [(0, 64)]
+    assert [a[0] for n, a, k in log if n == "placeShadowMapBasis"] == [0]
+    # materials: flags and alpha index as the oracle reads them, mipBias in the dict form
+    fake = type("F", (), {"gSize": [3] * len(sc.groups)})()
+    flags, aidx = real._material_args(fake, R.shaders)
+    assert flags.tolist() == [g.flags for g in sc.groups]
+    assert aidx.tolist() == [g.alpha_index for g in sc.groups]
+    assert real._dict_mip_biases(R.shaders, len(sc.groups)) == {1: np.float32(sc.groups[1].mip_bias)}
+
+
 # every method of the reference's CLDraw (PyOpenCL27C/Ops.py:127-1230)
 REFERENCE_CLDRAW_METHODS = """
 __init__ addBoneWeights addNrmMap addOpacityMap addRghMap addShadowMap addTexAlpha addTexture addTextureGroup
