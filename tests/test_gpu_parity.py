@@ -91,3 +91,24 @@ def test_c1_scene_parity():
     exact, psnr = check_frame(fr, smaps, got)
     st = R.draw.lastStats()
     assert st["n_small"] > 0
+
+
+@pytest.mark.parametrize("pos", [(0, 8, -20), (4, 3, -6)])
+def test_alpha_tested_trilinear_materials(pos):
+    """The composed material in full (alpha test, trilinear mip, double
+    cascade), with and without culling, as the 3840x2160 stress scene uses
+    it, on a miniature of that scene (64x64 terrain in 4 bands, 300
+    icospheres, 64^2 textures and mask, 512^2 + 256^2 cascades): against
+    the oracle at the parity bars."""
+    sc = S.scene_c5(seed=7, terrain_n=64, spheres=300, tex=64, terrain_groups=4, sphere_groups=2,
+                    alpha_terrain=(1, 2), alpha_spheres=(0,), cascades=(512, 256), extent=16.0)
+    view = S.default_view(320, 240, pos=pos)
+    fr, smaps, got, R = render_both(sc, view)
+    exact, psnr = check_frame(fr, smaps, got)
+    base = np.cumsum([0] + [g.ntris for g in sc.groups])
+    composed = np.zeros(fr.cov.shape, bool)
+    for k, g in enumerate(sc.groups):
+        if g.flags & S.ALPHA and g.flags & S.MIP:
+            composed |= (fr.tri_id >= base[k]) & (fr.tri_id < base[k + 1])
+    assert composed.sum() > 1000
+    assert exact > 0.999
