@@ -52,6 +52,17 @@ KERNELS = [
     ("ref_drawmulti", "PyOpenCL27C/Shaders/drawmulti.c", SAT_STORES),
 ]
 
+# kernels the reference generates from an AVSL source with its own
+# Shaders_src/AVSL.py (compile_AVSL: the tiled `draw`, then `drawSmall`, as
+# compile_file writes them): (namespace, AVSL source, prelude).  The
+# normal-mapped mip material calls `sampleShadow`, which the reference
+# defines nowhere; the prelude gives it a stand-in returning 0 (no shadow),
+# exact for the pin, which draws with a zero light intensity.
+NO_SHADOW = "inline float sampleShadow(float, float, float, float *, int, float) { return 0.f; }"
+GENERATED = [
+    ("ref_draw_mip", "PyOpenCL27C/Shaders_src/av_draw_normmap_mip.c", NO_SHADOW),
+]
+
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
             "-fopenmp", "-pthread", "-w", "-DBLOCK_SIZE=128"]
 
@@ -79,6 +90,23 @@ def translate(src: str, ns: str, prelude: str = "") -> str:
 DEFAULT_REFERENCE = os.environ.get("AXR_REFERENCE", "/root/reference")
 
 
+def avsl_expand(reference: str, rel: str) -> str:
+    """The OpenCL C the reference's generator makes from an AVSL source (run
+    in memory: Shaders_src is imported from the checkout as a package)."""
+    root = os.path.join(reference, "PyOpenCL27C")
+    sys.path.insert(0, root)
+    try:
+        import importlib
+        avsl = importlib.import_module("Shaders_src.AVSL")
+        with open(os.path.join(reference, rel)) as f:
+            lines = f.readlines()
+        return avsl.compile_AVSL(lines, True) + "\n\n\n" + avsl.compile_AVSL(lines, False)
+    finally:
+        sys.path.remove(root)
+        for k in [k for k in sys.modules if k == "Shaders_src" or k.startswith("Shaders_src.")]:
+            del sys.modules[k]
+
+
 def build(reference: str = DEFAULT_REFERENCE, verbose: bool = False) -> str | None:
     if not os.path.isdir(os.path.join(reference, "PyOpenCL27C")):
         print(f"build_ref: reference checkout not found at {reference}; skipped")
@@ -93,6 +121,14 @@ def build(reference: str = DEFAULT_REFERENCE, verbose: bool = False) -> str | No
         cmd = ["g++", *CXXFLAGS, "-I", HERE, "-x", "c++", "-c", "-", "-o", obj]
         if verbose:
             print(" ".join(cmd), "<", rel)
+        subprocess.run(cmd, input=src.encode(), check=True)
+        objs.append(obj)
+    for ns, rel, pre in GENERATED:
+        src = translate(avsl_expand(reference, rel), ns, pre)
+        obj = os.path.join(OUT, ns + ".o")
+        cmd = ["g++", *CXXFLAGS, "-I", HERE, "-x", "c++", "-c", "-", "-o", obj]
+        if verbose:
+            print(" ".join(cmd), "<", rel, "(expanded)")
         subprocess.run(cmd, input=src.encode(), check=True)
         objs.append(obj)
     harness = os.path.join(HERE, "ref_harness.cpp")

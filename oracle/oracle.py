@@ -339,6 +339,8 @@ def ref_lib():
         R.ref_ssao.argtypes = [C.c_void_p, C.c_void_p]
         R.ref_bloom.argtypes = [C.c_void_p]
         R.ref_dof.argtypes = [C.c_void_p, C.c_float]
+        R.ref_set_mip_kernels.restype = C.c_int
+        R.ref_set_mip_kernels.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         R.ref_get_geometry.restype = C.c_int
         R.ref_get_geometry.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 3
         _ref = R
@@ -373,6 +375,14 @@ class RefDraw:
             self.R.ref_destroy(self.h)
         except Exception:
             pass
+
+    def set_mip_kernels(self, on=True):
+        """Draw the mip groups with the reference's normal-mapped mip material
+        (Shaders_src/av_draw_normmap_mip.c as its AVSL generator expands it),
+        each group with its mipBias."""
+        bias = np.array([g.mip_bias for g in self.scene.groups], np.float32)
+        if self.R.ref_set_mip_kernels(self.h, 1 if on else 0, _ptr(bias), len(bias)) != 0:
+            raise RuntimeError("ref_set_mip_kernels")
 
     def clear_zbuffer(self):
         self.R.ref_clear_zbuffer(self.h)

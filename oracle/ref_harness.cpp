@@ -56,6 +56,18 @@ void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P,
                ushort *TB, const int lenT, const int wF, const int hF, const int lenP);
 float *local_ZBuf();
 }
+// Shaders_src/av_draw_normmap_mip.c expanded by the reference's AVSL generator
+namespace ref_draw_mip {
+void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+          float3 *I, float3 *N, float3 *PXYZ, ushort *TR, ushort *TG, ushort *TB, const int numMip, uchar3 *NM,
+          float *Vpos, float3 *LInt, float3 *LDir, float *SD, const int wS, const float sScale, float3 *SV,
+          float *SPos, const float mipBias, const int wF, const int hF);
+void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+               float3 *I, float3 *N, float3 *PXYZ, ushort *TR, ushort *TG, ushort *TB, const int numMip,
+               uchar3 *NM, float *Vpos, float3 *LInt, float3 *LDir, float *SD, const int wS, const float sScale,
+               float3 *SV, float *SPos, const float mipBias, const int wF, const int hF, const int lenP);
+float *local_ZBuf();
+}
 namespace ref_draw_alpha {
 void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
           float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, ushort *TR, ushort *TG, ushort *TB,
@@ -131,6 +143,10 @@ struct Group {
   std::vector<int> tia, tib, tna, tnb, toa, tob;
   std::vector<ushort> tr, tg, tb;
   int tex_size = 0;
+  // the normal-mapped mip material: its normal map (one texel per texel of
+  // the chain) and the draw's mipBias
+  std::vector<uchar3> nm;
+  float mip_bias = 0;
 };
 
 struct Shadow {
@@ -155,6 +171,7 @@ struct Ctx {
   float3 lint[1], ldir[1];
   Shadow shadows[8];
   int overflow = 0;
+  int mip_kernels = 0;   // mip groups (flags bit 0) drawn by ref_draw_mip
 };
 
 // run kernel `fn(bx, tx)` over a 1-D grid of `ng` groups of BS items
@@ -311,6 +328,25 @@ int ref_add_alpha(void *h, const uint8_t *mask, int len) {
   return (int)c->alphas.size() - 1;
 }
 
+// Draws the mip groups with the reference's normal-mapped mip material
+// (on != 0), each with its mipBias and a flat normal map (128, 128, 255).
+// Its shadow lookup `sampleShadow` is defined nowhere in the reference; the
+// build gives it a stand-in returning 0, which is exact for the pin's use:
+// with a zero light intensity the shadow term and the specular term vanish.
+int ref_set_mip_kernels(void *h, int on, const float *bias, int n) {
+  Ctx *c = (Ctx *)h;
+  if (n != (int)c->groups.size()) return -1;
+  c->mip_kernels = on;
+  for (int i = 0; i < n; i++) {
+    Group &G = c->groups[i];
+    G.mip_bias = bias ? bias[i] : 0.f;
+    uchar3 flat;
+    flat.x = 128; flat.y = 128; flat.z = 255; flat.pad_ = 0;
+    G.nm.assign(G.tr.size(), flat);
+  }
+  return 0;
+}
+
 void ref_set_view(void *h, const float *pos, const float *vv, float sscale, float cax, float cay) {
   Ctx *c = (Ctx *)h;
   for (int i = 0; i < 3; i++) c->vpos[i] = pos[i];
@@ -392,6 +428,12 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
                                  m.t[0][0], m.t[0][1], m.t[0][2], m.len[0], m.t[1][0], m.t[1][1], m.t[1][2], m.len[1],
                                  m.t[2][0], m.t[2][1], m.t[2][2], m.len[2], m.t[3][0], m.t[3][1], m.t[3][2], m.len[3],
                                  c->W, c->H, newSize[tn]);
+      } else if (!alpha && c->mip_kernels && (flags[tn] & 1)) {
+        float sd[4] = {0, 0, 0, 0};
+        ref_draw_mip::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(), G.sp.data(),
+                                G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), G.tr.data(),
+                                G.tg.data(), G.tb.data(), G.tex_size, G.nm.data(), c->vpos, c->lint, c->ldir, sd, 1,
+                                1.0f, c->vmat, c->vpos, G.mip_bias, c->W, c->H, newSize[tn]);
       } else if (alpha)
         ref_draw_alpha::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(),
                                   G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(),
@@ -429,7 +471,9 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
     bool *TA = alpha ? (bool *)c->alphas[alpha_index[tn]].data() : nullptr;
     int ntiles = c->WC * c->HC;
     auto tile = [&](int bx) {
-      float *zb = multi ? ref_drawmulti::local_ZBuf() : alpha ? ref_draw_alpha::local_ZBuf() : ref_draw::local_ZBuf();
+      bool mipk = !alpha && !multi && c->mip_kernels && (flags[tn] & 1);
+      float *zb = multi ? ref_drawmulti::local_ZBuf() : alpha ? ref_draw_alpha::local_ZBuf()
+                  : mipk ? ref_draw_mip::local_ZBuf() : ref_draw::local_ZBuf();
       int tileX = bx % c->WC, tileY = bx / c->WC;
       for (int r = 0; r < 16; r++)
         for (int i = 0; i < 16; i++) zb[r * 16 + i] = c->db[(size_t)c->W * (tileY * 16 + r) + tileX * 16 + i];
@@ -445,6 +489,12 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
                               c->ldir, m.t[0][0], m.t[0][1], m.t[0][2], m.len[0], m.t[1][0], m.t[1][1], m.t[1][2],
                               m.len[1], m.t[2][0], m.t[2][1], m.t[2][2], m.len[2], m.t[3][0], m.t[3][1], m.t[3][2],
                               m.len[3], c->W, c->H);
+        } else if (mipk) {
+          float sd[4] = {0, 0, 0, 0};
+          ref_draw_mip::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
+                             c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),
+                             G.xyz.data(), G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, G.nm.data(), c->vpos,
+                             c->lint, c->ldir, sd, 1, 1.0f, c->vmat, c->vpos, G.mip_bias, c->W, c->H);
         } else if (alpha)
           ref_draw_alpha::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
                                c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),

@@ -159,4 +159,27 @@ struct sat_u16 {
 static_assert(sizeof(sat_u16) == 2, "sat_u16 aliases a u16 buffer");
 inline float3 convert_float3(ushort3 a) { return make_float3((float)a.x, (float)a.y, (float)a.z); }
 
+// for the normal-mapped mip material (Shaders_src/av_draw_normmap_mip.c)
+struct uchar3 {
+  uchar x, y, z, pad_;   // OpenCL uchar3 occupies 4 bytes
+};
+static_assert(sizeof(uchar3) == 4, "OpenCL uchar3 occupies 4 bytes");
+inline float3 convert_float3(uchar3 a) { return make_float3((float)a.x, (float)a.y, (float)a.z); }
+inline float2 fabs(float2 a) { return make_float2(::fabsf(a.x), ::fabsf(a.y)); }
+// log2 correctly rounded (the convention pinned for the library and the
+// oracle): the double result rounded once to float
+inline float log2(float x) { return (float)::log2((double)x); }
+// pown(x, n) = x^n for integer n, by repeated squaring of |n| then, for
+// negative n, the reciprocal (OpenCL leaves its rounding to the device)
+inline float pown(float x, int n) {
+  unsigned k = n < 0 ? 0u - (unsigned)n : (unsigned)n;
+  float r = 1.0f, b = x;
+  while (k) {
+    if (k & 1u) r *= b;
+    b *= b;
+    k >>= 1;
+  }
+  return n < 0 ? 1.0f / r : r;
+}
+
 }  // namespace cl_shim

@@ -137,3 +137,44 @@ def test_multi_material_equals_reference_kernels_live(seed, pos):
     assert np.array_equal(r, fr.ro) and np.array_equal(g, fr.go) and np.array_equal(b, fr.bo)
     terrain = (fr.tri_id >= 0) & (fr.tri_id < sc.groups[0].ntris)
     assert terrain.sum() > 1000 or pos == (12, 4, 6)
+
+
+def _mip_pin_scenes():
+    """Scenes of trilinear materials only (no alpha, no shadow lookup):
+    kat's level-selection cases, and seeded terrain + spheres with mipBias
+    0, 0.7 and -0.4."""
+    import kat
+    out = [kat.mip_scene()[:2]]
+    for seed, bias in ((3, 0.0), (8, 0.7), (12, -0.4)):
+        sc = S.scene_small(seed=seed, flags=S.MIP, with_alpha=False)
+        for g in sc.groups:
+            g.mip_bias = bias
+        out.append((sc, S.default_view(160, 120, pos=(2, 6, -14))))
+    return out
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference checkout)")
+@pytest.mark.parametrize("i", range(4))
+def test_trilinear_core_equals_reference_mip_material(i):
+    """The oracle's trilinear colour against the reference's own code: its
+    normal-mapped mip material (Shaders_src/av_draw_normmap_mip.c, expanded
+    by the reference's AVSL generator, tiled and small kernels) drawn with a
+    zero light intensity, where its colour is exactly the trilinear texel
+    (level selection :26-59, both bilinear taps and the blend :73-123) times
+    the interpolated vertex light -- the composed material's colour with the
+    same zero intensity.  Depth and all three u16 planes bit for bit."""
+    sc, view = _mip_pin_scenes()[i]
+    sc.lint = np.zeros(3, np.float32)
+    fr = O.Frame(view.w, view.h)
+    O.clear_depth(fr.db)
+    O.draw_all(sc, view, fr)
+    rd = O.RefDraw(sc, view)
+    rd.set_mip_kernels(True)
+    rd.clear_zbuffer()
+    assert rd.draw_all() == 0
+    r, g, b, db = rd.get_frame()
+    assert (db < 65535).sum() > 500, "the scene covers the frame"
+    assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32)), "depth differs"
+    for n, a, o in (("r", r, fr.ro), ("g", g, fr.go), ("b", b, fr.bo)):
+        d = int((a != o).sum())
+        assert d == 0, f"{n}: {d} px differ (max {int(np.abs(a.astype(int) - o).max())})"
