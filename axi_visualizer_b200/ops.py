@@ -58,6 +58,7 @@ class CLDraw:
         self.gSize = []           # vertex counts per group (reference name)
         self.texSize = []
         self._mip_bias = []       # mipBias per group, as the library holds it
+        self._set_bias = []       # mipBias per group given by setMipBias (0 until set)
         self._tex_alpha = 0
         self.SHADOWMAP = {}
         self.ambLight = np.float32(0.2)
@@ -114,15 +115,23 @@ class CLDraw:
         self.gSize.append(np.int32(p.shape[0]))
         self.texSize.append(np.int32(np.log2(mip)) if mip else np.int32(int(round(rr.size ** 0.5))))
         self._mip_bias.append(np.float32(0.0))
+        self._set_bias.append(np.float32(0.0))
         return out.value
 
+    def _apply_mip_bias(self, tn, b):
+        if b != self._mip_bias[tn]:
+            check(self._L.axr_set_mip_bias(self._h, int(tn), C.c_float(b)), "setMipBias")
+            self._mip_bias[tn] = b
+
     def setMipBias(self, tn, bias):
-        """Sets group tn's mipBias (av_draw_normmap_mip.c:43), kept for every
-        later drawAll and batch render.  New: the reference passes it per
-        draw as a dict material's "mip" value, which drawAll also accepts."""
+        """Sets group tn's mipBias (av_draw_normmap_mip.c:43) for the later
+        drawAll calls and batch renders whose material for the group carries
+        none (new: the reference passes a bias per draw only in its
+        normal-mapped mip material, a dict with "normal" and "mip", Ops.py:687,
+        797-799; drawAll takes it from such a dict for that draw)."""
         b = np.float32(bias)
-        check(self._L.axr_set_mip_bias(self._h, int(tn), C.c_float(b)), "setMipBias")
-        self._mip_bias[int(tn)] = b
+        self._set_bias[int(tn)] = b
+        self._apply_mip_bias(int(tn), b)
 
     def setVertLight(self, tn, li):
         """Uploads the per-vertex light `I` of group tn (what vertLight computes)."""
@@ -247,16 +256,24 @@ class CLDraw:
 
     @staticmethod
     def _dict_mip_biases(shaders, n):
-        """{group: mipBias} for the dict materials that carry a "mip" value:
-        the reference reads it as np.float32(material["mip"]) (Ops.py:687)."""
+        """{group: mipBias} for the dict materials that carry one: the
+        reference reads np.float32(material["mip"]) only for its normal-mapped
+        mip material, a dict holding both "normal" and "mip" (Ops.py:687,
+        797-799); elsewhere "mip" is a flag."""
         items = shaders.items() if isinstance(shaders, dict) else enumerate(shaders)
-        return {int(i): np.float32(s["mip"]) for i, s in items if isinstance(s, dict) and "mip" in s and int(i) < n}
+        return {int(i): np.float32(s["mip"]) for i, s in items
+                if isinstance(s, dict) and "mip" in s and "normal" in s and int(i) < n}
+
+    def _draw_mip_biases(self, shaders):
+        """Sets every group's mipBias for one draw: its material's, where the
+        material carries one, else the setMipBias value (0 until set)."""
+        per_draw = self._dict_mip_biases(shaders, len(self.gSize))
+        for i in range(len(self.gSize)):
+            self._apply_mip_bias(i, per_draw.get(i, self._set_bias[i]))
 
     def drawAll(self, shaders, mask=None, shadowIds=(0, 1), useOpacitySM=False):
         flags, aidx = self._material_args(shaders)
-        for i, b in self._dict_mip_biases(shaders, len(self.gSize)).items():
-            if b != self._mip_bias[i]:
-                self.setMipBias(i, b)
+        self._draw_mip_biases(shaders)
         m = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
         ids = [int(i) for i in shadowIds if int(i) in self.SHADOWMAP][:2]
         sid = np.asarray(ids + [0, 0], np.int32)[:2]
@@ -418,6 +435,23 @@ class CLDraw:
         check(self._L.axr_launch_count(self._h, C.byref(v)), "launchCount")
         return v.value
 
+    def setShadowMode(self, mode, slice=0):
+        """0 (default): one work item per caster row chunk; 2 / 1: the tiled
+        shadow pass (maps up to 8192 a side), each tile's units front first /
+        as binned.  slice: a tile's units per block (0 keeps it).  The maps
+        are the same in every mode."""
+        check(self._L.axr_set_shadow_mode(self._h, int(mode), int(slice)), "setShadowMode")
+
+    def shadowOverflows(self):
+        """Per shadow map (in index order): (tiled passes whose unit queue
+        overflowed, units the last pass needed, queue capacity)."""
+        out = []
+        for i in sorted(self.SHADOWMAP):
+            v = [C.c_int64() for _ in range(3)]
+            check(self._L.axr_shadow_stats(self._h, int(i), *[C.byref(x) for x in v]), "shadowStats")
+            out.append(tuple(x.value for x in v))
+        return out
+
     def setKernelTiming(self, on=True):
         check(self._L.axr_set_kernel_timing(self._h, 1 if on else 0), "setKernelTiming")
 
@@ -477,9 +511,8 @@ class SceneRenderer:
         for k, g in enumerate(scene.groups):
             if g.mip_bias:
                 self.draw.setMipBias(k, g.mip_bias)
-        # a dict material's "mip" value is its mipBias (Ops.py:687)
-        self.shaders = [{"alpha": g.alpha_index, **{k: (np.float32(g.mip_bias) if k == "mip" else 1)
-                                                     for k, b in names if g.flags & b}} if g.flags & 2 else
+        # the mipBias goes through setMipBias; a dict's "mip" is a flag
+        self.shaders = [{"alpha": g.alpha_index, **{k: 1 for k, b in names if g.flags & b}} if g.flags & 2 else
                         " ".join(k for k, b in names if g.flags & b)
                         for g in scene.groups]
 

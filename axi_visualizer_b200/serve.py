@@ -363,10 +363,10 @@ class Server:
 
 def _shader(g, alpha_base):
     """CLDraw shader description of a scenes.Group (alpha index made global;
-    a dict material's "mip" value is its mipBias, Ops.py:687)."""
+    the group's mipBias is set with setMipBias, a dict's "mip" is a flag)."""
     names = [k for k, b in (("mip", 1), ("shadow", 4), ("cull", 8)) if g.flags & b]
     if g.flags & 2:
-        return {"alpha": alpha_base + g.alpha_index, **{k: (np.float32(g.mip_bias) if k == "mip" else 1) for k in names}}
+        return {"alpha": alpha_base + g.alpha_index, **{k: 1 for k in names}}
     return " ".join(names)
 
 

@@ -59,11 +59,13 @@ def test_cldraw_material_args_without_gpu():
         CLDraw._material_args(Fake(), ["mip"])
 
 
-def test_dict_material_mip_value_is_the_mip_bias():
-    """drawAll reads a dict material's "mip" value as the group's mipBias,
-    as the reference does (np.float32(material["mip"]), Ops.py:687), and
-    tells the library only when a group's bias changes; string materials
-    leave the bias as it is."""
+def test_mip_bias_per_draw_as_the_reference_passes_it():
+    """A group's mipBias for one drawAll: np.float32(material["mip"]) when
+    its material is the normal-mapped mip dict ("normal" and "mip",
+    Ops.py:687, 797-799), else the setMipBias value (0 until set).  In other
+    materials "mip" is only a flag, so {"alpha": a, "mip": 1} renders at bias
+    0, and a string material after a dict one does not keep the dict's bias.
+    The library is told only when a group's bias changes."""
     from axi_visualizer_b200.ops import CLDraw
     calls = []
 
@@ -81,22 +83,32 @@ def test_dict_material_mip_value_is_the_mip_bias():
         SHADOWMAP = {}
         _h = None
         _L = FakeLib()
-        _mip_bias = [np.float32(0)] * 4
         _material_args = CLDraw._material_args
         _dict_mip_biases = staticmethod(CLDraw._dict_mip_biases)
+        _draw_mip_biases = CLDraw._draw_mip_biases
+        _apply_mip_bias = CLDraw._apply_mip_bias
         setMipBias = CLDraw.setMipBias
 
     f = Fake()
-    shaders = ["mip shadow", {"alpha": 0, "mip": 0.5}, {"alpha": 1, "mip": True}, {"alpha": 0}]
+    f._mip_bias = [np.float32(0)] * 4
+    f._set_bias = [np.float32(0)] * 4
+    shaders = ["mip shadow", {"alpha": 0, "mip": 1}, {"normal": (0, 1.0), "roughness": 0, "mip": 0.5},
+               {"alpha": 0}]
     CLDraw.drawAll(f, shaders, shadowIds=[])
-    assert calls == [("bias", 1, 0.5), ("bias", 2, 1.0), ("draw",)]
-    assert [float(b) for b in f._mip_bias] == [0.0, 0.5, 1.0, 0.0]
+    assert calls == [("bias", 2, 0.5), ("draw",)]
     calls.clear()
     CLDraw.drawAll(f, shaders, shadowIds=[])          # unchanged: no library call
     assert calls == [("draw",)]
     calls.clear()
-    CLDraw.drawAll(f, {1: {"alpha": 0, "mip": 0.0}, 0: "mip"}, shadowIds=[])
-    assert calls == [("bias", 1, 0.0), ("draw",)]
+    CLDraw.drawAll(f, ["mip", "mip", "mip", "mip"], shadowIds=[])   # per draw: the dict's bias is gone
+    assert calls == [("bias", 2, 0.0), ("draw",)]
+    calls.clear()
+    CLDraw.setMipBias(f, 1, 2.0)
+    assert calls == [("bias", 1, 2.0)]
+    calls.clear()
+    CLDraw.drawAll(f, ["mip", {"alpha": 0, "mip": 1}, "mip", "mip"], shadowIds=[])   # the set value holds
+    assert calls == [("draw",)]
+    assert [float(b) for b in f._mip_bias] == [0.0, 2.0, 0.0, 0.0]
 
 
 def test_scene_renderer_hands_every_group_field_to_the_draw(monkeypatch):
@@ -136,12 +148,13 @@ def test_scene_renderer_hands_every_group_field_to_the_draw(monkeypatch):
     assert [n for n, a, k in log].count("addTexAlpha") == 1
     assert [a[:2] for n, a, k in log if n == "addShadowMap"] == [(0, 64)]
     assert [a[0] for n, a, k in log if n == "placeShadowMapBasis"] == [0]
-    # materials: flags and alpha index as the oracle reads them, mipBias in the dict form
+    # materials: flags and alpha index as the oracle reads them; the mipBias
+    # goes through setMipBias only (no dict bias)
     fake = type("F", (), {"gSize": [3] * len(sc.groups)})()
     flags, aidx = real._material_args(fake, R.shaders)
     assert flags.tolist() == [g.flags for g in sc.groups]
     assert aidx.tolist() == [g.alpha_index for g in sc.groups]
-    assert real._dict_mip_biases(R.shaders, len(sc.groups)) == {1: np.float32(sc.groups[1].mip_bias)}
+    assert real._dict_mip_biases(R.shaders, len(sc.groups)) == {}
 
 
 # every method of the reference's CLDraw (PyOpenCL27C/Ops.py:127-1230)
