@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libaxr.so")
 SOURCES = [os.path.join(CSRC, "axr.cu")]
-DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("raster.cuh", "kernels.cuh", "batch.cuh")] + [
+DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("raster.cuh", "kernels.cuh", "batch.cuh", "shadow_tiles.cuh")] + [
     os.path.join(HERE, "..", "include", "axr.h")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

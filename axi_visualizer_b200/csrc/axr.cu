@@ -22,6 +22,7 @@
 
 #include "../../include/axr.h"
 #include "batch.cuh"
+#include "shadow_tiles.cuh"
 
 using namespace axr;
 
@@ -72,8 +73,23 @@ struct Shadow {
   cudaStream_t st = nullptr;
   cudaEvent_t ev_write = nullptr, ev_read = nullptr;
   uint32_t *list = nullptr, *ctr = nullptr, *items = nullptr;
-  uint32_t cap = 0;
+  uint32_t cap = 0;          // casters the list (and the records) hold
+  bool items_ready = false;  // row-chunk items allocated (per-caster path)
   GroupDev *tab = nullptr;
+  // tiled pass: caster records, tile offsets/cursors/order, units; the
+  // per-tile counts sit right after the CTR_N counters (one clear for both)
+  uint4 *rec = nullptr;
+  uint32_t *tiles = nullptr, *units = nullptr;
+  uint32_t cap_units = 0;
+  int ntx = 0;
+  int64_t overflows = 0;      // tiled passes that overflowed the unit queue
+  uint32_t last_units = 0;    // units the last checked tiled pass needed
+  // counters of the last two passes (pinned, each with its event), checked
+  // once their pass has finished
+  uint32_t *h_ring = nullptr;
+  cudaEvent_t ev_ctr[2] = {nullptr, nullptr};
+  bool pend[2] = {false, false};
+  int last_slot = 1;
 };
 
 constexpr int MAX_GROUPS = 64;
@@ -147,6 +163,9 @@ struct axr_ctx {
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
   int min_chunk = MIN_CHUNK;
+  int shadow_mode = 0;                       // 0: per caster; tiled shadow pass where the map allows it
+                                             // (2: units front first, 1: as binned)
+  int shadow_slice = 512;                    // units per block of a tile in the tiled pass
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
   struct Pending { const char *name; cudaEvent_t a, b; };
@@ -221,11 +240,62 @@ int check_slot(axr_ctx *c, int k, bool blocking) {
   return 0;
 }
 
-// Checks every drawAll whose frame has finished, oldest first (no waiting).
+int grow_shadow_units(Shadow &sm, uint32_t need) {
+  if (need <= sm.cap_units) return 0;
+  uint64_t cap = std::max<uint64_t>((uint64_t)need + need / 4, (uint64_t)sm.cap_units * 2);
+  if (cap > 0x7fffffffull) cap = 0x7fffffffull;
+  cudaFree(sm.units);
+  sm.units = nullptr;
+  sm.cap_units = 0;
+  if (cudaMalloc(&sm.units, sizeof(uint32_t) * cap) != cudaSuccess)
+    return fail(AXR_ENOMEM, "shadow tile-unit queue of %llu entries", (unsigned long long)cap);
+  sm.cap_units = (uint32_t)cap;
+  return 0;
+}
+
+// Checks the counters of shadow pass slot k of map sm, as check_slot does
+// for drawAll: a raster loop at its safety limit is an error; an overflowed
+// unit queue (that pass was drawn by the per-caster path) grows.
+int check_shadow_slot(Shadow &sm, int k, bool blocking) {
+  if (!sm.pend[k]) return 0;
+  if (blocking) {
+    CK(cudaEventSynchronize(sm.ev_ctr[k]));
+  } else {
+    cudaError_t e = cudaEventQuery(sm.ev_ctr[k]);
+    if (e == cudaErrorNotReady) return 0;
+    if (e != cudaSuccess) return fail(AXR_ECUDA, "shadowMap: %s", cudaGetErrorString(e));
+  }
+  sm.pend[k] = false;
+  const uint32_t *h = sm.h_ring + k * CTR_N;
+  if (h[CTR_LIMIT]) return fail(AXR_ECUDA, "a shadow raster loop reached its safety limit; the map is incomplete");
+  sm.last_units = h[CTR_SH_UNITS_NEED];
+  if (h[CTR_SH_OVERFLOW]) sm.overflows++;
+  if (h[CTR_SH_OVERFLOW] && h[CTR_SH_UNITS_NEED] > sm.cap_units) {
+    CK(cudaStreamSynchronize(sm.st));   // passes in flight still use the old queue
+    return grow_shadow_units(sm, h[CTR_SH_UNITS_NEED]);
+  }
+  return 0;
+}
+
+// Checks the shadow passes of every map, oldest first; without blocking,
+// unfinished passes are left for a later check.
+int settle_shadows(axr_ctx *c, bool blocking) {
+  for (auto &sm : c->shadows) {
+    if (!sm.h_ring) continue;
+    int older = 1 - sm.last_slot;
+    int rc = check_shadow_slot(sm, older, blocking);
+    if (!rc && !sm.pend[older]) rc = check_shadow_slot(sm, sm.last_slot, blocking);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+// Checks every drawAll and shadow pass that has finished, oldest first (no waiting).
 int settle_ready(axr_ctx *c) {
   int older = 1 - c->last_slot;
   int rc = check_slot(c, older, false);
   if (!rc && !c->pend[older]) rc = check_slot(c, c->last_slot, false);
+  if (!rc) rc = settle_shadows(c, false);
   return rc;
 }
 
@@ -246,6 +316,7 @@ int settle(axr_ctx *c) {
   }
   int rc = check_slot(c, 1 - c->last_slot, true);
   if (!rc) rc = check_slot(c, c->last_slot, true);
+  if (!rc) rc = settle_shadows(c, true);
   return rc;
 }
 
@@ -492,6 +563,10 @@ int axr_destroy(axr_ctx *c) {
     if (sm.ev_write) cudaEventDestroy(sm.ev_write);
     if (sm.ev_read) cudaEventDestroy(sm.ev_read);
     cudaFree(sm.map); cudaFree(sm.list); cudaFree(sm.items); cudaFree(sm.ctr); cudaFree(sm.tab);
+    cudaFree(sm.rec); cudaFree(sm.tiles); cudaFree(sm.units);
+    if (sm.h_ring) cudaFreeHost(sm.h_ring);
+    for (auto e : sm.ev_ctr)
+      if (e) cudaEventDestroy(e);
   }
   if (c->s_alpha) { cudaStreamSynchronize(c->s_alpha); cudaStreamDestroy(c->s_alpha); }
   if (c->ev_setup) cudaEventDestroy(c->ev_setup);
@@ -1123,14 +1198,30 @@ int axr_add_shadow_map(axr_ctx *c, int i, int size, float scale, float amb) {
     if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s.ev_write, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s.ev_read, cudaEventDisableTiming) != cudaSuccess ||
-        cudaMalloc(&s.ctr, sizeof(uint32_t) * CTR_N) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s.ev_ctr[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s.ev_ctr[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost(&s.h_ring, sizeof(uint32_t) * 2 * CTR_N) != cudaSuccess ||
         cudaMalloc(&s.tab, sizeof(GroupDev) * MAX_GROUPS) != cudaSuccess)
       return fail(AXR_ENOMEM, "shadow map %d state", i);
   }
-  if (s.map && s.dim != size) { CK(cudaStreamSynchronize(s.st)); cudaFree(s.map); s.map = nullptr; }
+  if (s.map && s.dim != size) {
+    CK(cudaStreamSynchronize(s.st));
+    if ((rc = settle_shadows(c, true))) return rc;
+    cudaFree(s.map); cudaFree(s.ctr); cudaFree(s.tiles);
+    s.map = nullptr; s.ctr = s.tiles = nullptr;
+  }
   CK(cudaStreamWaitEvent(s.st, s.ev_read, 0));
-  if (!s.map && cudaMalloc(&s.map, sizeof(float) * (size_t)size * size) != cudaSuccess)
-    return fail(AXR_ENOMEM, "shadow map %dx%d", size, size);
+  if (!s.map) {
+    // counters, then the per-tile unit counts and claim counters of the
+    // tiled pass (opaque, alpha); tile offsets, cursors (2 per tile), order
+    // and the prefix of blocks per tile
+    s.ntx = (size + STILE - 1) / STILE;
+    size_t nt = (size_t)s.ntx * s.ntx;
+    if (cudaMalloc(&s.map, sizeof(float) * (size_t)size * size) != cudaSuccess ||
+        cudaMalloc(&s.ctr, sizeof(uint32_t) * (CTR_N + 4 * nt)) != cudaSuccess ||
+        cudaMalloc(&s.tiles, sizeof(uint32_t) * (5 * nt + 1)) != cudaSuccess)
+      return fail(AXR_ENOMEM, "shadow map %dx%d", size, size);
+  }
   s.dim = size;
   s.scale = scale;
   // a fresh map holds 65535 (Ops.py:1049)
@@ -1189,16 +1280,33 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
     }
   }
   Shadow &sm = c->shadows[i];
+  const bool tiled = c->shadow_mode >= 1 && sm.dim <= SHADOW_TILED_MAX_DIM;
   if (sm.cap < c->cap_list) {
     CK(cudaStreamSynchronize(sm.st));
-    cudaFree(sm.list);
-    cudaFree(sm.items);
+    cudaFree(sm.list); cudaFree(sm.items); cudaFree(sm.rec);
     sm.list = sm.items = nullptr;
+    sm.rec = nullptr;
+    sm.items_ready = false;
     sm.cap = 0;
-    if (cudaMalloc(&sm.list, sizeof(uint32_t) * c->cap_list) != cudaSuccess ||
-        cudaMalloc(&sm.items, sizeof(uint32_t) * c->cap_list * MAX_CHUNKS) != cudaSuccess)
+    if (cudaMalloc(&sm.list, sizeof(uint32_t) * c->cap_list) != cudaSuccess)
       return fail(AXR_ENOMEM, "caster list of shadow map %d", i);
     sm.cap = c->cap_list;
+  }
+  if (tiled && !sm.rec) {
+    if (cudaMalloc(&sm.rec, 2 * sizeof(uint4) * sm.cap) != cudaSuccess)
+      return fail(AXR_ENOMEM, "caster records of shadow map %d", i);
+    // initial tile-unit queue (grows after an overflow); AXR_SHADOW_UNIT_QUEUE overrides
+    uint32_t units0 = sm.cap + sm.cap / 2 + 1024;
+    if (const char *e = getenv("AXR_SHADOW_UNIT_QUEUE")) {
+      long v = atol(e);
+      if (v >= 1 && v <= (1L << 30)) units0 = (uint32_t)v;
+    }
+    if ((rc = grow_shadow_units(sm, units0))) return rc;
+  }
+  if (!tiled && !sm.items_ready) {
+    if (cudaMalloc(&sm.items, sizeof(uint32_t) * sm.cap * MAX_CHUNKS) != cudaSuccess)
+      return fail(AXR_ENOMEM, "row chunks of shadow map %d", i);
+    sm.items_ready = true;
   }
   CK(cudaStreamWaitEvent(sm.st, sm.ev_read, 0));
   CK(cudaStreamWaitEvent(sm.st, c->ev_geo, 0));   // rotate / translate / copyTo queued before
@@ -1210,21 +1318,60 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   memcpy(S.sh.pos, sm.pos, sizeof sm.pos);
   memcpy(S.sh.vv, sm.vv, sizeof sm.vv);
   S.map = sm.map; S.bias = bias; S.list = sm.list; S.cap_list = sm.cap; S.ctr = sm.ctr;
-  S.items = sm.items; S.min_chunk = c->min_chunk;
+  S.min_chunk = c->min_chunk;
+  const size_t nt = (size_t)sm.ntx * sm.ntx;
+  if (tiled) {
+    S.rec = sm.rec;
+    S.tcnt = sm.ctr + CTR_N; S.tclaim = sm.ctr + CTR_N + 2 * nt;
+    S.toff = sm.tiles; S.tcur = sm.tiles + nt; S.tord = sm.tiles + 3 * nt; S.hpre = sm.tiles + 4 * nt;
+    S.units = sm.units; S.cap_units = sm.cap_units;
+    S.ntx = sm.ntx; S.ntiles = (int)nt;
+    S.slice = c->shadow_slice; S.sort = c->shadow_mode == 2;
+  } else {
+    S.items = sm.items;
+  }
   if (c->total_tris == 0) return 0;
   bool any_alpha = false;
   for (int g = 0; g < ngroups; g++)
     if (cast[g] && (tab[g].flags & F_ALPHA)) any_alpha = true;
   static_assert(CTR_SH_LIST_A == CTR_SH_LIST + 1 && CTR_SH_WORK == CTR_SH_LIST + 2 && CTR_SH_WORK_A == CTR_SH_LIST + 3,
                 "shadow counters are contiguous");
-  CK(cudaMemsetAsync(sm.ctr, 0, sizeof(uint32_t) * CTR_N, sm.st));
+  CK(cudaMemsetAsync(sm.ctr, 0, sizeof(uint32_t) * (CTR_N + (tiled ? 4 * nt : 0)), sm.st));
   cudaStream_t st = sm.st;
   launch(c, st, "k_shadow_setup", [&] { k_shadow_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, st>>>(S); });
-  launch(c, st, "k_shadow_raster", [&] { k_shadow_raster<false><<<c->sms * 8, 128, 0, st>>>(S); });
-  if (any_alpha)
-    launch(c, st, "k_shadow_raster_alpha", [&] { k_shadow_raster<true><<<c->sms * 6, 128, 0, st>>>(S); });
+  if (tiled) {
+    launch(c, st, "k_shadow_scan", [&] { k_shadow_scan<<<1, SCAN_THREADS, 0, st>>>(S); });
+    launch(c, st, "k_shadow_bin", [&] { k_shadow_bin<<<c->sms * 8, 256, 0, st>>>(S); });
+    if (S.sort) launch(c, st, "k_shadow_sort", [&] { k_shadow_sort<<<c->sms * 4, 256, 0, st>>>(S); });
+    launch(c, st, "k_shadow_tiles", [&] { k_shadow_tiles<false><<<c->sms * 8, 128, 0, st>>>(S); });
+    if (any_alpha)
+      launch(c, st, "k_shadow_tiles_alpha", [&] { k_shadow_tiles<true><<<c->sms * 6, 128, 0, st>>>(S); });
+  } else {
+    launch(c, st, "k_shadow_raster", [&] { k_shadow_raster<false><<<c->sms * 8, 128, 0, st>>>(S); });
+    if (any_alpha)
+      launch(c, st, "k_shadow_raster_alpha", [&] { k_shadow_raster<true><<<c->sms * 6, 128, 0, st>>>(S); });
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(sm.ev_write, st));
+  // the pass's counters to the ring (the slot before last is checked first)
+  int slot = 1 - sm.last_slot;
+  if (sm.pend[slot] && (rc = check_shadow_slot(sm, slot, true))) return rc;
+  CK(cudaMemcpyAsync(sm.h_ring + slot * CTR_N, sm.ctr, sizeof(uint32_t) * CTR_N, cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(sm.ev_ctr[slot], st));
+  sm.pend[slot] = true;
+  sm.last_slot = slot;
+  return 0;
+}
+
+int axr_shadow_stats(axr_ctx *c, int i, int64_t *overflows, int64_t *units, int64_t *cap_units) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
+  if ((rc = settle(c))) return rc;
+  const Shadow &s = c->shadows[i];
+  if (overflows) *overflows = s.overflows;
+  if (units) *units = s.last_units;
+  if (cap_units) *cap_units = s.cap_units;
   return 0;
 }
 
@@ -1878,6 +2025,16 @@ int axr_batch_inject_barrier_stall(axr_batch *b, int phantom_blocks, long long s
   return 0;
 }
 
+int axr_set_shadow_mode(axr_ctx *c, int mode, int slice) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  if (mode < 0 || mode > 2) return fail(AXR_EINVAL, "shadow mode %d outside [0, 2]", mode);
+  if (slice != 0 && (slice < 32 || slice > (1 << 20)))
+    return fail(AXR_EINVAL, "shadow slice %d outside [32, 2^20] (0 keeps it)", slice);
+  c->shadow_mode = mode;
+  if (slice) c->shadow_slice = slice;
+  return 0;
+}
+
 int axr_set_tuning(axr_ctx *c, int min_chunk) {
   if (!c) return fail(AXR_EINVAL, "null handle");
   if (min_chunk < 1 || min_chunk > 256) return fail(AXR_EINVAL, "chunk rows %d outside [1, 256]", min_chunk);
@@ -1948,8 +2105,9 @@ __global__ void __launch_bounds__(256) k_shadow_setup_noalloc(GroupDev G, Shadow
   for (int base = blockIdx.x * blockDim.x; base < S.total_tris; base += gridDim.x * blockDim.x) {
     int t = base + threadIdx.x;
     bool ok, alpha;
-    int rows;
-    shadow_classify(sg, S, t, ok, alpha, rows);
+    int rows, g, ix[3], iy[3];
+    float z[3];
+    shadow_classify(sg, S, t, ok, alpha, rows, g, ix, iy, z);
     shadow_append(S, t, ok, alpha, rows, lane);   // S.items is null: no row chunks
   }
 }

@@ -49,7 +49,11 @@ struct DrawParams {
 enum {
   CTR_SMALL = 0, CTR_SMALL_A, CTR_LARGE, CTR_UNITS, CTR_UNITS_A, CTR_WORK_SMALL, CTR_WORK_SMALL_A, CTR_WORK_LARGE,
   CTR_WORK_UNITS, CTR_WORK_UNITS_A, CTR_OVERFLOW, CTR_SH_LIST, CTR_SH_LIST_A, CTR_SH_WORK, CTR_SH_WORK_A,
-  CTR_UNITS_RESERVED, CTR_LIMIT, CTR_ITEMS, CTR_ITEMS_A, CTR_SH_ITEMS, CTR_SH_ITEMS_A, CTR_N = 32
+  CTR_UNITS_RESERVED, CTR_LIMIT, CTR_ITEMS, CTR_ITEMS_A, CTR_SH_ITEMS, CTR_SH_ITEMS_A,
+  // tiled shadow pass: unit queue overflowed (the per-caster path drew the
+  // map), units the map needed, non-empty tiles, tiles claimed (opaque, alpha)
+  CTR_SH_OVERFLOW, CTR_SH_UNITS_NEED, CTR_SH_TILES, CTR_SH_TILE_WORK, CTR_SH_TILE_WORK_A, CTR_SH_ITEMS_TILED,
+  CTR_N = 32
 };
 
 // Every data-dependent loop is bounded by construction (rows of a small
@@ -1609,19 +1613,30 @@ struct ShadowParams {
   uint32_t *items;     // row chunks of the casters, same two ends (cap_list * MAX_CHUNKS);
                        // null: one work item per caster
   int min_chunk;       // rows per chunk (at least)
+  // tiled pass (rec != null): one record per caster at its list position,
+  // per-tile unit counts (opaque [0, ntiles), alpha [ntiles, 2 ntiles)),
+  // offsets, scatter cursors and claim counters (opaque, alpha per tile),
+  // the non-empty tiles in order with the prefix of their block counts, units
+  uint4 *rec;          // 2 per caster: sorted vertices, z, triangle, vertex order
+  uint32_t *tcnt, *toff, *tcur, *tclaim, *tord, *hpre, *units;
+  uint32_t cap_units;
+  int ntx, ntiles;     // tiles per side, tiles
+  int slice;           // units per block of a tile: a tile with n units gets ceil(n / slice) blocks
+  int sort;            // 1: each tile's units front (nearest the light) first
 };
 
-// rows = the caster's row count in the map (drawmin.c: y1..y2 up, y3..y2+1 down)
+// rows = the caster's row count in the map (drawmin.c: y1..y2 up, y3..y2+1 down);
+// g, ix, iy, z = its group and projected vertices (trisetupOrtho.c)
 __device__ __forceinline__ void shadow_classify(const GroupDev *sg, const ShadowParams &S, int t, bool &ok, bool &alpha,
-                                                int &rows) {
+                                                int &rows, int &g, int ix[3], int iy[3], float z[3]) {
   ok = false;
   alpha = false;
   rows = 0;
+  g = 0;
   if (t < S.total_tris) {
-    const GroupDev &G = sg[find_group(sg, S.ngroups, (uint32_t)t)];
+    g = find_group(sg, S.ngroups, (uint32_t)t);
+    const GroupDev &G = sg[g];
     if (G.enabled) {
-      int ix[3], iy[3];
-      float z[3];
       ok = project_ortho(G, t - G.tri_base, S.sh, S.bias, ix, iy, z);
       alpha = (G.flags & F_ALPHA) != 0;
       rows = max(iy[0], max(iy[1], iy[2])) - min(iy[0], min(iy[1], iy[2])) + 1;
@@ -1629,7 +1644,11 @@ __device__ __forceinline__ void shadow_classify(const GroupDev *sg, const Shadow
   }
 }
 
-__device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int rows, int lane) {
+// Appends the casters of a warp to the list (opaque from the front,
+// alpha-tested from the back) and their row chunks to the work items;
+// returns the caster's list slot.
+__device__ __forceinline__ uint32_t shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int rows,
+                                                  int lane) {
   unsigned mo = __ballot_sync(FULL, ok && !alpha), ma = __ballot_sync(FULL, ok && alpha);
   uint32_t bo = 0, ba = 0;
   if (lane == 0) {
@@ -1642,7 +1661,8 @@ __device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool
   uint32_t pos = 0;
   if (ok && !alpha) { pos = bo + __popc(mo & lt); S.list[pos] = (uint32_t)t; }
   if (ok && alpha) { pos = ba + __popc(ma & lt); S.list[S.cap_list - 1 - pos] = (uint32_t)t; }
-  if (!S.items) return;
+  uint32_t slot = alpha ? S.cap_list - 1 - pos : pos;
+  if (!S.items) return slot;
   // row chunks of the casters, as for the small triangles of the view
   int nch = 0;
   if (ok) {
@@ -1670,6 +1690,73 @@ __device__ __forceinline__ void shadow_append(const ShadowParams &S, int t, bool
     if (!alpha) S.items[oo + c] = item;
     else S.items[cap_items - 1 - (oa + c)] = item;
   }
+  return slot;
+}
+
+// ---- tiled shadow pass: caster records and tile binning
+
+constexpr int STILE_LOG = 5;
+constexpr int STILE = 1 << STILE_LOG;   // a map tile is STILE x STILE texels
+constexpr int TROW = STILE + 1;         // row stride of a tile in shared memory (rows in different banks)
+constexpr int SUB_LOG = 3;              // the tile's texel maxima are kept per 8 x 8 sub-block
+constexpr int SUBS = STILE >> SUB_LOG;  // sub-blocks per tile side
+
+// drawmin.c's vertex order: sorted by y with its three compare-and-swaps;
+// perm packs which of the triangle's vertices became vertex k (2 bits each)
+__device__ __forceinline__ int caster_sort(int ix[3], int iy[3], float z[3]) {
+  int p0 = 0, p1 = 1, p2 = 2;
+  if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(p0, p1); }
+  if (iy[1] > iy[2]) { swap_(iy[1], iy[2]); swap_(ix[1], ix[2]); swap_(z[1], z[2]); swap_(p1, p2); }
+  if (iy[0] > iy[1]) { swap_(iy[0], iy[1]); swap_(ix[0], ix[1]); swap_(z[0], z[1]); swap_(p0, p1); }
+  return p0 | (p1 << 2) | (p2 << 4);
+}
+
+__device__ __forceinline__ uint32_t pack_xy(int x, int y) { return ((uint32_t)x & 0xffffu) | ((uint32_t)y << 16); }
+__device__ __forceinline__ int unpack_x(uint32_t w) { return (int)(int16_t)(w & 0xffffu); }
+__device__ __forceinline__ int unpack_y(uint32_t w) { return (int)w >> 16; }
+
+// The tiles a caster (sorted vertices) can write: rows y1..y3, and columns
+// x_min..x_max widened by the drift of the accumulated edge positions (an
+// addition rounds by at most |x| 2^-24, so `rows` of them stay below
+// rows * X * 2^-23) and by one for the truncated split vertex x4; all
+// clipped to the map.  False when nothing of the caster lies on the map.
+__device__ __forceinline__ bool caster_tiles(const int x[3], int y1, int y3, int dim, int &tx0, int &tx1, int &ty0,
+                                             int &ty1) {
+  if (!(y1 < dim && y3 >= 0)) return false;
+  int mn = min(x[0], min(x[1], x[2])), mx = max(x[0], max(x[1], x[2]));
+  long long X = (long long)max(iabs_(mn), iabs_(mx)) + 2;
+  long long rows = (long long)y3 - y1 + 1;
+  int m = 1 + (int)((rows * X) >> 22);
+  int c0 = mn - m, c1 = mx + m;
+  if (c1 < 0 || c0 > dim - 1) return false;
+  c0 = max(c0, 0);
+  c1 = min(c1, dim - 1);
+  tx0 = c0 >> STILE_LOG;
+  tx1 = c1 >> STILE_LOG;
+  ty0 = max(y1, 0) >> STILE_LOG;
+  ty1 = min(y3, dim - 1) >> STILE_LOG;
+  return true;
+}
+
+// Writes caster t's record at its list slot and counts it in every tile it
+// can write (opaque counts first, alpha-tested after them).
+__device__ __forceinline__ void shadow_record(const ShadowParams &S, int t, int g, bool alpha, int ix[3], int iy[3],
+                                              float z[3], uint32_t slot) {
+  int perm = caster_sort(ix, iy, z);
+  S.rec[2 * (size_t)slot] = make_uint4(pack_xy(ix[0], iy[0]), pack_xy(ix[1], iy[1]), pack_xy(ix[2], iy[2]),
+                                       __float_as_uint(z[0]));
+  S.rec[2 * (size_t)slot + 1] = make_uint4(__float_as_uint(z[1]), __float_as_uint(z[2]), (uint32_t)t,
+                                           (uint32_t)perm | ((uint32_t)g << 8));
+  int tx0, tx1, ty0, ty1;
+  if (!caster_tiles(ix, iy[0], iy[2], S.sh.dim, tx0, tx1, ty0, ty1)) return;
+  const uint32_t base = alpha ? (uint32_t)S.ntiles : 0u;
+  for (int ty = ty0; ty <= ty1; ty++)
+    for (int tx = tx0; tx <= tx1; tx++) {
+      // lanes counting into the same tile add once (casters crowd into few tiles)
+      uint32_t key = base + (uint32_t)(ty * S.ntx + tx);
+      unsigned peers = __match_any_sync(__activemask(), key);
+      if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&S.tcnt[key], (uint32_t)__popc(peers));
+    }
 }
 
 __device__ __forceinline__ void shadow_setup_phase(const ShadowParams &S, const GroupDev *sg, int first, int step) {
@@ -1677,9 +1764,11 @@ __device__ __forceinline__ void shadow_setup_phase(const ShadowParams &S, const 
   for (int base = first; base < S.total_tris; base += step) {
     int t = base + threadIdx.x;
     bool ok, alpha;
-    int rows;
-    shadow_classify(sg, S, t, ok, alpha, rows);
-    shadow_append(S, t, ok, alpha, rows, lane);
+    int rows, g, ix[3], iy[3];
+    float z[3];
+    shadow_classify(sg, S, t, ok, alpha, rows, g, ix, iy, z);
+    uint32_t slot = shadow_append(S, t, ok, alpha, rows, lane);
+    if (S.rec && ok) shadow_record(S, t, g, alpha, ix, iy, z, slot);
   }
 }
 
@@ -1695,10 +1784,29 @@ __device__ __forceinline__ void atomic_min_depth(float *addr, float v) {
   else atomicMax((unsigned int *)addr, __float_as_uint(v));
 }
 
+// The texel test of the tiled pass.  Every pixel of a span stores
+// tz = RN(1 / v), v = RN(RN((1 - t) cz2) + RN(t cz1)), t in [0, 1]; when cz1
+// and cz2 are positive, v <= max(cz1, cz2) (1 + 2^-24)^3, so tz stays above
+// (1 / max) (1 - 2^-22).  The returned threshold is one more than the bits
+// of a float below that (an approximate reciprocal, within 2 ulp, taken
+// down by 2^-18): a texel whose bits are smaller already holds a depth no
+// pixel of the span undercuts, so its min update would change nothing.
+// Spans whose ends are not positive and within [2^-60, 2^60] get INT_MIN,
+// which no texel is below.  (A NaN end makes every pixel's depth NaN, which
+// is never stored.)
+__device__ __forceinline__ int depth_floor_bits(float cz1, float cz2) {
+  float hi = fmaxf(cz1, cz2), lo = fminf(cz1, cz2);
+  if (!(lo > 0.f) || !(hi >= 0x1p-60f) || !(hi <= 0x1p60f)) return INT_MIN;
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(hi));
+  return __float_as_int(__fmul_rn(r, 1.0f - 0x1p-18f)) + 1;
+}
+
 template <bool ALPHA>
 struct ShadowQ {
   float4 a[32];                  // cx2, d, 1/d (0: divide), cz1
-  float4 b[32];                  // cz2, texel address - first pixel number, x - first pixel number, unused
+  float4 b[32];                  // cz2, texel address - first pixel number, x - first pixel number,
+                                 // depth floor bits (tiled pass)
   float4 c[ALPHA ? 32 : 1];      // cu1, cv1, cu2, cv2
   int g[ALPHA ? 32 : 1];
   int r2l[32];
@@ -1771,6 +1879,13 @@ struct ShadowLane {
     x1 = ix[0]; x2 = ix[1]; x3 = ix[2]; y1 = iy[0]; y2 = iy[1]; y3 = iy[2];
     z1 = z[0]; z2 = z[1]; z3 = z[2];
     if (!((y1 < S.sh.dim) && (y3 >= 0))) return false;
+    finish(uv);
+    return true;
+  }
+
+  // drawmin.c:49-51 (split vertex) and the first half's slopes, from the
+  // sorted vertices
+  __device__ __forceinline__ void finish(const V2 uv[3]) {
     float q = (float)(y2 - y1) / (float)(y3 - y1);
     x4 = f2i((float)x1 + q * (float)(x3 - x1));
     z4 = z1 + q * (z3 - z1);
@@ -1781,6 +1896,43 @@ struct ShadowLane {
     }
     start_half0();
     left = y3 - y1 + 1;
+  }
+
+  // The caster of record r (the setup projected and sorted it).  Only
+  // casters with rows on the map have units.
+  __device__ __forceinline__ void init_rec(const ShadowParams &S, const GroupDev *sg, uint32_t r) {
+    uint4 a = S.rec[2 * (size_t)r], b = S.rec[2 * (size_t)r + 1];
+    x1 = unpack_x(a.x); y1 = unpack_y(a.x);
+    x2 = unpack_x(a.y); y2 = unpack_y(a.y);
+    x3 = unpack_x(a.z); y3 = unpack_y(a.z);
+    z1 = __uint_as_float(a.w); z2 = __uint_as_float(b.x); z3 = __uint_as_float(b.y);
+    g = (int)(b.w >> 8);
+    V2 uv[3] = {V2{0, 0}, V2{0, 0}, V2{0, 0}};
+    if (ALPHA) {
+      const GroupDev &G = sg[g];
+      size_t v0 = ((size_t)b.z - (size_t)G.tri_base) * 3;
+      uv[0] = mul2(ld2(G.uv + (v0 + (b.w & 3)) * 2), z1);
+      uv[1] = mul2(ld2(G.uv + (v0 + ((b.w >> 2) & 3)) * 2), z2);
+      uv[2] = mul2(ld2(G.uv + (v0 + ((b.w >> 4) & 3)) * 2), z3);
+    }
+    finish(uv);
+  }
+
+  // Restricts the walk to the rows ty0..ty1 of a tile: replays the rows
+  // before the first of them and leaves in `left` the rows up to the last
+  // (rows outside the tile in between are skipped as they come).  The walk
+  // visits bottom-half rows y1..y2 (positions 0..n0-1), then top-half rows
+  // y3 down to y2 + 1.
+  __device__ __forceinline__ bool clip_rows(int ty0, int ty1) {
+    int n0 = y2 - y1 + 1;
+    int a0 = max(y1, ty0) - y1, a1 = min(y2, ty1) - y1;
+    int blo = max(y2 + 1, ty0), bhi = min(y3, ty1);
+    bool ha = a0 <= a1, hb = blo <= bhi;
+    if (!ha && !hb) return false;
+    int first = ha ? a0 : n0 + (y3 - bhi);
+    int last = hb ? n0 + (y3 - blo) : a1;
+    for (int r = 0; r < first; r++) skip_row();
+    left = last - first + 1;
     return true;
   }
 
@@ -1834,17 +1986,58 @@ struct ShadowLane {
     live = --left > 0;
     return cnt;
   }
+
+  // emit() inside a tile: the current row lies in rows ty0..ty1; its span is
+  // clipped to columns tx0..tx1 and written with its texel offset in the
+  // tile and its depth floor.  Then advances to the next row in the tile.
+  // A span whose depth floor lies above every texel it covers (by the
+  // tile's sub-block maxima `smax`) is not queued.
+  __device__ __forceinline__ int emit_tile(ShadowQ<ALPHA> &q, int lane, int tx0, int tx1, int ty0, int ty1,
+                                           const int *smax, bool &live) {
+    int a0 = half == 0 ? f2i(cx2) : f2i(cx1);
+    int a1 = half == 0 ? f2i(cx1) : f2i(cx2);
+    int lo = max(a0, tx0), hi = min(a1, tx1);
+    int cnt = hi >= lo ? hi - lo + 1 : 0;
+    int floor_bits = 0;
+    if (cnt) {
+      floor_bits = depth_floor_bits(cz1, cz2);
+      const int *row = smax + ((cy - ty0) >> SUB_LOG) * SUBS;
+      int m = INT_MIN;
+      for (int bx = (lo - tx0) >> SUB_LOG; bx <= (hi - tx0) >> SUB_LOG; bx++) m = max(m, row[bx]);
+      if (m < floor_bits) cnt = 0;
+    }
+    if (cnt) {
+      float d = cx1 - cx2;
+      q.a[lane] = make_float4(cx2, d, span_recip_exact(d, cx2, lo), cz1);
+      q.b[lane] = make_float4(cz2, __int_as_float((cy - ty0) * TROW + (lo - tx0)), __int_as_float(lo),
+                              __int_as_float(floor_bits));
+      if (ALPHA) {
+        q.c[lane] = make_float4(cu1, cv1, cu2, cv2);
+        q.g[lane] = g;
+      }
+    }
+    skip_row();
+    --left;
+    while (left > 0 && (cy < ty0 || cy > ty1)) {
+      skip_row();
+      --left;
+    }
+    live = left > 0;
+    return cnt;
+  }
 };
 
-// drawmin.c:71-76 / drawminalpha.c:83-97 for one pixel of span s
+// drawmin.c:71-76 / drawminalpha.c:83-97 for pixel number p of span s: the
+// depth tz, or false when nothing is written (NaN depth, alpha discard)
 template <bool ALPHA>
-__device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p) {
-  const float4 a = q.a[s], b = q.b[s];
+__device__ __forceinline__ bool shadow_depth(const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p, float4 b,
+                                             float &tz) {
+  const float4 a = q.a[s];
   float n = (float)(p + __float_as_int(b.z)) - a.x;
   float t = a.z != 0.f ? quot_fast(n, a.y, a.z) : n / a.y;
   t = clamp_t(t);
-  float tz = __frcp_rn((1 - t) * b.x + t * a.w);
-  if (tz != tz) return;
+  tz = __frcp_rn((1 - t) * b.x + t * a.w);
+  if (tz != tz) return false;
   if (ALPHA) {
     const float4 c = q.c[s];
     const GroupDev &G = sg[q.g[s]];
@@ -1854,9 +2047,17 @@ __device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, con
     t1 = iabs_(t1) & (len - 1);
     int t2 = f2i((lm1 * ((1 - t) * c.w + t * c.y)) * tz);
     t2 = iabs_(t2) & (len - 1);
-    if (!__ldg(G.amask + t1 + t2 * len)) return;
+    if (!__ldg(G.amask + t1 + t2 * len)) return false;
   }
-  atomic_min_depth(map + (size_t)(p + __float_as_int(b.y)), tz);
+  return true;
+}
+
+// drawmin.c:71-76 / drawminalpha.c:83-97 for one pixel of span s
+template <bool ALPHA>
+__device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p) {
+  const float4 b = q.b[s];
+  float tz;
+  if (shadow_depth<ALPHA>(sg, q, s, p, b, tz)) atomic_min_depth(map + (size_t)(p + __float_as_int(b.y)), tz);
 }
 
 template <bool ALPHA>

@@ -361,6 +361,24 @@ int axr_batch_set_mode(axr_batch *b, int mode);
 int axr_batch_inject_barrier_stall(axr_batch *b, int phantom_blocks, long long spin_limit);
 int axr_set_tuning(axr_ctx *ctx, int min_chunk);
 
+/* How CLDraw.shadowMap (Ops.py:1089-1141) draws the casters: 0 (the
+ * default) = one work item per caster row chunk with global atomics; 2 and 1
+ * = for maps of side <= 8192, the tiled pass -- casters binned to 32 x
+ * 32-texel tiles, each tile's minimum taken in shared memory, casters, spans
+ * and texels that cannot lower the tile skipped before the exact depth --
+ * with each tile's units taken front first (2) or as binned (1).  `slice`
+ * (32 .. 2^20, 0 keeps the current value, 512 at first) is the number of a
+ * tile's units per block: a tile of n units is drawn by ceil(n / slice)
+ * blocks.  The maps are identical in every mode. */
+int axr_set_shadow_mode(axr_ctx *ctx, int mode, int slice);
+
+/* New (no reference counterpart; the reference has no tiled pass): the tiled
+ * passes of shadow map i that overflowed their unit queue (each was drawn
+ * per caster in the same launches, and the queue grew), the units the last
+ * finished pass needed and the queue's capacity.  Waits for the handle's
+ * work.  Any output may be NULL. */
+int axr_shadow_stats(axr_ctx *ctx, int i, int64_t *overflows, int64_t *units, int64_t *cap_units);
+
 int axr_batch_destroy(axr_batch *b);
 
 /* Shadow-map depth pass that allocates no device memory.  No counterpart in
