@@ -84,6 +84,7 @@ struct Shadow {
   int ntx = 0;
   int64_t overflows = 0;      // tiled passes that overflowed the unit queue
   uint32_t last_units = 0;    // units the last checked tiled pass needed
+  uint32_t last_casters[2] = {0, 0};   // opaque, alpha-tested casters of the last checked pass
   // counters of the last two passes (pinned, each with its event), checked
   // once their pass has finished
   uint32_t *h_ring = nullptr;
@@ -269,6 +270,8 @@ int check_shadow_slot(Shadow &sm, int k, bool blocking) {
   const uint32_t *h = sm.h_ring + k * CTR_N;
   if (h[CTR_LIMIT]) return fail(AXR_ECUDA, "a shadow raster loop reached its safety limit; the map is incomplete");
   sm.last_units = h[CTR_SH_UNITS_NEED];
+  sm.last_casters[0] = h[CTR_SH_LIST];
+  sm.last_casters[1] = h[CTR_SH_LIST_A];
   if (h[CTR_SH_OVERFLOW]) sm.overflows++;
   if (h[CTR_SH_OVERFLOW] && h[CTR_SH_UNITS_NEED] > sm.cap_units) {
     CK(cudaStreamSynchronize(sm.st));   // passes in flight still use the old queue
@@ -1363,15 +1366,15 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   return 0;
 }
 
-int axr_shadow_stats(axr_ctx *c, int i, int64_t *overflows, int64_t *units, int64_t *cap_units) {
+int axr_shadow_stats(axr_ctx *c, int i, int64_t *out, int n) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (i < 0 || i >= MAX_SHADOWS || !c->shadows[i].map) return fail(AXR_ESTATE, "shadow map %d does not exist", i);
-  if ((rc = settle(c))) return rc;
+  if (!out || n < 0) return fail(AXR_EINVAL, "shadowStats output");
+  if ((rc = axr_sync(c))) return rc;
   const Shadow &s = c->shadows[i];
-  if (overflows) *overflows = s.overflows;
-  if (units) *units = s.last_units;
-  if (cap_units) *cap_units = s.cap_units;
+  const int64_t v[5] = {s.overflows, s.last_units, s.cap_units, s.last_casters[0], s.last_casters[1]};
+  for (int k = 0; k < n && k < 5; k++) out[k] = v[k];
   return 0;
 }
 
@@ -1417,6 +1420,17 @@ int axr_last_stats(axr_ctx *c, int64_t *kernels, int64_t *n_small, int64_t *n_la
   if (n_small) *n_small = (int64_t)c->h_ctr[CTR_SMALL] + c->h_ctr[CTR_SMALL_A];
   if (n_large) *n_large = c->h_ctr[CTR_LARGE];
   if (n_units) *n_units = c->h_ctr[CTR_UNITS_RESERVED];   // units the frame needed (queued or not)
+  return 0;
+}
+
+int axr_last_queues(axr_ctx *c, int64_t *out, int n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out || n < 0) return fail(AXR_EINVAL, "lastQueues output");
+  if ((rc = axr_sync(c))) return rc;
+  const uint32_t *h = c->h_ctr;
+  const int64_t v[5] = {h[CTR_SMALL], h[CTR_SMALL_A], h[CTR_LARGE], h[CTR_UNITS], h[CTR_UNITS_A]};
+  for (int k = 0; k < n && k < 5; k++) out[k] = v[k];
   return 0;
 }
 

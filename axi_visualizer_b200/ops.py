@@ -442,15 +442,25 @@ class CLDraw:
         are the same in every mode."""
         check(self._L.axr_set_shadow_mode(self._h, int(mode), int(slice)), "setShadowMode")
 
+    def shadowStats(self, i):
+        """Shadow map i's passes: tiled passes whose unit queue overflowed,
+        units and queue capacity of the last pass, its opaque and
+        alpha-tested casters."""
+        v = (C.c_int64 * 5)()
+        check(self._L.axr_shadow_stats(self._h, int(i), v, 5), "shadowStats")
+        return dict(zip(("overflows", "units", "cap_units", "casters", "casters_alpha"), (int(x) for x in v)))
+
     def shadowOverflows(self):
-        """Per shadow map (in index order): (tiled passes whose unit queue
-        overflowed, units the last pass needed, queue capacity)."""
-        out = []
-        for i in sorted(self.SHADOWMAP):
-            v = [C.c_int64() for _ in range(3)]
-            check(self._L.axr_shadow_stats(self._h, int(i), *[C.byref(x) for x in v]), "shadowStats")
-            out.append(tuple(x.value for x in v))
-        return out
+        """Per shadow map (in index order): (overflowed passes, units of the
+        last pass, queue capacity)."""
+        return [tuple(self.shadowStats(i)[k] for k in ("overflows", "units", "cap_units"))
+                for i in sorted(self.SHADOWMAP)]
+
+    def lastQueues(self):
+        """Work queues of the last drawAll by kind."""
+        v = (C.c_int64 * 5)()
+        check(self._L.axr_last_queues(self._h, v, 5), "lastQueues")
+        return dict(zip(("small", "small_alpha", "large", "units", "units_alpha"), (int(x) for x in v)))
 
     def setKernelTiming(self, on=True):
         check(self._L.axr_set_kernel_timing(self._h, 1 if on else 0), "setKernelTiming")

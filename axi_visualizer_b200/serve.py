@@ -122,6 +122,7 @@ class Slab:
     assigned: dict = field(default_factory=dict)   # slot -> Request
     launched_at: float = math.nan
     launches: int = 0
+    solo: bool = False                  # one slot: takes a request that arrives alone
 
     def free_slot(self, w, h):
         for k, wh in enumerate(self.slots):
@@ -231,23 +232,36 @@ class Server:
             pass
         return len(self.slabs)
 
-    def _new_slab(self, now, force=False):
-        if len([s for s in self.slabs if s.state != "retired"]) >= self.max_slabs:
+    def prepare_solo(self):
+        """Makes one single-slot slab per served resolution (as the budget
+        allows): a request that arrives while nothing renders and nothing
+        else waits is launched there, without the other slots of a full
+        slab."""
+        for wh in self.layout:
+            if not any(s.solo and s.slots[0] == wh for s in self.slabs):
+                self._new_slab(-math.inf, force=True, slots=[wh])
+        return sum(1 for s in self.slabs if s.solo)
+
+    def _new_slab(self, now, force=False, slots=None):
+        solo = slots is not None
+        slots = list(slots) if solo else list(self.slot_list)
+        nbytes = int(self.b.slab_bytes(slots)) if solo else self.slab_bytes
+        if not solo and len([s for s in self.slabs if s.state != "retired" and not s.solo]) >= self.max_slabs:
             return None
-        if self.used + self.slab_bytes > self.budget or (now < self._next_alloc and not force):
+        if self.used + nbytes > self.budget or (now < self._next_alloc and not force):
             return None
         free = getattr(self.b, "free_bytes", None)
-        if free is not None and free() < self.slab_bytes + self.hbm_reserve:
+        if free is not None and free() < nbytes + self.hbm_reserve:
             self.low_memory += 1          # the device has less free HBM than the budget assumed
             return None
         try:
-            h = self.b.create(self.slot_list)
+            h = self.b.create(slots)
         except (MemoryError, RuntimeError) as e:   # AxrError is a RuntimeError
             self.alloc_failures += 1
             self._next_alloc = now + self.retry_after
             self.last_alloc_error = str(e)
             return None
-        s = Slab(self._sid, list(self.slot_list), self.slab_bytes, h)
+        s = Slab(self._sid, slots, nbytes, h, solo=solo)
         self._sid += 1
         self.slabs.append(s)
         self.used += s.nbytes
@@ -255,6 +269,8 @@ class Server:
         return s
 
     def _fill(self, s, now):
+        if s.solo:
+            return
         for k, wh in enumerate(s.slots):
             q = self.queues[wh]
             if q and k not in s.assigned:
@@ -265,7 +281,18 @@ class Server:
     def _admit(self, now):
         """Free slots of idle slabs take the oldest waiting request of their
         resolution; while requests still wait, new slabs are made as the
-        budget allows."""
+        budget allows.  A request that waits alone while nothing renders
+        goes to an idle single-slot slab of its resolution, if there is one."""
+        waiting = [q for q in self.queues.values() if q]
+        if len(waiting) == 1 and len(waiting[0]) == 1 and not any(s.state == "inflight" for s in self.slabs) \
+                and not any(s.assigned for s in self.slabs):
+            r = waiting[0][0]
+            solo = next((s for s in self.slabs if s.solo and s.state == "idle" and s.slots[0] == (r.w, r.h)), None)
+            if solo is not None:
+                waiting[0].popleft()
+                solo.assigned[0] = r
+                r.status, r.admitted = "admitted", now
+                return
         for s in self.slabs:
             if s.state == "idle":
                 self._fill(s, now)

@@ -37,11 +37,14 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
-# each kernel on this workload, from the ncu capture summarised under
-# profiles/; None until captured.
-NCU_TRAFFIC = {"k_raster_small": 33614848, "k_raster_small_alpha": 13604608,
-               "k_shadow_raster": 48411392 + 18432, "k_shadow_raster_alpha": 10116608,
-               "k_shade": 30231296 + 1395968}
+# each kernel on this workload: (bytes, the summary under profiles/ that
+# gives the capture).  A kernel changed since its capture has no entry.
+NCU_TRAFFIC = {
+    "k_raster_small": (33614848, "profiles/ncu_kernels_1080p_1m.md"),
+    "k_raster_small_alpha": (13604608, "profiles/ncu_kernels_1080p_1m.md"),
+    "k_shadow_raster": (48411392 + 18432, "profiles/ncu_kernels_1080p_1m.md"),
+    "k_shadow_raster_alpha": (10116608, "profiles/ncu_kernels_1080p_1m.md"),
+}
 
 
 def progress(msg):
@@ -108,30 +111,60 @@ class Clocks:
 
 # ------------------------------------------------------------------ roofline bookkeeping
 
-def algorithmic_bytes(scene, stats, visible_tris):
+def algorithmic_bytes(scene, q, shadow_q, visible_tris):
     """Lower-bound bytes each kernel must move per launch: the geometry it has
-    to read once and the framebuffer / map bytes it has to write once."""
+    to read once and the framebuffer / map bytes it has to write once.  `q`
+    is the last drawAll's queues by kind (CLDraw.lastQueues), `shadow_q`
+    each map's last pass (CLDraw.shadowStats); per-map figures are averaged
+    over the maps, as the per-kernel times are."""
     T = scene.ntris
     cull_T = sum(g.ntris for g in scene.groups if g.flags & 8)
-    alpha_T = sum(g.ntris for g in scene.groups if g.flags & 2)
     npx = W * H
-    smap = [sc.dim * sc.dim for sc in scene.shadows]
+    nm = max(1, len(scene.shadows))
+    smap = sum(sc.dim * sc.dim for sc in scene.shadows) / nm
+    cast = sum(s["casters"] for s in shadow_q) / nm
+    cast_a = sum(s["casters_alpha"] for s in shadow_q) / nm
+    units = sum(s["units"] for s in shadow_q) / nm
     return {
         # xyz of every triangle (+ normals of culled groups), 4 B per list entry
-        "k_setup": 36 * T + 36 * cull_T + 4 * (stats["n_small"] + stats["n_large"]),
-        # xyz of every small triangle, visibility word written once per pixel
-        "k_raster_small": 36 * stats["n_small"] + 8 * npx,
-        "k_coarse": 36 * stats["n_large"] + 8 * stats["n_units"],
-        "k_raster_tiled": 36 * stats["n_large"] + 8 * stats["n_units"],
+        "k_setup": 36 * T + 36 * cull_T + 4 * (q["small"] + q["small_alpha"] + q["large"]),
+        # xyz (+ uv of alpha-tested ones) of every small triangle; the
+        # visibility word of every pixel updated once by the opaque pass
+        "k_raster_small": 36 * q["small"] + 8 * npx,
+        "k_raster_small_alpha": 60 * q["small_alpha"],
+        # xyz of every large triangle and its (triangle, tile) units
+        "k_coarse": 36 * q["large"] + 8 * (q["units"] + q["units_alpha"]),
+        "k_raster_tiled": 36 * q["large"] + 8 * q["units"],
+        "k_raster_tiled_alpha": 8 * q["units_alpha"],
         # visibility word read, colour + depth written, attributes of the visible triangles read once
         "k_shade": 8 * npx + 10 * npx + 132 * visible_tris,
         "k_init_keys": 4 * npx + 8 * npx,
         "k_clear_depth": 4 * npx,
-        # per cascade: xyz (+ uv of alpha casters) read, map written once
-        "k_shadow_setup": 36 * T,
-        "k_shadow_raster": 36 * T + 24 * alpha_T + 4 * (sum(smap) // max(1, len(smap))),
-        "k_clear_shadow": 4 * (sum(smap) // max(1, len(smap))),
+        # per cascade: xyz of every triangle read, the casters listed
+        "k_shadow_setup": 36 * T + 4 * (cast + cast_a),
+        # xyz (+ uv) of the casters read, the map written once
+        "k_shadow_raster": 36 * cast + 4 * smap,
+        "k_shadow_raster_alpha": 60 * cast_a,
+        # tiled pass: caster records (32 B) and units (4 B), map tiles read and written once
+        "k_shadow_bin": 16 * (cast + cast_a) + 4 * units,
+        "k_shadow_sort": 8 * units,
+        "k_shadow_tiles": 32 * cast + 4 * units + 8 * smap,
+        "k_shadow_tiles_alpha": 56 * cast_a,
+        "k_clear_shadow": 4 * smap,
     }
+
+
+def roofline_of(kernel, ktimes, alg, hbm, peak_kind, steps):
+    """achieved = the kernel's algorithmic bytes per launch / its average
+    CUDA-event launch time; frac against the measured HBM peak."""
+    ms, n = ktimes[kernel]
+    avg_s = ms / n / 1000.0
+    a = alg.get(kernel, 0)
+    achieved = a / avg_s / 1e9
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": peak_kind, "traffic": NCU_TRAFFIC.get(kernel, (None,))[0],
+            "traffic_capture": NCU_TRAFFIC.get(kernel, (None, None))[1], "algorithmic_bytes": a,
+            "avg_us": 1e6 * avg_s, "launches_per_frame": n / steps}
 
 
 def frame_bytes(scene):
@@ -657,7 +690,9 @@ def served_section(device, n_poisson=1000, n_burst=400, rates=(200.0, 1000.0), t
     warm = SV.poisson_trace(40, 1e6, len(scenes), seed=99, burst=True)
     log("served: warm-up")
     srv.prepare(srv.max_slabs)
+    srv.prepare_solo()
     srv.run(warm)
+    srv.run(SV.poisson_trace(8, 50.0, len(scenes), seed=98))    # warms the single-slot slabs too
     plain.run(SV.poisson_trace(40, 1e6, len(scenes), seed=99, burst=True))
     keep = ("frames_per_s", "Mpix_per_s", "p50_ms", "p99_ms", "max_ms", "done")
     sched = ("views_per_launch", "launches", "max_inflight", "slabs")
@@ -837,20 +872,23 @@ def main():
     D.setKernelTiming(False)
     tid, cov = D.getIDs()
     visible = int(np.unique(tid[tid >= 0]).size)
-    alg = algorithmic_bytes(scene, stats, visible)
+    queues = D.lastQueues()
+    shadow_q = [D.shadowStats(k) for k in range(len(scene.shadows))]
+    alg = algorithmic_bytes(scene, queues, shadow_q, visible)
     hbm, peak_kind = peaks()
     per_kernel = {k: {"avg_us": 1000 * ms / n, "launches_per_frame": n / args.steps,
                       "share": 0.0} for k, (ms, n) in ktimes.items()}
     tot = sum(ms for ms, n in ktimes.values())
     for k, (ms, n) in ktimes.items():
         per_kernel[k]["share"] = ms / tot if tot else 0.0
+        per_kernel[k]["algorithmic_bytes"] = alg.get(k)
+        if k in alg:
+            per_kernel[k]["frac_of_hbm"] = alg[k] / (ms / n / 1000.0) / 1e9 / hbm
+    # the dominant kernel by its share of the frame, and by its time per launch
     dom = max(ktimes.items(), key=lambda kv: kv[1][0])[0]
-    dom_avg_s = ktimes[dom][0] / ktimes[dom][1] / 1000.0
-    achieved = alg.get(dom, 0) / dom_avg_s / 1e9
-    traffic = NCU_TRAFFIC.get(dom)
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
-                "algorithmic_bytes": alg.get(dom, 0)}
+    dom_launch = max(ktimes.items(), key=lambda kv: kv[1][0] / kv[1][1])[0]
+    roofline = roofline_of(dom, ktimes, alg, hbm, peak_kind, args.steps)
+    roofline["by_launch"] = roofline_of(dom_launch, ktimes, alg, hbm, peak_kind, args.steps)
     fb = frame_bytes(scene)
     frame_roof = {"bytes": fb, "achieved_gbs": fb / (t_ms / args.steps / 1000.0) / 1e9}
     frame_roof["frac"] = frame_roof["achieved_gbs"] / hbm
@@ -989,7 +1027,7 @@ def main():
                             "what": "setPos/setVM/clearZBuffer/drawAll with the cascades resident (the "
                                     "reference's render loop); the headline frame also renders both cascades"},
             "kernels": per_kernel,
-            "queues": stats,
+            "queues": dict(stats, **queues, shadow=shadow_q),
             "clocks": clk,
             "cpu_baseline": cpu,
             "batched": batched,

@@ -243,6 +243,11 @@ int axr_frame_device_ptrs(axr_ctx *ctx, void **r, void **g, void **b, void **dep
  * work-queue sizes (small triangles, large triangles, tile units). */
 int axr_last_stats(axr_ctx *ctx, int64_t *kernels, int64_t *n_small, int64_t *n_large, int64_t *n_units);
 
+/* Work-queue sizes of the last drawAll by kind (new; waits for the
+ * handle's work): out[0..n) of, in order, opaque and alpha-tested small
+ * triangles, large triangles, and opaque and alpha-tested tile units. */
+int axr_last_queues(axr_ctx *ctx, int64_t *out, int n);
+
 /* Number of kernels the handle has launched since axr_create. */
 int axr_launch_count(axr_ctx *ctx, int64_t *total);
 
@@ -372,12 +377,12 @@ int axr_set_tuning(axr_ctx *ctx, int min_chunk);
  * blocks.  The maps are identical in every mode. */
 int axr_set_shadow_mode(axr_ctx *ctx, int mode, int slice);
 
-/* New (no reference counterpart; the reference has no tiled pass): the tiled
- * passes of shadow map i that overflowed their unit queue (each was drawn
- * per caster in the same launches, and the queue grew), the units the last
- * finished pass needed and the queue's capacity.  Waits for the handle's
- * work.  Any output may be NULL. */
-int axr_shadow_stats(axr_ctx *ctx, int i, int64_t *overflows, int64_t *units, int64_t *cap_units);
+/* Queue sizes of shadow map i's passes (new, like axr_last_stats; waits for
+ * the handle's work): out[0..n) of, in order, the tiled passes that
+ * overflowed their unit queue (each was drawn per caster in the same
+ * launches, and the queue grew), the units the last pass needed, the
+ * queue's capacity, and the last pass's opaque and alpha-tested casters. */
+int axr_shadow_stats(axr_ctx *ctx, int i, int64_t *out, int n);
 
 int axr_batch_destroy(axr_batch *b);
 

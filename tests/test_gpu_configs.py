@@ -4,6 +4,9 @@
   trilinear 2048^2 textures, two 2048^2 cascades): CUDA frame against the
   oracle (OpenMP), same bars as the small parity cases -- coverage, triangle
   ids, depth and shadow maps bit-exact, colour within 1/255 after gamma.
+- 3840x2160 / 9,988,608 triangles: the CUDA frame and both 4096^2 cascades
+  against the oracle at the same bars, and the batched launch of the
+  cascades, the main view and six cube faces against the plain path.
 - The batched view set of the 24,192-triangle scene (six 512^2 cube faces,
   2048^2 + 1024^2 cascades, the 1920x1080 main view) in one persistent
   launch: every view bit-identical to the same view rendered alone.
@@ -79,13 +82,13 @@ def test_batched_view_set_equals_single_views():
     assert B.stats()["graph"]
 
 
-def test_stress_scene_batched_launch_equals_plain_frame():
+def test_stress_scene_equals_oracle_and_batched_launch():
     """3840x2160 / 9,988,608 triangles, 16 trilinear 4096^2 textures, 29%
-    alpha-tested, 4096^2 cascades (too large for the oracle to finish in
-    seconds): the batched launch of both cascades, the main view and six
-    1024^2 cube faces gives the main view and the cascades bit for bit as the
-    plain shadowMap + drawAll path, whose arithmetic the smaller cases pin to
-    the oracle."""
+    alpha-tested, 4096^2 cascades: the plain shadowMap + drawAll frame
+    against the oracle (OpenMP, all host cores) at the parity bars --
+    coverage, triangle ids, depth and both cascades bit-exact, colour within
+    1/255 after gamma -- and the batched launch of both cascades, the main
+    view and six 1024^2 cube faces bit for bit as the plain path."""
     from axi_visualizer_b200.batch import Batch, scene_batch_views
     from axi_visualizer_b200.ops import SceneRenderer
     sc = S.scene_c5()
@@ -107,3 +110,7 @@ def test_stress_scene_batched_launch_equals_plain_frame():
     assert np.array_equal(B.ids(nd)[0], tid)
     st = R.draw.lastStats()
     assert st["n_small"] > 1_000_000 and cov.mean() > 0.5
+    fr, smaps = O.render(sc, main, nthreads=os.cpu_count() or 1)
+    shm = [R.draw.getSHM(k) for k in range(nd)]
+    exact, psnr = check_frame(fr, smaps, (*want, tid, cov, shm))
+    print(f"4K/10M: exact u16 fraction {exact:.6f}, PSNR {psnr:.1f} dB")

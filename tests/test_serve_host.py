@@ -248,3 +248,28 @@ def test_scene_range_checked(bad):
     srv = SV.Server(FakeBackend(), budget_bytes=1e9, layout={RES[0]: 1})
     srv.submit(req(0, scene=bad), 0.0)
     assert srv.requests[0].status == "rejected"
+
+
+def test_lone_request_goes_to_a_single_slot_slab():
+    """A request that arrives while nothing renders and nothing else waits is
+    launched in a one-slot slab of its resolution; requests that overlap
+    fill the full slabs as before, and every result is still delivered."""
+    be = FakeBackend(complete_after=1)
+    srv = SV.Server(be, budget_bytes=10_000, layout={RES[0]: 2, RES[1]: 1}, max_slabs=2, depth=2, keep_frames=True)
+    assert srv.prepare(1) == 1 and srv.prepare_solo() == 2
+    assert sorted(len(h["slots"]) for h in be.created) == [1, 1, 3]
+    srv.submit(req(1, res=RES[1]), 0.0)
+    srv.step(0.0)
+    solo = [s for s in srv.slabs if s.solo and s.state == "inflight"]
+    assert len(solo) == 1 and solo[0].slots == [RES[1]] and be.launches == [[1]]
+    drive(srv, 1.0)
+    # two requests at once: they share a full slab
+    srv.submit(req(2, res=RES[0]), 1.0)
+    srv.submit(req(3, res=RES[0]), 1.0)
+    srv.step(1.0)
+    assert be.launches[-1] == [2, 3]
+    assert not any(s.solo and s.state == "inflight" for s in srv.slabs)
+    drive(srv, 2.0, t=1.0)
+    for rid in (1, 2, 3):
+        r = srv.requests[rid]
+        assert r.status == "done" and int(r.frame[0][0, 0]) == rid
