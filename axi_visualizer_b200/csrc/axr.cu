@@ -2096,6 +2096,12 @@ int axr_batch_destroy(axr_batch *b) {
 namespace {
 
 constexpr uint32_t NOALLOC_MAX_TRIS = 1u << 20;     // 4 MiB of triangle list per GPU
+constexpr int NOALLOC_MAX_DIM = 16384;
+// Each caster is one work item whose rows lie in the map plus the setup's
+// 120-texel guard bands (trisetupOrtho.c), so no raster loop reaches the
+// safety cap, which this entry point could not report (it returns before
+// the GPU runs).
+static_assert(NOALLOC_MAX_DIM + 240 < LOOP_LIMIT, "a caster's rows stay below the loop cap");
 constexpr uint32_t NOALLOC_WORDS = NOALLOC_MAX_TRIS + CTR_N;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_WORDS];
 
@@ -2202,7 +2208,8 @@ extern "C" int axr_shadow_map_noalloc(const float *xyz, const float *uv, const u
   if (ntris < 0 || (uint32_t)ntris > NOALLOC_MAX_TRIS)
     return fail(AXR_EINVAL, "axr_shadow_map_noalloc takes at most %u triangles per call, got %d", NOALLOC_MAX_TRIS,
                 ntris);
-  if (dim < 4 || dim > 16384) return fail(AXR_EINVAL, "shadow map size %d outside [4, 16384]", dim);
+  if (dim < 4 || dim > NOALLOC_MAX_DIM)
+    return fail(AXR_EINVAL, "shadow map size %d outside [4, %d]", dim, NOALLOC_MAX_DIM);
   if (alpha_mask && (!uv || !is_pow2(alpha_side)))
     return fail(AXR_EINVAL, "alpha casters need uv and a power-of-two mask side (got %d)", alpha_side);
   uint32_t *scratch = nullptr;

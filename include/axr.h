@@ -407,7 +407,10 @@ int axr_batch_destroy(axr_batch *b);
  * (cudaGetSymbolAddress); make the first call on each device before any
  * stream capture.  Every call shares the array, so calls that overlap on the
  * GPU (concurrent streams, or several host threads) race and give wrong
- * maps: serialise them. */
+ * maps: serialise them.  It returns before the GPU runs, so unlike
+ * axr_shadow_map it reports no device-side condition: the raster loops'
+ * safety cap (65,536 rounds) cannot trip here, since each caster is one
+ * work item of at most dim + 240 rows (16,624 for the largest map). */
 int axr_shadow_map_noalloc(const float *xyz, const float *uv, const uint8_t *alpha_mask, int alpha_side, int ntris,
                            const float pos[3], const float vm[9], float scale, float bias, float *map, int dim,
                            void *stream);
