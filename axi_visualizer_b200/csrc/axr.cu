@@ -1295,9 +1295,10 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
       return fail(AXR_ENOMEM, "caster list of shadow map %d", i);
     sm.cap = c->cap_list;
   }
-  if (tiled && !sm.rec) {
-    if (cudaMalloc(&sm.rec, 2 * sizeof(uint4) * sm.cap) != cudaSuccess)
-      return fail(AXR_ENOMEM, "caster records of shadow map %d", i);
+  // caster records of the tiled pass
+  if (tiled && !sm.rec && cudaMalloc(&sm.rec, 2 * sizeof(uint4) * sm.cap) != cudaSuccess)
+    return fail(AXR_ENOMEM, "caster records of shadow map %d", i);
+  if (tiled && !sm.units) {
     // initial tile-unit queue (grows after an overflow); AXR_SHADOW_UNIT_QUEUE overrides
     uint32_t units0 = sm.cap + sm.cap / 2 + 1024;
     if (const char *e = getenv("AXR_SHADOW_UNIT_QUEUE")) {

@@ -665,28 +665,31 @@ __device__ __forceinline__ void fill_round(Q &q, int lane, int cnt, F &&pix) {
 }
 
 // Writes lane's span record: row offset cyw, first pixel lo, ends cx1 / cx2.
+// Returns false when the span must be drawn by its own lane (span_queueable).
 template <bool ALPHA>
-__device__ __forceinline__ void vis_put(VisQ<ALPHA> &q, int lane, int cyw, int lo, uint32_t ord, float cx1, float cx2,
+__device__ __forceinline__ bool vis_put(VisQ<ALPHA> &q, int lane, int cyw, int lo, uint32_t ord, float cx1, float cx2,
                                         float cz1, float cz2, V2 cu1, V2 cu2, int g) {
   float d = cx1 - cx2;
-  q.a[lane] = make_float4(cx2, d, span_recip_exact(d, cx2, lo), cz1);
+  float y = span_recip_exact(d, cx2, lo);
+  q.a[lane] = make_float4(cx2, d, y, cz1);
   q.b[lane] = make_float4(cz2, __int_as_float(cyw + lo), __int_as_float(lo), __uint_as_float(ord));
   if (ALPHA) {
     q.c[lane] = make_float4(cu1.x, cu1.y, cu2.x, cu2.y);
     q.g[lane] = g;
   }
+  return span_queueable(d, y);
 }
 
 // Per-fragment visibility: alpha test (av_draw_alpha.c:80-97) then the
 // packed depth/order atomicMin.
 // Pixel number p of span s (x = p + b.z, address = p + b.y).  The reciprocal
 // of the interpolated 1/z is correctly rounded (__frcp_rn), i.e. 1.0f / x.
-template <bool ALPHA>
+// DIV: a span its own lane draws, with the true division.
+template <bool ALPHA, bool DIV = false>
 __device__ __forceinline__ void vis_pixel(const DrawParams &P, const GroupDev *sg, const VisQ<ALPHA> &q, int s, int p) {
   const float4 a = q.a[s], b = q.b[s];
   float n = (float)(p + __float_as_int(b.z)) - a.x;
-  float t = a.z != 0.f ? quot_fast(n, a.y, a.z) : n / a.y;
-  t = clamp_t(t);
+  float t = DIV ? clamp_t(n / a.y) : span_t(n, a.y, a.z);
   float tz = __frcp_rn((1 - t) * b.x + t * a.w);
   if (tz != tz) return;
   if (ALPHA) {
@@ -699,6 +702,13 @@ __device__ __forceinline__ void vis_pixel(const DrawParams &P, const GroupDev *s
   }
   atomicMin((unsigned long long *)&P.keys[(size_t)(p + __float_as_int(b.y))],
             (unsigned long long)frag_key(tz, __float_as_uint(b.w)));
+}
+
+// The lane's own span record, drawn by the lane alone with the true division.
+template <bool ALPHA>
+__device__ __forceinline__ void vis_serial(const DrawParams &P, const GroupDev *sg, const VisQ<ALPHA> &q, int lane,
+                                           int cnt) {
+  for (int j = 0; j < cnt; j++) vis_pixel<ALPHA, true>(P, sg, q, lane, j);
 }
 
 template <bool ALPHA>
@@ -823,13 +833,17 @@ struct SmallLane {
 
   // writes the current row's span into q[lane], advances; returns the span's
   // pixel count and sets `live` false after the last row
-  __device__ __forceinline__ int emit(const DrawParams &P, VisQ<ALPHA> &q, int lane, bool &live) {
+  __device__ __forceinline__ int emit(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, bool &live) {
     int lo = 0, cnt = 0;
     if (cy >= 0 && cy < P.view.h) {
       if (half == 0) span_clip(f2i(cx2), cx1, P.view.w, lo, cnt);
       else span_clip(f2i(cx1), cx2, P.view.w, lo, cnt);
     }
-    if (cnt) vis_put<ALPHA>(q, lane, cy * P.view.w, lo, make_order(0, gtri, half), cx1, cx2, cz1, cz2, cu1, cu2, g);
+    if (cnt && !vis_put<ALPHA>(q, lane, cy * P.view.w, lo, make_order(0, gtri, half), cx1, cx2, cz1, cz2, cu1, cu2,
+                               g)) {
+      vis_serial<ALPHA>(P, sg, q, lane, cnt);
+      cnt = 0;
+    }
     skip_row();
     live = --left > 0;
     return cnt;
@@ -859,7 +873,7 @@ __device__ __forceinline__ void raster_small_loop(const DrawParams &P, const Gro
         break;
       }
       int cnt = 0;
-      if (live) cnt = L.emit(P, q, lane, live);
+      if (live) cnt = L.emit(P, sg, q, lane, live);
       vis_fill<ALPHA>(P, sg, q, lane, cnt);
     }
   }
@@ -1106,18 +1120,24 @@ struct TileLane {
     return live_half;
   }
 
-  __device__ __forceinline__ void put(const DrawParams &P, VisQ<ALPHA> &q, int lane, int lo) {
-    vis_put<ALPHA>(q, lane, cy * P.view.w, lo, make_order(1, gtri, half), cx1, cx2, cz1, cz2, cu1, cu2, g);
+  // queues the row's span, or draws it with the lane alone (span_queueable);
+  // returns the pixels queued
+  __device__ __forceinline__ int put(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, int lo,
+                                     int cnt) {
+    if (vis_put<ALPHA>(q, lane, cy * P.view.w, lo, make_order(1, gtri, half), cx1, cx2, cz1, cz2, cu1, cu2, g))
+      return cnt;
+    vis_serial<ALPHA>(P, sg, q, lane, cnt);
+    return 0;
   }
 
-  __device__ __forceinline__ int emit(const DrawParams &P, VisQ<ALPHA> &q, int lane, bool &live) {
+  __device__ __forceinline__ int emit(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, bool &live) {
     int cnt = 0;
     if (half == 0) {
       if (cx2 < xMax && cx1 > xMin) {
         int lo = f2i(clampf_(cx2, xMin, xMax));
         int hi = f2i(floorf(clampf_(cx1, xMin, xMax)));
         cnt = hi >= lo ? hi - lo + 1 : 0;
-        if (cnt) put(P, q, lane, lo);
+        if (cnt) cnt = put(P, sg, q, lane, lo, cnt);
       }
       cx1 += s1; cx2 += s2; cz1 += sz1; cz2 += sz2;
       if (ALPHA) { cu1 = add2(cu1, su1); cu2 = add2(cu2, su2); }
@@ -1132,7 +1152,7 @@ struct TileLane {
       int lo = f2i(clampf_(cx1, xMin, xMax));
       int hi = f2i(floorf(clampf_(cx2, xMin, xMax)));
       cnt = hi >= lo ? hi - lo + 1 : 0;
-      if (cnt) put(P, q, lane, lo);
+      if (cnt) cnt = put(P, sg, q, lane, lo, cnt);
     }
     cx1 -= s1; cx2 -= s2; cz1 -= sz1; cz2 -= sz2;
     if (ALPHA) { cu1 = sub2(cu1, su1); cu2 = sub2(cu2, su2); }
@@ -1163,7 +1183,7 @@ __device__ __forceinline__ void raster_tiled_loop(const DrawParams &P, const Gro
         break;
       }
       int cnt = 0;
-      if (live) cnt = L.emit(P, q, lane, live);
+      if (live) cnt = L.emit(P, sg, q, lane, live);
       vis_fill<ALPHA>(P, sg, q, lane, cnt);
     }
   }
@@ -1187,7 +1207,7 @@ __device__ __forceinline__ void fallback_unit(const DrawParams &P, const GroupDe
   TileLane<ALPHA> L;
   bool live = L.init(P, sg, make_uint2(gt, (uint32_t)tile));
   for (int round = 0; live && round < LOOP_LIMIT; round++) {
-    int cnt = L.emit(P, q, lane, live);   // the lane's own record: pixel j is x = lo + j
+    int cnt = L.emit(P, sg, q, lane, live);   // the lane's own record: pixel j is x = lo + j
     for (int j = 0; j < cnt; j++) vis_pixel<ALPHA>(P, sg, q, lane, j);
   }
 }
@@ -1738,8 +1758,8 @@ __device__ __forceinline__ bool caster_tiles(const int x[3], int y1, int y3, int
   return true;
 }
 
-// Writes caster t's record at its list slot and counts it in every tile it
-// can write (opaque counts first, alpha-tested after them).
+// Writes caster t's record at its list slot and, in the tiled pass, counts
+// it in every tile it can write (opaque counts first, alpha-tested after them).
 __device__ __forceinline__ void shadow_record(const ShadowParams &S, int t, int g, bool alpha, int ix[3], int iy[3],
                                               float z[3], uint32_t slot) {
   int perm = caster_sort(ix, iy, z);
@@ -1748,7 +1768,7 @@ __device__ __forceinline__ void shadow_record(const ShadowParams &S, int t, int 
   S.rec[2 * (size_t)slot + 1] = make_uint4(__float_as_uint(z[1]), __float_as_uint(z[2]), (uint32_t)t,
                                            (uint32_t)perm | ((uint32_t)g << 8));
   int tx0, tx1, ty0, ty1;
-  if (!caster_tiles(ix, iy[0], iy[2], S.sh.dim, tx0, tx1, ty0, ty1)) return;
+  if (!S.tcnt || !caster_tiles(ix, iy[0], iy[2], S.sh.dim, tx0, tx1, ty0, ty1)) return;
   const uint32_t base = alpha ? (uint32_t)S.ntiles : 0u;
   for (int ty = ty0; ty <= ty1; ty++)
     for (int tx = tx0; tx <= tx1; tx++) {
@@ -1936,7 +1956,8 @@ struct ShadowLane {
     return true;
   }
 
-  int left;   // rows left in this lane's chunk (a whole caster: y3 - y1 + 1)
+  int left;      // rows left in this lane's chunk (a whole caster: y3 - y1 + 1)
+  bool serial;   // emit_tile: the span just written needs the true division
 
   // advances one row without drawing (the replay up to a chunk's first row)
   __device__ __forceinline__ void skip_row() {
@@ -1965,7 +1986,10 @@ struct ShadowLane {
     return true;
   }
 
+  // sets `serial` when the span just written needs the true division (the
+  // caller then draws it with this lane alone)
   __device__ __forceinline__ int emit(int dim, ShadowQ<ALPHA> &q, int lane, bool &live) {
+    serial = false;
     int cnt = 0;
     if (cy >= 0 && cy < dim) {
       int a0 = half == 0 ? f2i(cx2) : f2i(cx1);
@@ -1974,12 +1998,14 @@ struct ShadowLane {
       cnt = hi >= lo ? hi - lo + 1 : 0;
       if (cnt) {
         float d = cx1 - cx2;
-        q.a[lane] = make_float4(cx2, d, span_recip_exact(d, cx2, lo), cz1);
+        float y = span_recip_exact(d, cx2, lo);
+        q.a[lane] = make_float4(cx2, d, y, cz1);
         q.b[lane] = make_float4(cz2, __int_as_float(cy * dim + lo), __int_as_float(lo), 0.f);
         if (ALPHA) {
           q.c[lane] = make_float4(cu1, cv1, cu2, cv2);
           q.g[lane] = g;
         }
+        serial = !span_queueable(d, y);
       }
     }
     skip_row();
@@ -2006,9 +2032,12 @@ struct ShadowLane {
       for (int bx = (lo - tx0) >> SUB_LOG; bx <= (hi - tx0) >> SUB_LOG; bx++) m = max(m, row[bx]);
       if (m < floor_bits) cnt = 0;
     }
+    serial = false;
     if (cnt) {
       float d = cx1 - cx2;
-      q.a[lane] = make_float4(cx2, d, span_recip_exact(d, cx2, lo), cz1);
+      float y = span_recip_exact(d, cx2, lo);
+      serial = !span_queueable(d, y);   // then the caller draws the span with this lane alone
+      q.a[lane] = make_float4(cx2, d, y, cz1);
       q.b[lane] = make_float4(cz2, __int_as_float((cy - ty0) * TROW + (lo - tx0)), __int_as_float(lo),
                               __int_as_float(floor_bits));
       if (ALPHA) {
@@ -2029,13 +2058,12 @@ struct ShadowLane {
 
 // drawmin.c:71-76 / drawminalpha.c:83-97 for pixel number p of span s: the
 // depth tz, or false when nothing is written (NaN depth, alpha discard)
-template <bool ALPHA>
+template <bool ALPHA, bool DIV = false>
 __device__ __forceinline__ bool shadow_depth(const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p, float4 b,
                                              float &tz) {
   const float4 a = q.a[s];
   float n = (float)(p + __float_as_int(b.z)) - a.x;
-  float t = a.z != 0.f ? quot_fast(n, a.y, a.z) : n / a.y;
-  t = clamp_t(t);
+  float t = DIV ? clamp_t(n / a.y) : span_t(n, a.y, a.z);
   tz = __frcp_rn((1 - t) * b.x + t * a.w);
   if (tz != tz) return false;
   if (ALPHA) {
@@ -2053,11 +2081,11 @@ __device__ __forceinline__ bool shadow_depth(const GroupDev *sg, const ShadowQ<A
 }
 
 // drawmin.c:71-76 / drawminalpha.c:83-97 for one pixel of span s
-template <bool ALPHA>
+template <bool ALPHA, bool DIV = false>
 __device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p) {
   const float4 b = q.b[s];
   float tz;
-  if (shadow_depth<ALPHA>(sg, q, s, p, b, tz)) atomic_min_depth(map + (size_t)(p + __float_as_int(b.y)), tz);
+  if (shadow_depth<ALPHA, DIV>(sg, q, s, p, b, tz)) atomic_min_depth(map + (size_t)(p + __float_as_int(b.y)), tz);
 }
 
 template <bool ALPHA>
@@ -2091,7 +2119,13 @@ __device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const Gr
         break;
       }
       int cnt = 0;
-      if (live) cnt = L.emit(dim, q, lane, live);
+      if (live) {
+        cnt = L.emit(dim, q, lane, live);
+        if (L.serial) {   // a span the queue cannot take: this lane draws it
+          for (int j = 0; j < cnt; j++) shadow_pixel<ALPHA, true>(S.map, sg, q, lane, j);
+          cnt = 0;
+        }
+      }
       fill_round(q, lane, cnt, [&](int s, int p) { shadow_pixel<ALPHA>(S.map, sg, q, s, p); });
     }
   }

@@ -129,6 +129,20 @@ __device__ __forceinline__ float quot_fast(float n, float d, float y) {
   return __fmaf_rn(r, y, q);
 }
 
+// t = clamp(n / d, 0, 1) of a pixel of a span queued with its reciprocal y
+// (span_recip_exact).  y != 0: the quotient through the reciprocal.  y == 0
+// is queued only for d = +-0, where n / d is an infinity whose sign is
+// sign(n) xor sign(d) (clamped to 1 or 0), or NaN for n = 0 (clamped to 1),
+// so no pixel of a queued span divides.
+__device__ __forceinline__ float span_t(float n, float d, float y) {
+  if (y != 0.f) return clamp_t(quot_fast(n, d, y));
+  return (n == 0.f || ((__float_as_uint(n) ^ __float_as_uint(d)) & 0x80000000u) == 0u) ? 1.f : 0.f;
+}
+// Whether every pixel of a span can take span_t: otherwise (a reciprocal out
+// of the safe range with d != 0, which real scenes almost never produce)
+// the span's own lane draws it with the true division.
+__device__ __forceinline__ bool span_queueable(float d, float y) { return y != 0.f || d == 0.f; }
+
 __device__ __forceinline__ float quot_by_recip(float n, float d, float y) {
   float an = fabsf(n);
   if (y != 0.f && an <= 1.1529215e18f && (an >= 8.6736174e-19f || n == 0.f)) {

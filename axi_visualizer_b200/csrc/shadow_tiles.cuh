@@ -215,13 +215,13 @@ __global__ void __launch_bounds__(256) k_shadow_sort(ShadowParams S) {
 
 // One texel of a tile: the depth-floor test, then drawmin.c's depth and the
 // minimum in shared memory (the per-caster path's atomic_min_depth).
-template <bool ALPHA>
+template <bool ALPHA, bool DIV = false>
 __device__ __forceinline__ void tile_pixel(int *tile, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p) {
   const float4 b = q.b[s];
   int off = p + __float_as_int(b.y);
   if (tile[off] < __float_as_int(b.w)) return;
   float tz;
-  if (!shadow_depth<ALPHA>(sg, q, s, p, b, tz)) return;
+  if (!shadow_depth<ALPHA, DIV>(sg, q, s, p, b, tz)) return;
   if (tz >= 0.f) atomicMin(tile + off, __float_as_int(tz));
   else atomicMax((unsigned int *)(tile + off), __float_as_uint(tz));
 }
@@ -326,7 +326,13 @@ __device__ __forceinline__ void tile_units(const ShadowParams &S, const GroupDev
         break;
       }
       int cnt = 0;
-      if (live) cnt = L.emit_tile(q, lane, tx0, tx1, ty0, ty1, smax, live);
+      if (live) {
+        cnt = L.emit_tile(q, lane, tx0, tx1, ty0, ty1, smax, live);
+        if (L.serial) {   // a span the queue cannot take: this lane draws it
+          for (int j = 0; j < cnt; j++) tile_pixel<ALPHA, true>(tile, sg, q, lane, j);
+          cnt = 0;
+        }
+      }
       fill_round(q, lane, cnt, [&](int s, int p) { tile_pixel<ALPHA>(tile, sg, q, s, p); });
     }
   }
