@@ -28,7 +28,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-MIP, ALPHA, SHADOW, CULL, MULTI = 1, 2, 4, 8, 16
+MIP, ALPHA, SHADOW, CULL, MULTI, NORMAL = 1, 2, 4, 8, 16, 32
 
 
 def flags_from_string(s) -> int:
@@ -48,6 +48,8 @@ def flags_from_string(s) -> int:
         f |= CULL
     if "multi" in keys:
         f |= MULTI
+    if "normal" in keys:
+        f |= NORMAL
     return f
 
 
@@ -132,6 +134,11 @@ class Group:
     alpha_index: int = 0
     mip_bias: float = 0.0
     cast: bool = True
+    # normal-mapped materials: RGBA bytes, one texel per texel of the texture
+    # (or chain); the "normal" pair's second value (roughness); metal
+    nm: np.ndarray = None
+    roughness: float = 0.5
+    metal: bool = False
 
     @property
     def ntris(self) -> int:
@@ -280,6 +287,21 @@ def create_mips(rgb):
         levels.append(a)
     levels.reverse()
     return np.concatenate([x.reshape(-1, 3) for x in levels], axis=0)
+
+
+def normal_map(rng, n, mip: bool):
+    """Seeded bumpy tangent-space normal map of side n as RGBA bytes (the
+    layout CLDraw.addNrmMap stores; A = 0), full resolution or a create_mips
+    chain smallest level first."""
+    h = rng.standard_normal((n + 1, n + 1))
+    gx, gy = h[:-1, 1:] - h[:-1, :-1], h[1:, :-1] - h[:-1, :-1]
+    v = np.stack([-gx, -gy, np.full_like(gx, 2.0)], axis=-1)
+    v /= np.linalg.norm(v, axis=-1, keepdims=True)
+    rgb = np.clip(np.round((v * 0.5 + 0.5) * 255.0), 0, 255).astype(np.int64)
+    flat = create_mips(rgb) if mip else rgb.reshape(-1, 3)
+    out = np.zeros((flat.shape[0], 4), np.uint8)
+    out[:, :3] = flat
+    return out.reshape(-1)
 
 
 def texture_planes(rgb, mip: bool):
@@ -491,6 +513,31 @@ def scene_served(seed, tmin=50_000, tmax=1_000_000, tex=1024, alpha_tex=512, cas
     shadows = [ShadowCam.facing(cascades[0], cascades[0] / 2 / (extent * 0.75), (0, 0, 0), SUN),
                ShadowCam.facing(cascades[1], cascades[1] / 2 / (extent * 1.5), (0, 0, 0), SUN)]
     return _finish(groups, [(qmask.reshape(-1), alpha_tex)], shadows)
+
+
+def scene_normal(seed=6, terrain_n=16, spheres=20, nquads=30, tex=64, shadow_dim=256):
+    """The normal-mapped materials on one raster (av_draw_normmap.c,
+    _alpha.c, _mip.c): terrain with a normal map (roughness 0.5), metal
+    icospheres (roughness 0.3) and trilinear icospheres with a normal-map
+    chain (mipBias 0.4), alpha-tested quads with a normal map; two cascades
+    (the normal-mapped materials sample the first)."""
+    rng = np.random.default_rng(seed)
+    xyz, vn, uv = terrain(rng, terrain_n, 2.0, (-terrain_n, 0.0, -terrain_n), 1.0)
+    sx, sn, su = icospheres(rng, spheres, 0.5, 2.5, -12, 12)
+    qx, qn, qu = quads(rng, nquads, -10, 10, 1.0, 4.0)
+    rgb, _ = noise_texture(rng, tex)
+    qrgb, qmask = noise_texture(rng, tex, alpha_p=0.6)
+    half = (spheres // 2) * 80 * 3
+    groups = [_group(xyz, vn, uv, rgb, NORMAL | SHADOW, 0.2),
+              _group(sx[:half], sn[:half], su[:half], rgb, NORMAL | SHADOW | CULL, 0.2),
+              _group(sx[half:], sn[half:], su[half:], rgb, NORMAL | MIP | SHADOW | CULL, 0.2, mip_bias=0.4),
+              _group(qx, qn, qu, qrgb, NORMAL | ALPHA | SHADOW, 0.2, alpha_index=0)]
+    for g, rough, metal in zip(groups, (0.5, 0.3, 0.5, 0.7), (False, True, False, False)):
+        g.nm = normal_map(rng, tex, bool(g.flags & MIP))
+        g.roughness, g.metal = rough, metal
+    shadows = [ShadowCam.facing(shadow_dim, shadow_dim / 2 / 30.0, (0, 0, 0), SUN),
+               ShadowCam.facing(shadow_dim // 2, shadow_dim / 4 / 60.0, (0, 0, 0), SUN)]
+    return _finish(groups, [(qmask.reshape(-1), tex)], shadows)
 
 
 def default_view(w, h, pos=(0.0, 5.0, -25.0), target=(0.0, 0.0, 0.0), fov=70.0):

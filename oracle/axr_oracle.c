@@ -181,6 +181,8 @@ typedef struct {
   int num_mip;                 /* mip materials */
   float fmip;                  /* per-triangle mip fraction */
   int mip, len_mip, len_mip2, start_mip, start_mip2;
+  f3 tangent, bitangent;       /* normal-mapped materials: per-triangle frame */
+  int spec_pow, spec_pow2;     /* (int)exp2(12 (1 - roughness)), (int)half_sqrt of it */
 } shade_ctx;
 
 /* attribute bundle interpolated along the two active edges
@@ -294,6 +296,139 @@ static void multi_core(const shade_ctx *c, size_t pix, float t, float tz, f2 uvi
   f->bo[pix] = u16sat((float)u16sat(m * tb[1] + n * tb[2] + o * tb[3] + w1 * tb[0]) * (light * dirCol.z + col.z));
 }
 
+/* ---- normal-mapped materials (av_draw_normmap.c, _alpha.c, _mip.c) ---- */
+
+/* pown(x, n) for n >= 0 by repeated squaring (the convention pinned where
+ * OpenCL leaves pown's rounding to the device) */
+static inline float pown_rs(float x, int n) {
+  unsigned k = n < 0 ? 0u - (unsigned)n : (unsigned)n;
+  float r = 1.0f, b = x;
+  while (k) {
+    if (k & 1u) r *= b;
+    b *= b;
+    k >>= 1;
+  }
+  return n < 0 ? 1.0f / r : r;
+}
+
+/* sampleShadow, which the reference calls but defines nowhere, as this
+ * library defines it: the five taps of one cascade (centre, +-2 texels in x
+ * and y) at the truncated map position, counted where the map is nearer
+ * than `depth`, only when the centre lies in [2, 2 wS - 2) on both axes;
+ * the shadowed fraction is count * 0.2 */
+static float sample_shadow5(const orc_shadow *s, float depth, float sfx, float sfy) {
+  int wS = s->dim / 2;
+  int sx = f2i(sfx), sy = f2i(sfy), n = 0;
+  if (sx >= 2 && sx < 2 * wS - 2 && sy >= 2 && sy < 2 * wS - 2) {
+    const float *SD = s->map;
+    int r = 2 * wS;
+    if (SD[r * sy + sx] < depth) n += 1;
+    if (SD[r * (sy + 2) + sx] < depth) n += 1;
+    if (SD[r * (sy - 2) + sx] < depth) n += 1;
+    if (SD[r * sy + (sx + 2)] < depth) n += 1;
+    if (SD[r * sy + (sx - 2)] < depth) n += 1;
+  }
+  return (float)n * 0.2f;
+}
+
+/* bilinear normal-map texel (R, G, B bytes) at the taps, as the sources'
+ * texi1*texi2*convert_float3(NM[tex]) + ... */
+static inline f3 bilerp_nm(const taps *q, const uint8_t *NM) {
+  const uint8_t *a = NM + 4 * (size_t)q->tex, *b = NM + 4 * (size_t)q->tex10;
+  const uint8_t *cc = NM + 4 * (size_t)q->tex01, *d = NM + 4 * (size_t)q->tex11;
+  float w00 = q->texi1 * q->texi2, w10 = q->texr1 * q->texi2, w01 = q->texi1 * q->texr2, w11 = q->texr1 * q->texr2;
+  f3 r;
+  r.x = w00 * (float)a[0] + w10 * (float)b[0] + w01 * (float)cc[0] + w11 * (float)d[0];
+  r.y = w00 * (float)a[1] + w10 * (float)b[1] + w01 * (float)cc[1] + w11 * (float)d[1];
+  r.z = w00 * (float)a[2] + w10 * (float)b[2] + w01 * (float)cc[2] + w11 * (float)d[2];
+  return r;
+}
+
+/* av_draw_normmap.c:47-149 (_alpha.c shares it after its alpha test) and
+ * av_draw_normmap_mip.c:73-160 for a fragment that passed the depth test */
+static void normal_core(const shade_ctx *c, size_t pix, float t, float tz, f2 uvi, const attrs *a1,
+                        const attrs *a2) {
+  const orc_frame *f = c->f;
+  const orc_group *g = c->g;
+  const int mip = (g->flags & ORC_MIP) != 0;
+  float omt = 1 - t;
+  float outR, outG, outB;
+  f3 tg;
+  taps q = make_taps(uvi, tz, mip ? c->len_mip : g->tex_size, mip ? c->start_mip : 0);
+  outR = bilerp_u16(&q, g->tr);
+  outG = bilerp_u16(&q, g->tg);
+  outB = bilerp_u16(&q, g->tb);
+  tg = bilerp_nm(&q, g->nm);
+  if (mip) {
+    taps q2 = make_taps(uvi, tz, c->len_mip2, c->start_mip2);
+    float fm = c->fmip, ofm = 1 - c->fmip;
+    outR = ofm * outR + fm * bilerp_u16(&q2, g->tr);
+    outG = ofm * outG + fm * bilerp_u16(&q2, g->tg);
+    outB = ofm * outB + fm * bilerp_u16(&q2, g->tb);
+    tg = f3add(f3smul(ofm, tg), f3smul(fm, bilerp_nm(&q2, g->nm)));
+  }
+  float light = 1;
+  if (c->nsh > 0) {
+    const orc_shadow *sh = &c->sh[0];
+    f3 sp = {sh->pos[0], sh->pos[1], sh->pos[2]};
+    f3 pos = f3sub(f3mul(f3add(f3smul(omt, a2->p), f3smul(t, a1->p)), tz), sp);
+    float depth = dot3(pos, f3ld(sh->vv));
+    float wS = (float)(sh->dim / 2);
+    float sfx = (dot3(pos, f3ld(sh->vv + 3)) * sh->scale) + wS;
+    float sfy = (dot3(pos, f3ld(sh->vv + 6)) * -sh->scale) + wS;
+    light = 1 - sample_shadow5(sh, depth, sfx, sfy);
+  } else {
+    light = 1 - 0.f;
+  }
+  f3 col = f3mul(f3add(f3smul(omt, a2->li), f3smul(t, a1->li)), tz);
+  f3 norm = fast_normalize(f3mul(f3add(f3smul(omt, a2->n), f3smul(t, a1->n)), tz));
+  tg = f3sub(f3mul(f3div(tg, 255.f), 2.f), (f3){1.f, 1.f, 1.f});
+  tg = fast_normalize(tg);
+  norm = fast_normalize(f3add(f3add(f3smul(tg.z, norm), f3smul(-tg.y, c->tangent)), f3smul(-tg.x, c->bitangent)));
+  f3 vp = {f->pos[0], f->pos[1], f->pos[2]};
+  f3 lint = {f->lint[0], f->lint[1], f->lint[2]};
+  f3 ldir = {f->ldir[0], f->ldir[1], f->ldir[2]};
+  f3 pos = f3mul(f3add(f3smul(omt, a2->p), f3smul(t, a1->p)), tz);
+  f3 spec;
+  if (mip) {
+    f3 a = f3sub(pos, vp);
+    f3 h = fast_normalize(f3add(fast_normalize(a), ldir));
+    float theta = fmaxf(0.f, dot3(h, norm));
+    float mf = (float)c->mip + c->fmip;
+    int sp = f2i(1.f * (mf * mf));
+    spec = f3smul(((pown_rs(theta, sp) * 256.f) * light) * 2.f, lint);
+    spec = f3mul(spec, (float)(sp + 1) / (2.f * 3.1416f));
+  } else {
+    f3 a = fast_normalize(f3sub(pos, vp));
+    f3 h = fast_normalize(f3add(a, ldir));
+    float theta = fmaxf(0.f, dot3(h, norm));
+    int sp = c->spec_pow;
+    spec = f3smul(((pown_rs(theta, sp) * 256.f) * 4.f) * light, lint);
+    spec = f3mul(spec, (float)(sp + 2) / (8.f * 3.1416f));
+    a = f3sub(pos, vp);
+    float nd = dot3(a, norm);
+    f3 refl = fast_normalize(f3sub(a, f3smul(2.f * nd, norm)));
+    f3 up = {0.f, 1.f, 0.f};
+    theta = fmaxf(0.f, dot3(refl, up));
+    f3 sky = {0.1f, 0.3f, 0.5f};
+    spec = f3add(spec, f3smul((pown_rs(theta, 2) * 128.f) * (float)(1 + g->is_metal), sky));
+    theta = fmaxf(0.f, dot3(fast_normalize(a), refl));
+    f3 grey = {0.2f, 0.2f, 0.2f};
+    spec = f3add(spec, f3smul(pown_rs(theta, c->spec_pow2) * 256.f, grey));
+    if (g->is_metal) {
+      spec.x *= (float)g->tr[q.tex] / 1024.f;
+      spec.y *= (float)g->tg[q.tex] / 1024.f;
+      spec.z *= (float)g->tb[q.tex] / 1024.f;
+      light = 0.f;
+      col.x = col.y = col.z = 0.f;
+    }
+  }
+  f3 dirCol = f3smul(fmaxf(0.f, dot3(norm, ldir)), lint);
+  f->ro[pix] = u16sat(spec.x + outR * (light * dirCol.x + col.x));
+  f->go[pix] = u16sat(spec.y + outG * (light * dirCol.y + col.y));
+  f->bo[pix] = u16sat(spec.z + outB * (light * dirCol.z + col.z));
+}
+
 /* One fragment at (cy, ax) with edge interpolants a1 (edge 1) and a2
  * (edge 2).  `zcur` points at the depth sample the test reads (the global
  * depth buffer in the serial model).  Returns 1 if it wrote. */
@@ -320,6 +455,12 @@ static int fragment(const shade_ctx *c, int tri, int cy, int ax, float t, float 
   f->db[pix] = tz;
   if ((flags & ORC_MULTI) && !(flags & ORC_ALPHA)) {
     multi_core(c, pix, t, tz, uvi, a1, a2);
+    f->tri_id[pix] = c->gid_base + tri;
+    f->cov[pix] = 1;
+    return 1;
+  }
+  if (flags & ORC_NORMAL) {
+    normal_core(c, pix, t, tz, uvi, a1, a2);
     f->tri_id[pix] = c->gid_base + tri;
     f->cov[pix] = 1;
     return 1;
@@ -448,6 +589,26 @@ static void mip_setup(shade_ctx *c, tri_setup *s, int small, const int *ix, cons
   s->v[0].p = f3mul(p1, z1); s->v[1].p = f3mul(p2, z2); s->v[2].p = f3mul(p3, z3);
 }
 
+/* shader_setup of the normal-mapped sources (av_draw_normmap.c:24-38): the
+ * tangent frame from the sorted vertices' uv and position divided by z,
+ * before they are multiplied back.  Called before the mip setup, which
+ * divides the same values; without ORC_MIP this setup makes the round trip
+ * itself. */
+static void normal_setup(shade_ctx *c, tri_setup *s) {
+  float z1 = s->z[0], z2 = s->z[1], z3 = s->z[2];
+  f2 uv1 = f2div(s->v[0].uv, z1), uv2 = f2div(s->v[1].uv, z2), uv3 = f2div(s->v[2].uv, z3);
+  f3 p1 = f3div(s->v[0].p, z1), p2 = f3div(s->v[1].p, z2), p3 = f3div(s->v[2].p, z3);
+  f2 dUV1 = f2sub(uv2, uv1), dUV2 = f2sub(uv3, uv1);
+  f3 dPos1 = f3sub(p2, p1), dPos2 = f3sub(p3, p1);
+  float rdet = 1.f / (dUV1.x * dUV2.y - dUV1.y * dUV2.x);
+  c->tangent = fast_normalize(f3mul(f3sub(f3mul(dPos1, dUV2.y), f3mul(dPos2, dUV1.y)), rdet));
+  c->bitangent = fast_normalize(f3mul(f3sub(f3mul(dPos2, dUV1.x), f3mul(dPos1, dUV2.x)), rdet));
+  if (!(c->g->flags & ORC_MIP)) {
+    s->v[0].uv = f2mul(uv1, z1); s->v[1].uv = f2mul(uv2, z2); s->v[2].uv = f2mul(uv3, z3);
+    s->v[0].p = f3mul(p1, z1); s->v[1].p = f3mul(p2, z2); s->v[2].p = f3mul(p3, z3);
+  }
+}
+
 /* ------------------------------------------------------------------ */
 /* direct raster of small triangles: Templates.py:210-323              */
 /* rows restricted to [row0, row1) (strip-parallel baseline)           */
@@ -484,6 +645,7 @@ static void draw_small_tri(shade_ctx *c, int tri, const float sp[6], const float
   float z4 = z1 + ydiff1 * (z3 - z1);
   attrs v4 = attrs_add(s.v[0], attrs_smul(ydiff1, attrs_sub(s.v[2], s.v[0])));
   s.v[3] = v4;
+  if (g->flags & ORC_NORMAL) normal_setup(c, &s);
   if (g->flags & ORC_MIP) {
     s.x[0] = (float)x1; s.x[1] = (float)x2; s.x[2] = (float)x3;
     s.y[0] = (float)y1; s.y[1] = (float)y2; s.y[2] = (float)y3;
@@ -580,6 +742,7 @@ static void draw_tiled_tri(shade_ctx *c, int tri, int bx, const float sp[6], con
   float z4 = z1 + ydiff1 * (z3 - z1);
   attrs v4 = attrs_add(s.v[0], attrs_smul(ydiff1, attrs_sub(s.v[2], s.v[0])));
   s.v[3] = v4;
+  if (g->flags & ORC_NORMAL) normal_setup(c, &s);
   if (g->flags & ORC_MIP) mip_setup(c, &s, 0, NULL, NULL);
   attrs a1v = s.v[0], a2v = s.v[1], a3v = s.v[2];
 
@@ -765,6 +928,14 @@ static void init_ctx(shade_ctx *c, const orc_frame *f, const orc_group *g, int g
   c->sh = sh;
   c->nsh = nsh;
   c->num_mip = (g->flags & ORC_MIP) ? g->tex_size : 0;
+  if (g->flags & ORC_NORMAL) {
+    /* av_draw_normmap.c:127: int specPow = exp2(12*(1.f - roughness)), with
+     * exp2 correctly rounded; the third specular term's power is
+     * (int)half_sqrt((float)specPow), half_sqrt correctly rounded */
+    float e = 12.f * (1.f - g->roughness);
+    c->spec_pow = f2i((float)exp2((double)e));
+    c->spec_pow2 = f2i(sqrtf((float)c->spec_pow));
+  }
 }
 
 int orc_draw_all(orc_frame *f, const orc_group *g, int ng, const uint8_t *mask,

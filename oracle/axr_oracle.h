@@ -44,6 +44,7 @@ extern "C" {
 #define ORC_SHADOW 4
 #define ORC_CULL   8
 #define ORC_MULTI 16   /* av_draw_multi.c: blend with the next three groups' textures */
+#define ORC_NORMAL 32  /* av_draw_normmap.c (+ _alpha.c with ORC_ALPHA, _mip.c with ORC_MIP) */
 
 typedef struct orc_group {
   int ntris;
@@ -56,6 +57,11 @@ typedef struct orc_group {
   int flags;         /* ORC_* */
   int alpha_index;   /* which alpha mask the alpha test samples */
   float mip_bias;
+  /* normal-mapped materials: RGBA normal map with one texel per texel of the
+   * texture (or chain), roughness (the "normal" pair's second value), metal */
+  const uint8_t *nm;
+  float roughness;
+  int is_metal;
 } orc_group;
 
 typedef struct orc_alpha {
@@ -86,7 +92,8 @@ typedef struct orc_frame {
 
 /* One CLDraw.drawAll: mask[g] != 0 skips group g (Ops0.py:482-485).
  * shadows[0..nshadow) are the cascades the `shadow` materials sample
- * (drawAll's shadowIds).  nthreads > 1 runs the OpenMP build (same result). */
+ * (drawAll's shadowIds); the normal-mapped materials sample shadows[0].
+ * nthreads > 1 runs the OpenMP build (same result). */
 int orc_draw_all(orc_frame *f, const orc_group *g, int ng, const uint8_t *mask,
                  const orc_alpha *alphas, int nalpha,
                  const orc_shadow *shadows, int nshadow, int nthreads);

@@ -55,12 +55,29 @@ KERNELS = [
 # kernels the reference generates from an AVSL source with its own
 # Shaders_src/AVSL.py (compile_AVSL: the tiled `draw`, then `drawSmall`, as
 # compile_file writes them): (namespace, AVSL source, prelude).  The
-# normal-mapped mip material calls `sampleShadow`, which the reference
-# defines nowhere; the prelude gives it a stand-in returning 0 (no shadow),
-# exact for the pin, which draws with a zero light intensity.
-NO_SHADOW = "inline float sampleShadow(float, float, float, float *, int, float) { return 0.f; }"
+# normal-mapped materials call `sampleShadow`, which the reference defines
+# nowhere; the prelude defines it as this library does (its own choice):
+# the five taps of one cascade (centre, +-2 texels in x and y) at the
+# truncated map position, counted where the map is nearer than `depth`,
+# only when the centre lies in [2, 2 wS - 2) on both axes; the shadowed
+# fraction is count * 0.2.
+SHADOW5 = """
+inline float sampleShadow(float depth, float sfx, float sfy, float *SD, int wS, float) {
+  int sx = cvt_int(sfx), sy = cvt_int(sfy), n = 0;
+  if (sx >= 2 && sx < 2 * wS - 2 && sy >= 2 && sy < 2 * wS - 2) {
+    if (SD[2 * wS * sy + sx] < depth) n += 1;
+    if (SD[2 * wS * (sy + 2) + sx] < depth) n += 1;
+    if (SD[2 * wS * (sy - 2) + sx] < depth) n += 1;
+    if (SD[2 * wS * sy + (sx + 2)] < depth) n += 1;
+    if (SD[2 * wS * sy + (sx - 2)] < depth) n += 1;
+  }
+  return (float)n * 0.2f;
+}
+"""
 GENERATED = [
-    ("ref_draw_mip", "PyOpenCL27C/Shaders_src/av_draw_normmap_mip.c", NO_SHADOW),
+    ("ref_draw_mip", "PyOpenCL27C/Shaders_src/av_draw_normmap_mip.c", SHADOW5),
+    ("ref_draw_nrm", "PyOpenCL27C/Shaders_src/av_draw_normmap.c", SHADOW5),
+    ("ref_draw_nrm_alpha", "PyOpenCL27C/Shaders_src/av_draw_normmap_alpha.c", SHADOW5),
 ]
 
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",

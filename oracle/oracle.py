@@ -31,7 +31,8 @@ def build_oracle(force: bool = False) -> str:
 class OrcGroup(C.Structure):
     _fields_ = [("ntris", C.c_int), ("xyz", C.c_void_p), ("vn", C.c_void_p), ("uv", C.c_void_p),
                 ("li", C.c_void_p), ("tr", C.c_void_p), ("tg", C.c_void_p), ("tb", C.c_void_p),
-                ("tex_size", C.c_int), ("flags", C.c_int), ("alpha_index", C.c_int), ("mip_bias", C.c_float)]
+                ("tex_size", C.c_int), ("flags", C.c_int), ("alpha_index", C.c_int), ("mip_bias", C.c_float),
+                ("nm", C.c_void_p), ("roughness", C.c_float), ("is_metal", C.c_int)]
 
 
 class OrcAlpha(C.Structure):
@@ -165,9 +166,11 @@ def _groups(scene):
     keep = []
     for k, g in enumerate(scene.groups):
         r, gg, b = g.tex
-        keep += [g.xyz, g.vn, g.uv, g.li, r, gg, b]
+        nm = getattr(g, "nm", None)
+        keep += [g.xyz, g.vn, g.uv, g.li, r, gg, b, nm]
         arr[k] = OrcGroup(g.ntris, _ptr(g.xyz), _ptr(g.vn), _ptr(g.uv), _ptr(g.li), _ptr(r), _ptr(gg), _ptr(b),
-                          g.tex_size, g.flags, g.alpha_index, g.mip_bias)
+                          g.tex_size, g.flags, g.alpha_index, g.mip_bias, _ptr(nm) if nm is not None else None,
+                          getattr(g, "roughness", 0.0), int(getattr(g, "metal", False)))
     return arr, keep
 
 
@@ -339,6 +342,9 @@ def ref_lib():
         R.ref_ssao.argtypes = [C.c_void_p, C.c_void_p]
         R.ref_bloom.argtypes = [C.c_void_p]
         R.ref_dof.argtypes = [C.c_void_p, C.c_float]
+        R.ref_set_normal.restype = C.c_int
+        R.ref_set_normal.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_long, C.c_float, C.c_int, C.c_float]
+        R.ref_set_normal_shadow.argtypes = [C.c_void_p, C.c_int]
         R.ref_set_mip_kernels.restype = C.c_int
         R.ref_set_mip_kernels.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         R.ref_get_geometry.restype = C.c_int
@@ -369,6 +375,16 @@ class RefDraw:
         self.R.ref_set_light(self.h, _ptr(self._light[0]), _ptr(self._light[1]))
         self.flags = np.array([g.flags for g in scene.groups], np.int32)
         self.aidx = np.array([g.alpha_index for g in scene.groups], np.int32)
+        # the normal-mapped materials (flags bit 5): their maps, and the
+        # first cascade as the one they sample
+        for k, g in enumerate(scene.groups):
+            if g.flags & 32:
+                nm = np.ascontiguousarray(g.nm, np.uint8)
+                self._keep.append(nm)
+                if self.R.ref_set_normal(self.h, k, _ptr(nm), nm.size // 4, g.roughness, int(g.metal),
+                                         g.mip_bias) != 0:
+                    raise RuntimeError(f"ref_set_normal: group {k}")
+        self.R.ref_set_normal_shadow(self.h, 0 if scene.shadows else -1)
 
     def __del__(self):
         try:

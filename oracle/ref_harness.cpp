@@ -68,6 +68,30 @@ void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P,
                float3 *SV, float *SPos, const float mipBias, const int wF, const int hF, const int lenP);
 float *local_ZBuf();
 }
+// Shaders_src/av_draw_normmap.c and av_draw_normmap_alpha.c, expanded likewise
+namespace ref_draw_nrm {
+void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+          float3 *I, float3 *N, float3 *PXYZ, ushort *TR, ushort *TG, ushort *TB, const int lenT, uchar3 *NM,
+          float roughness, char isMetal, float *Vpos, float3 *LInt, float3 *LDir, float *SD, const int wS,
+          const float sScale, float3 *SV, float *SPos, const int wF, const int hF);
+void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+               float3 *I, float3 *N, float3 *PXYZ, ushort *TR, ushort *TG, ushort *TB, const int lenT, uchar3 *NM,
+               float roughness, char isMetal, float *Vpos, float3 *LInt, float3 *LDir, float *SD, const int wS,
+               const float sScale, float3 *SV, float *SPos, const int wF, const int hF, const int lenP);
+float *local_ZBuf();
+}
+namespace ref_draw_nrm_alpha {
+void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+          float3 *I, float3 *N, float3 *PXYZ, ushort *TR, ushort *TG, ushort *TB, const int lenT, bool *TA,
+          uchar3 *NM, float roughness, char isMetal, float *Vpos, float3 *LInt, float3 *LDir, float *SD,
+          const int wS, const float sScale, float3 *SV, float *SPos, const int wF, const int hF);
+void drawSmall(int *TO, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
+               float3 *I, float3 *N, float3 *PXYZ, ushort *TR, ushort *TG, ushort *TB, const int lenT, bool *TA,
+               uchar3 *NM, float roughness, char isMetal, float *Vpos, float3 *LInt, float3 *LDir, float *SD,
+               const int wS, const float sScale, float3 *SV, float *SPos, const int wF, const int hF,
+               const int lenP);
+float *local_ZBuf();
+}
 namespace ref_draw_alpha {
 void draw(int *TO, int *TN, ushort *Ro, ushort *Go, ushort *Bo, float *F, float2 *P, float *Z, float2 *UV,
           float3 *I, float3 *N, float3 *PXYZ, float3 *LInt, float3 *LDir, ushort *TR, ushort *TG, ushort *TB,
@@ -143,9 +167,11 @@ struct Group {
   std::vector<int> tia, tib, tna, tnb, toa, tob;
   std::vector<ushort> tr, tg, tb;
   int tex_size = 0;
-  // the normal-mapped mip material: its normal map (one texel per texel of
-  // the chain) and the draw's mipBias
+  // the normal-mapped materials: the normal map (one texel per texel of the
+  // texture or chain), roughness and metal switch, and the mipBias
   std::vector<uchar3> nm;
+  float roughness = 0;
+  int is_metal = 0;
   float mip_bias = 0;
 };
 
@@ -172,7 +198,28 @@ struct Ctx {
   Shadow shadows[8];
   int overflow = 0;
   int mip_kernels = 0;   // mip groups (flags bit 0) drawn by ref_draw_mip
+  int normal_shadow = -1; // the cascade the normal-mapped materials sample (-1: none)
 };
+
+// the shadow arguments of the normal-mapped materials (getShadow, Ops.py:621-622)
+struct NormalShadow {
+  float *SD;
+  int wS;
+  float scale;
+  float3 *SV;
+  float *SPos;
+};
+float g_no_shadow_map[16] = {65535, 65535, 65535, 65535, 65535, 65535, 65535, 65535,
+                             65535, 65535, 65535, 65535, 65535, 65535, 65535, 65535};
+float3 g_no_shadow_vec[3];
+float g_no_shadow_pos[3] = {0, 0, 0};
+NormalShadow normal_shadow(Ctx *c) {
+  if (c->normal_shadow >= 0 && c->normal_shadow < 8 && !c->shadows[c->normal_shadow].map.empty()) {
+    Shadow &s = c->shadows[c->normal_shadow];
+    return {s.map.data(), s.dim / 2, s.scale, s.vec, s.pos};
+  }
+  return {g_no_shadow_map, 2, 1.0f, g_no_shadow_vec, g_no_shadow_pos};   // no tap can lie in [2, 2)
+}
 
 // run kernel `fn(bx, tx)` over a 1-D grid of `ng` groups of BS items
 template <class F>
@@ -340,12 +387,36 @@ int ref_set_mip_kernels(void *h, int on, const float *bias, int n) {
   for (int i = 0; i < n; i++) {
     Group &G = c->groups[i];
     G.mip_bias = bias ? bias[i] : 0.f;
-    uchar3 flat;
-    flat.x = 128; flat.y = 128; flat.z = 255; flat.pad_ = 0;
-    G.nm.assign(G.tr.size(), flat);
+    if (G.nm.empty()) {
+      uchar3 flat;
+      flat.x = 128; flat.y = 128; flat.z = 255; flat.pad_ = 0;
+      G.nm.assign(G.tr.size(), flat);
+    }
   }
   return 0;
 }
+
+// CLDraw.addNrmMap + a normal-mapped material on group g: the normal map as
+// RGBA bytes (one texel per texel of the group's texture or chain), the
+// material's roughness (its "normal" pair's second value) and metal switch,
+// and its mipBias (the normal-mapped mip material).  The cascade the
+// materials sample is set with ref_set_normal_shadow.
+int ref_set_normal(void *h, int g, const uint8_t *rgba, long ntexels, float roughness, int is_metal,
+                   float mip_bias) {
+  Ctx *c = (Ctx *)h;
+  if (g < 0 || g >= (int)c->groups.size() || ntexels < (long)c->groups[g].tr.size()) return -1;
+  Group &G = c->groups[g];
+  G.nm.resize(ntexels);
+  for (long i = 0; i < ntexels; i++) {
+    G.nm[i].x = rgba[4 * i]; G.nm[i].y = rgba[4 * i + 1]; G.nm[i].z = rgba[4 * i + 2]; G.nm[i].pad_ = rgba[4 * i + 3];
+  }
+  G.roughness = roughness;
+  G.is_metal = is_metal;
+  G.mip_bias = mip_bias;
+  return 0;
+}
+
+void ref_set_normal_shadow(void *h, int i) { ((Ctx *)h)->normal_shadow = i; }
 
 void ref_set_view(void *h, const float *pos, const float *vv, float sscale, float cax, float cay) {
   Ctx *c = (Ctx *)h;
@@ -428,6 +499,25 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
                                  m.t[0][0], m.t[0][1], m.t[0][2], m.len[0], m.t[1][0], m.t[1][1], m.t[1][2], m.len[1],
                                  m.t[2][0], m.t[2][1], m.t[2][2], m.len[2], m.t[3][0], m.t[3][1], m.t[3][2], m.len[3],
                                  c->W, c->H, newSize[tn]);
+      } else if (flags[tn] & 32) {   // av_draw_normmap(_alpha, _mip).c
+        NormalShadow ns = normal_shadow(c);
+        if (alpha)
+          ref_draw_nrm_alpha::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(),
+                                        G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(),
+                                        G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, TA, G.nm.data(),
+                                        G.roughness, (char)G.is_metal, c->vpos, c->lint, c->ldir, ns.SD, ns.wS,
+                                        ns.scale, ns.SV, ns.SPos, c->W, c->H, newSize[tn]);
+        else if (flags[tn] & 1)
+          ref_draw_mip::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(), G.sp.data(),
+                                  G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), G.tr.data(),
+                                  G.tg.data(), G.tb.data(), G.tex_size, G.nm.data(), c->vpos, c->lint, c->ldir,
+                                  ns.SD, ns.wS, ns.scale, ns.SV, ns.SPos, G.mip_bias, c->W, c->H, newSize[tn]);
+        else
+          ref_draw_nrm::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(), G.sp.data(),
+                                  G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(), G.xyz.data(), G.tr.data(),
+                                  G.tg.data(), G.tb.data(), G.tex_size, G.nm.data(), G.roughness, (char)G.is_metal,
+                                  c->vpos, c->lint, c->ldir, ns.SD, ns.wS, ns.scale, ns.SV, ns.SPos, c->W, c->H,
+                                  newSize[tn]);
       } else if (!alpha && c->mip_kernels && (flags[tn] & 1)) {
         float sd[4] = {0, 0, 0, 0};
         ref_draw_mip::drawSmall(G.toa.data(), c->ro.data(), c->go.data(), c->bo.data(), c->db.data(), G.sp.data(),
@@ -471,9 +561,12 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
     bool *TA = alpha ? (bool *)c->alphas[alpha_index[tn]].data() : nullptr;
     int ntiles = c->WC * c->HC;
     auto tile = [&](int bx) {
-      bool mipk = !alpha && !multi && c->mip_kernels && (flags[tn] & 1);
-      float *zb = multi ? ref_drawmulti::local_ZBuf() : alpha ? ref_draw_alpha::local_ZBuf()
-                  : mipk ? ref_draw_mip::local_ZBuf() : ref_draw::local_ZBuf();
+      bool nrm = !multi && (flags[tn] & 32);
+      bool mipk = !alpha && !multi && (flags[tn] & 1) && (c->mip_kernels || nrm);
+      float *zb = multi ? ref_drawmulti::local_ZBuf() : (nrm && alpha) ? ref_draw_nrm_alpha::local_ZBuf()
+                  : mipk ? ref_draw_mip::local_ZBuf() : nrm ? ref_draw_nrm::local_ZBuf()
+                  : alpha ? ref_draw_alpha::local_ZBuf() : ref_draw::local_ZBuf();
+      NormalShadow ns = normal_shadow(c);
       int tileX = bx % c->WC, tileY = bx / c->WC;
       for (int r = 0; r < 16; r++)
         for (int i = 0; i < 16; i++) zb[r * 16 + i] = c->db[(size_t)c->W * (tileY * 16 + r) + tileX * 16 + i];
@@ -489,6 +582,23 @@ int ref_draw_all(void *h, const int *flags, const int *alpha_index, const uint8_
                               c->ldir, m.t[0][0], m.t[0][1], m.t[0][2], m.len[0], m.t[1][0], m.t[1][1], m.t[1][2],
                               m.len[1], m.t[2][0], m.t[2][1], m.t[2][2], m.len[2], m.t[3][0], m.t[3][1], m.t[3][2],
                               m.len[3], c->W, c->H);
+        } else if (nrm && alpha) {
+          ref_draw_nrm_alpha::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
+                                   c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),
+                                   G.xyz.data(), G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, TA, G.nm.data(),
+                                   G.roughness, (char)G.is_metal, c->vpos, c->lint, c->ldir, ns.SD, ns.wS, ns.scale,
+                                   ns.SV, ns.SPos, c->W, c->H);
+        } else if (mipk && nrm) {
+          ref_draw_mip::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
+                             c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),
+                             G.xyz.data(), G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, G.nm.data(), c->vpos,
+                             c->lint, c->ldir, ns.SD, ns.wS, ns.scale, ns.SV, ns.SPos, G.mip_bias, c->W, c->H);
+        } else if (nrm) {
+          ref_draw_nrm::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),
+                             c->db.data(), G.sp.data(), G.zz.data(), G.uv.data(), G.li.data(), G.vn.data(),
+                             G.xyz.data(), G.tr.data(), G.tg.data(), G.tb.data(), G.tex_size, G.nm.data(),
+                             G.roughness, (char)G.is_metal, c->vpos, c->lint, c->ldir, ns.SD, ns.wS, ns.scale,
+                             ns.SV, ns.SPos, c->W, c->H);
         } else if (mipk) {
           float sd[4] = {0, 0, 0, 0};
           ref_draw_mip::draw(c->ibuf.data(), c->nbuf.data(), c->ro.data(), c->go.data(), c->bo.data(),

@@ -169,6 +169,11 @@ inline float2 fabs(float2 a) { return make_float2(::fabsf(a.x), ::fabsf(a.y)); }
 // log2 correctly rounded (the convention pinned for the library and the
 // oracle): the double result rounded once to float
 inline float log2(float x) { return (float)::log2((double)x); }
+// exp2 correctly rounded (the double result rounded once), half_sqrt as the
+// correctly rounded square root: conventions where OpenCL leaves the
+// precision to the device
+inline float exp2(float x) { return (float)::exp2((double)x); }
+inline float half_sqrt(float x) { return ::sqrtf(x); }
 // pown(x, n) = x^n for integer n, by repeated squaring of |n| then, for
 // negative n, the reciprocal (OpenCL leaves its rounding to the device)
 inline float pown(float x, int n) {

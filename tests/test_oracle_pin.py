@@ -178,3 +178,34 @@ def test_trilinear_core_equals_reference_mip_material(i):
     for n, a, o in (("r", r, fr.ro), ("g", g, fr.go), ("b", b, fr.bo)):
         d = int((a != o).sum())
         assert d == 0, f"{n}: {d} px differ (max {int(np.abs(a.astype(int) - o).max())})"
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference checkout)")
+@pytest.mark.parametrize("seed,pos", [(6, (2, 6, -14)), (13, (-4, 9, -10))])
+def test_normal_mapped_materials_equal_reference_kernels(seed, pos):
+    """The oracle's normal-mapped materials against the reference's own
+    kernels (Shaders_src/av_draw_normmap.c, _alpha.c and _mip.c expanded by
+    its AVSL generator, tiled and small): tangent frames, normal-map taps,
+    the specular terms, the metal switch, the alpha test and the trilinear
+    chain, with the light on and the first cascade sampled.  The reference
+    defines sampleShadow nowhere; both sides use this library's definition.
+    Depth and all three u16 planes bit for bit."""
+    sc = S.scene_normal(seed=seed)
+    view = S.default_view(160, 120, pos=pos)
+    fr, smaps = O.render(sc, view)
+    rd = O.RefDraw(sc, view)
+    for k in range(len(sc.shadows)):
+        rc, m = rd.shadow_map(k)
+        assert rc == 0 and np.array_equal(m.view(np.uint32), smaps[k].view(np.uint32))
+    rd.clear_zbuffer()
+    assert rd.draw_all() == 0
+    r, g, b, db = rd.get_frame()
+    covered = fr.cov.astype(bool)
+    assert covered.sum() > 2000, "the scene covers the frame"
+    for gi in range(len(sc.groups)):
+        base = sum(x.ntris for x in sc.groups[:gi])
+        assert ((fr.tri_id >= base) & (fr.tri_id < base + sc.groups[gi].ntris)).any(), f"group {gi} visible"
+    assert np.array_equal(db.view(np.uint32), fr.db.view(np.uint32)), "depth differs"
+    for n, a, o in (("r", r, fr.ro), ("g", g, fr.go), ("b", b, fr.bo)):
+        d = int((a != o).sum())
+        assert d == 0, f"{n}: {d} px differ (max {int(np.abs(a.astype(int) - o).max())})"
