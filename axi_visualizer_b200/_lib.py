@@ -25,7 +25,7 @@ EXPORTS = [
     "axr_batch_set_tuning", "axr_set_tuning", "axr_batch_query", "axr_batch_read_async", "axr_batch_bytes",
     "axr_clear_color", "axr_batch_phase_times", "axr_batch_set_mode", "axr_read_frame_async", "axr_wait_frame",
     "axr_frame_done", "axr_batch_inject_barrier_stall", "axr_read_frame_rgb8_async", "axr_set_shadow_mode",
-    "axr_shadow_stats", "axr_last_queues",
+    "axr_shadow_stats", "axr_last_queues", "axr_add_normal_map", "axr_set_normal_material",
 ]
 
 
@@ -93,6 +93,8 @@ _SIGS = {
     "axr_set_shadow_mode": (i32, [vp, i32, i32]),
     "axr_shadow_stats": (i32, [vp, i32, C.POINTER(C.c_int64), i32]),
     "axr_last_queues": (i32, [vp, C.POINTER(C.c_int64), i32]),
+    "axr_add_normal_map": (i32, [vp, vp, C.c_long, C.POINTER(i32)]),
+    "axr_set_normal_material": (i32, [vp, i32, i32, f32, i32]),
     "axr_batch_query": (i32, [vp]),
     "axr_batch_read_async": (i32, [vp, i32, vp, vp, vp, vp]),
     "axr_batch_bytes": (i32, [vp, C.POINTER(C.c_int64)]),

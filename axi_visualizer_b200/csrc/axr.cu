@@ -52,6 +52,14 @@ struct Group {
   int ntris = 0, tri_base = 0, tex_size = 0, mip_side = 0;
   long ntexels = 0;
   float mip_bias = 0.f;       // mipBias of the trilinear level selection (axr_set_mip_bias)
+  int nmap = -1;              // normal map of the normal-mapped materials (axr_set_normal_material)
+  float roughness = 0.f;
+  int metal = 0;
+};
+
+struct NormalMap {
+  uchar4 *texels = nullptr;   // (R, G, B, unused)
+  long n = 0;
 };
 
 struct Alpha {
@@ -107,6 +115,7 @@ struct axr_ctx {
   cudaEvent_t ev_setup = nullptr, ev_coarse = nullptr, ev_alpha = nullptr;
   std::vector<Group> groups;
   std::vector<Alpha> alphas;
+  std::vector<NormalMap> nmaps;
   int total_tris = 0;
   float sscale = 1, cax = 1, cay = 1;
   float pos[3] = {0, 0, 0};
@@ -411,6 +420,24 @@ int grid_for(axr_ctx *c, long n, int block, int per_sm) {
 }
 
 // Builds the per-call group table (host copy).
+// float -> int as the kernels convert (truncation, saturation, NaN -> 0)
+int host_f2i(float x) {
+  if (x != x) return 0;
+  if (x >= 2147483648.0f) return INT_MAX;
+  if (x <= -2147483648.0f) return INT_MIN;
+  return (int)x;
+}
+
+// The specular powers of av_draw_normmap.c:127-146 for a roughness, the same
+// for every pixel of a draw: int specPow = exp2(12*(1.f - roughness)) and
+// (int)half_sqrt((float)specPow), exp2 and half_sqrt correctly rounded
+// (the double result rounded once; sqrtf).
+void normal_powers(float roughness, int &p, int &p2) {
+  float e = 12.f * (1.f - roughness);
+  p = host_f2i((float)exp2((double)e));
+  p2 = host_f2i(sqrtf((float)p));
+}
+
 int group_table(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, const uint8_t *enabled_mask,
                 bool mask_means_enabled, int ngroups, GroupDev *tab) {
   memset(tab, 0, sizeof(GroupDev) * MAX_GROUPS);
@@ -438,6 +465,20 @@ int group_table(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, co
         if (c->groups[g + k].ntexels < (long)G.tex_size * G.tex_size)
           return fail(AXR_EINVAL, "group %d: texture of group %d has fewer than %d x %d texels", g, g + k,
                       G.tex_size, G.tex_size);
+    }
+    if (d.flags & F_NORMAL) {
+      // av_draw_normmap*.c: the normal map is tapped at the texture's texel
+      // indices; the alpha-tested variant has no mip level (Ops.py:772-805)
+      if ((d.flags & F_MULTI) || ((d.flags & F_ALPHA) && (d.flags & F_MIP)))
+        return fail(AXR_EINVAL, "group %d: the normal-mapped material combines with either alpha or mip, not multi", g);
+      if (G.nmap < 0 || G.nmap >= (int)c->nmaps.size())
+        return fail(AXR_ESTATE, "group %d: normal-mapped material with no normal map set", g);
+      if (c->nmaps[G.nmap].n < G.ntexels)
+        return fail(AXR_EINVAL, "group %d: normal map has %ld texels, the texture %ld", g, c->nmaps[G.nmap].n,
+                    G.ntexels);
+      d.nm = c->nmaps[G.nmap].texels;
+      normal_powers(G.roughness, d.spec_pow, d.spec_pow2);
+      d.is_metal = G.metal ? 1 : 0;
     }
     if ((d.flags & F_MIP) && G.mip_side == 0)
       return fail(AXR_EINVAL, "group %d: mip flag on a group added without a mip chain", g);
@@ -561,6 +602,7 @@ int axr_destroy(axr_ctx *c) {
     cudaFree(g.tex);
   }
   for (auto &a : c->alphas) { cudaFree(a.mask); cudaFree(a.quad); }
+  for (auto &m : c->nmaps) cudaFree(m.texels);
   for (auto &sm : c->shadows) {
     if (sm.st) { cudaStreamSynchronize(sm.st); cudaStreamDestroy(sm.st); }
     if (sm.ev_write) cudaEventDestroy(sm.ev_write);
@@ -857,6 +899,30 @@ int axr_add_tex_alpha(axr_ctx *c, const uint8_t *mask, int side, int *out_id) {
   return 0;
 }
 
+int axr_add_normal_map(axr_ctx *c, const uint8_t *rgba, long ntexels, int *out_id) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!rgba || ntexels < 1) return fail(AXR_EINVAL, "normal map of %ld texels", ntexels);
+  NormalMap m;
+  m.n = ntexels;
+  if ((rc = upload(c, &m.texels, reinterpret_cast<const uchar4 *>(rgba), (size_t)ntexels))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->nmaps.push_back(m);
+  if (out_id) *out_id = (int)c->nmaps.size() - 1;
+  return 0;
+}
+
+int axr_set_normal_material(axr_ctx *c, int group, int map, float roughness, int metal) {
+  if (!c) return fail(AXR_EINVAL, "null handle");
+  if (group < 0 || group >= (int)c->groups.size()) return fail(AXR_EINVAL, "group %d out of range", group);
+  if (map < -1 || map >= (int)c->nmaps.size()) return fail(AXR_EINVAL, "normal map %d out of range", map);
+  Group &G = c->groups[group];
+  G.nmap = map;
+  G.roughness = roughness;
+  G.metal = metal ? 1 : 0;
+  return 0;
+}
+
 int axr_set_primary_light(axr_ctx *c, const float i[3], const float d[3]) {
   if (!c || !i || !d) return fail(AXR_EINVAL, "null argument");
   memcpy(c->lint, i, sizeof c->lint);
@@ -907,10 +973,11 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   if ((rc = settle_next(c))) return rc;
   DrawParams P;
   memset(&P, 0, sizeof P);
-  bool any_shadow = false, any_alpha = false;
+  bool any_shadow = false, any_alpha = false, any_normal = false;
   for (int g = 0; g < ngroups; g++) {
     if ((!mask || !mask[g]) && flags && (flags[g] & F_SHADOW)) any_shadow = true;
     if ((!mask || !mask[g]) && flags && (flags[g] & F_ALPHA)) any_alpha = true;
+    if ((!mask || !mask[g]) && flags && (flags[g] & F_NORMAL)) any_normal = true;
   }
   P.nsh = nshadow;
   for (int k = 0; k < nshadow; k++) {
@@ -967,7 +1034,11 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   // shading samples the cascades: wait for their last writers
   for (int k = 0; k < nshadow; k++) CK(cudaStreamWaitEvent(s, c->shadows[shadow_ids[k]].ev_write, 0));
   dim3 sb(256), sgd((c->w + 15) / 16, (c->h + 15) / 16);   // a 16x16 tile per block
-  launch(c, s, "k_shade", [&] { k_shade<<<sgd, sb, 0, s>>>(P); }); nk++;
+  if (any_normal)
+    launch(c, s, "k_shade", [&] { k_shade<true><<<sgd, sb, 0, s>>>(P); });
+  else
+    launch(c, s, "k_shade", [&] { k_shade<false><<<sgd, sb, 0, s>>>(P); });
+  nk++;
   for (int k = 0; k < nshadow; k++) CK(cudaEventRecord(c->shadows[shadow_ids[k]].ev_read, s));
   CK(cudaGetLastError());
   int slot = 1 - c->last_slot;

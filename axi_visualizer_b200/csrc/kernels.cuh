@@ -1281,7 +1281,21 @@ struct RowState {
   Attr<true> c1, c2;
   float fmip;
   int mip, g;
+  V3 tan, bit;   // F_NORMAL: the triangle's tangent frame
 };
+
+// shader_setup of the normal-mapped sources (av_draw_normmap.c:24-38): the
+// tangent frame from the sorted vertices' uv and position divided by z
+// (before the round trip multiplies them back)
+__device__ __noinline__ void normal_frame(const Attr<true> a[3], const float z[3], V3 &tan, V3 &bit) {
+  V2 uv1 = div2(a[0].uv, z[0]), uv2 = div2(a[1].uv, z[1]), uv3 = div2(a[2].uv, z[2]);
+  V3 p1 = div3(a[0].p, z[0]), p2 = div3(a[1].p, z[1]), p3 = div3(a[2].p, z[2]);
+  V2 dUV1 = sub2(uv2, uv1), dUV2 = sub2(uv3, uv1);
+  V3 dPos1 = sub3(p2, p1), dPos2 = sub3(p3, p1);
+  float rdet = 1.f / (dUV1.x * dUV2.y - dUV1.y * dUV2.x);
+  tan = fast_normalize(mul3(sub3(mul3(dPos1, dUV2.y), mul3(dPos2, dUV1.y)), rdet));
+  bit = fast_normalize(mul3(sub3(mul3(dPos2, dUV1.x), mul3(dPos1, dUV2.x)), rdet));
+}
 
 // Replays `steps` rows of the two edge chains (add: downwards, else upwards)
 // and stores them in st: edge 0 the first chain (cx1, cz1, c1), edge 1 the
@@ -1319,7 +1333,10 @@ __device__ __forceinline__ void replay_edges(int edge, int steps, bool add, floa
 }
 
 // The row state of winner `ord` on row cy: the edge chain(s) `edge` selects
-// (see replay_edges) and, for edge 0 or 2, the mip level and group.
+// (see replay_edges) and, for edge 0 or 2, the mip level, group and (NRM,
+// F_NORMAL groups) the tangent frame.  NRM = false: draws without
+// normal-mapped groups, whose shade then carries none of that code.
+template <bool NRM = true>
 __device__ __forceinline__ void shade_row_edge(const DrawParams &P, const GroupDev *sg, uint32_t ord, int cy, int edge,
                                                RowState &st) {
   uint32_t o = ord - 1;
@@ -1342,6 +1359,7 @@ __device__ __forceinline__ void shade_row_edge(const DrawParams &P, const GroupD
     ix[k] = f2i(sx[k]); iy[k] = f2i(sy[k]);
   }
   const bool mip = (G.flags & F_MIP) != 0;
+  const bool normal = NRM && (G.flags & F_NORMAL) != 0;
   MipSel ms;
   ms.fmip = 0; ms.mip = 0; ms.len_mip = 1; ms.len_mip2 = 2; ms.start_mip = 0; ms.start_mip2 = 1;
   float cx1, cx2, cz1, cz2;
@@ -1357,6 +1375,10 @@ __device__ __forceinline__ void shade_row_edge(const DrawParams &P, const GroupD
     float x4 = (float)x1 + yd * (float)(x3 - x1);
     float z4 = z1 + yd * (z3 - z1);
     Attr<true> a4 = a_add(a[0], a_smul(yd, a_sub(a[2], a[0])));
+    if (normal) {
+      if (edge != 1) normal_frame(a, z, st.tan, st.bit);
+      if (!mip) mip_attr_roundtrip<true>(a, z);
+    }
     if (mip) ms = mip_setup<true>(a, z, true, ix, iy, nullptr, nullptr, G.tex_size, G.mip_bias);
     float s1, s2, sz1, sz2;
     Attr<true> sa1, sa2;
@@ -1389,6 +1411,10 @@ __device__ __forceinline__ void shade_row_edge(const DrawParams &P, const GroupD
     float x4 = x1 + yd * (x3 - x1);
     float z4 = z1 + yd * (z3 - z1);
     Attr<true> a4 = a_add(a[0], a_smul(yd, a_sub(a[2], a[0])));
+    if (normal) {
+      if (edge != 1) normal_frame(a, z, st.tan, st.bit);
+      if (!mip) mip_attr_roundtrip<true>(a, z);
+    }
     if (mip) {
       if (P.mipc) {
         mip_attr_roundtrip<true>(a, z);
@@ -1476,7 +1502,134 @@ __device__ __forceinline__ void shade_multi(const DrawParams &P, const GroupDev 
   P.db[pix] = tz;
 }
 
+// pown(x, n), n >= 0, by repeated squaring (the convention pinned for
+// OpenCL's pown, whose rounding the device chooses)
+__device__ __forceinline__ float pown_rs(float x, int n) {
+  unsigned k = n < 0 ? 0u - (unsigned)n : (unsigned)n;
+  float r = 1.0f, b = x;
+  while (k) {
+    if (k & 1u) r *= b;
+    b *= b;
+    k >>= 1;
+  }
+  return n < 0 ? 1.0f / r : r;
+}
+
+// sampleShadow of the normal-mapped sources, which the reference calls but
+// defines nowhere, as this library defines it: the five taps of one cascade
+// (centre, +-2 texels in x and y) at the truncated map position, counted
+// where the map is nearer than `depth`, only when the centre lies in
+// [2, 2 wS - 2) on both axes; the shadowed fraction is count * 0.2.
+__device__ __forceinline__ float sample_shadow5(const ShadowDev &s, float depth, float sfx, float sfy) {
+  int wS = s.dim / 2;
+  int sx = f2i(sfx), sy = f2i(sfy), n = 0;
+  if (sx >= 2 && sx < 2 * wS - 2 && sy >= 2 && sy < 2 * wS - 2) {
+    const float *SD = s.map;
+    int r = 2 * wS;
+    if (__ldg(SD + r * sy + sx) < depth) n += 1;
+    if (__ldg(SD + r * (sy + 2) + sx) < depth) n += 1;
+    if (__ldg(SD + r * (sy - 2) + sx) < depth) n += 1;
+    if (__ldg(SD + r * sy + (sx + 2)) < depth) n += 1;
+    if (__ldg(SD + r * sy + (sx - 2)) < depth) n += 1;
+  }
+  return (float)n * 0.2f;
+}
+
+// bilinear normal-map texel at the taps (texi1*texi2*convert_float3(NM[tex]) + ...)
+__device__ __forceinline__ V3 bilerp_nm(const Taps &q, const uchar4 *__restrict__ NM) {
+  uchar4 a = __ldg(NM + q.tex), b = __ldg(NM + q.tex10), c = __ldg(NM + q.tex01), d = __ldg(NM + q.tex11);
+  float w00 = q.texi1 * q.texi2, w10 = q.texr1 * q.texi2, w01 = q.texi1 * q.texr2, w11 = q.texr1 * q.texr2;
+  V3 r;
+  r.x = w00 * (float)a.x + w10 * (float)b.x + w01 * (float)c.x + w11 * (float)d.x;
+  r.y = w00 * (float)a.y + w10 * (float)b.y + w01 * (float)c.y + w11 * (float)d.y;
+  r.z = w00 * (float)a.z + w10 * (float)b.z + w01 * (float)c.z + w11 * (float)d.z;
+  return r;
+}
+
+// The normal-mapped fragment cores: av_draw_normmap.c:47-149 (its alpha
+// variant after the visibility pass's alpha test) and, with F_MIP,
+// av_draw_normmap_mip.c:73-160.  The light comes from the draw's first
+// cascade (sample_shadow5), 1 without one.  Kept out of line so that the
+// other materials keep their registers.
+__device__ __noinline__ void shade_normal(const DrawParams &P, const GroupDev &G, size_t pix, float t, float tz,
+                                          V2 uvi, const RowState &st, MipSel ms) {
+  const bool mip = (G.flags & F_MIP) != 0;
+  float omt = 1 - t;
+  Taps q = make_taps(uvi, tz, mip ? ms.len_mip : G.tex_size, mip ? ms.start_mip : 0);
+  V3 c = bilerp_rgb(q, G.tex);
+  float outR = c.x, outG = c.y, outB = c.z;
+  V3 tg = bilerp_nm(q, G.nm);
+  if (mip) {
+    Taps q2 = make_taps(uvi, tz, ms.len_mip2, ms.start_mip2);
+    float ofm = 1 - ms.fmip;
+    V3 c2 = bilerp_rgb(q2, G.tex);
+    outR = ofm * outR + ms.fmip * c2.x;
+    outG = ofm * outG + ms.fmip * c2.y;
+    outB = ofm * outB + ms.fmip * c2.z;
+    tg = add3(smul3(ofm, tg), smul3(ms.fmip, bilerp_nm(q2, G.nm)));
+  }
+  float light = 1;
+  if (P.nsh > 0) {
+    const ShadowDev &sh = P.sh[0];
+    V3 pos = sub3(mul3(add3(smul3(omt, st.c2.p), smul3(t, st.c1.p)), tz), V3{sh.pos[0], sh.pos[1], sh.pos[2]});
+    float depth = dot3(pos, V3{sh.vv[0], sh.vv[1], sh.vv[2]});
+    float wS = (float)(sh.dim / 2);
+    float sfx = (dot3(pos, V3{sh.vv[3], sh.vv[4], sh.vv[5]}) * sh.scale) + wS;
+    float sfy = (dot3(pos, V3{sh.vv[6], sh.vv[7], sh.vv[8]}) * -sh.scale) + wS;
+    light = 1 - sample_shadow5(sh, depth, sfx, sfy);
+  } else {
+    light = 1 - 0.f;
+  }
+  V3 col = mul3(add3(smul3(omt, st.c2.li), smul3(t, st.c1.li)), tz);
+  V3 norm = fast_normalize(mul3(add3(smul3(omt, st.c2.n), smul3(t, st.c1.n)), tz));
+  tg = sub3(mul3(div3(tg, 255.f), 2.f), V3{1.f, 1.f, 1.f});
+  tg = fast_normalize(tg);
+  norm = fast_normalize(add3(add3(smul3(tg.z, norm), smul3(-tg.y, st.tan)), smul3(-tg.x, st.bit)));
+  V3 vp{P.view.pos[0], P.view.pos[1], P.view.pos[2]};
+  V3 lint{P.light.lint[0], P.light.lint[1], P.light.lint[2]};
+  V3 ldir{P.light.ldir[0], P.light.ldir[1], P.light.ldir[2]};
+  V3 pos = mul3(add3(smul3(omt, st.c2.p), smul3(t, st.c1.p)), tz);
+  V3 spec;
+  if (mip) {
+    V3 a = sub3(pos, vp);
+    V3 h = fast_normalize(add3(fast_normalize(a), ldir));
+    float theta = fmaxf(0.f, dot3(h, norm));
+    float mf = (float)ms.mip + ms.fmip;
+    int sp = f2i(1.f * (mf * mf));
+    spec = smul3(((pown_rs(theta, sp) * 256.f) * light) * 2.f, lint);
+    spec = mul3(spec, (float)(sp + 1) / (2.f * 3.1416f));
+  } else {
+    V3 a = fast_normalize(sub3(pos, vp));
+    V3 h = fast_normalize(add3(a, ldir));
+    float theta = fmaxf(0.f, dot3(h, norm));
+    int sp = G.spec_pow;
+    spec = smul3(((pown_rs(theta, sp) * 256.f) * 4.f) * light, lint);
+    spec = mul3(spec, (float)(sp + 2) / (8.f * 3.1416f));
+    a = sub3(pos, vp);
+    float nd = dot3(a, norm);
+    V3 refl = fast_normalize(sub3(a, smul3(2.f * nd, norm)));
+    theta = fmaxf(0.f, dot3(refl, V3{0.f, 1.f, 0.f}));
+    spec = add3(spec, smul3((pown_rs(theta, 2) * 128.f) * (float)(1 + G.is_metal), V3{0.1f, 0.3f, 0.5f}));
+    theta = fmaxf(0.f, dot3(fast_normalize(a), refl));
+    spec = add3(spec, smul3(pown_rs(theta, G.spec_pow2) * 256.f, V3{0.2f, 0.2f, 0.2f}));
+    if (G.is_metal) {
+      ushort4 tx = __ldg(G.tex + q.tex);
+      spec.x *= (float)tx.x / 1024.f;
+      spec.y *= (float)tx.y / 1024.f;
+      spec.z *= (float)tx.z / 1024.f;
+      light = 0.f;
+      col = V3{0.f, 0.f, 0.f};
+    }
+  }
+  V3 dc = smul3(fmaxf(0.f, dot3(norm, ldir)), lint);
+  P.ro[pix] = u16sat(spec.x + outR * (light * dc.x + col.x));
+  P.go[pix] = u16sat(spec.y + outG * (light * dc.y + col.y));
+  P.bo[pix] = u16sat(spec.z + outB * (light * dc.z + col.z));
+  P.db[pix] = tz;
+}
+
 // Shades pixel ax of row cy from its winner's row state.
+template <bool NRM = true>
 __device__ __forceinline__ void shade_from_row(const DrawParams &P, const GroupDev *sg, int ax, int cy,
                                                const RowState &st) {
   const GroupDev &G = sg[st.g];
@@ -1495,6 +1648,10 @@ __device__ __forceinline__ void shade_from_row(const DrawParams &P, const GroupD
   V2 uvi = add2(smul2(omt, c2.uv), smul2(t, c1.uv));
   if (G.flags & F_MULTI) {                 // the group table clears F_MULTI on alpha-tested groups
     shade_multi(P, &G, (size_t)P.view.w * cy + ax, t, tz, uvi, st);
+    return;
+  }
+  if (NRM && (G.flags & F_NORMAL)) {
+    shade_normal(P, G, (size_t)P.view.w * cy + ax, t, tz, uvi, st, ms);
     return;
   }
   float outR, outG, outB;
@@ -1557,7 +1714,7 @@ struct ShadeSmem {
 // row (one edge chain each), then every pixel shades from its pair's row
 // state.  The arithmetic is shade_pixel's, done once per pair instead of once
 // per pixel.
-template <int NT>
+template <int NT, bool NRM = true>
 __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *sg, int x0, int y0, ShadeSmem<NT> &sm) {
   const unsigned long long EMPTY = ~0ull;
   int tid = threadIdx.x;
@@ -1592,21 +1749,23 @@ __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *
   int ne = sm.nent;
   for (int j = tid; j < 2 * ne; j += NT) {   // two threads a pair, one edge chain each
     unsigned long long k = sm.ekey[j >> 1];
-    shade_row_edge(P, sg, (uint32_t)(k >> 32), (int)(uint32_t)k, j & 1, sm.rs[j >> 1]);
+    shade_row_edge<NRM>(P, sg, (uint32_t)(k >> 32), (int)(uint32_t)k, j & 1, sm.rs[j >> 1]);
   }
   __syncthreads();
-  if (valid) shade_from_row(P, sg, ax, cy, sm.rs[sm.hent[slot]]);
+  if (valid) shade_from_row<NRM>(P, sg, ax, cy, sm.rs[sm.hent[slot]]);
   __syncthreads();                       // the next tile reuses the shared memory
 }
 
 
 // one 256-thread block per 16x16 tile
+// NRM: the draw has normal-mapped groups
+template <bool NRM>
 __global__ void __launch_bounds__(256, 4) k_shade(DrawParams P) {   // 64 registers: 4 blocks per SM
   __shared__ GroupDev sg[64];
   __shared__ ShadeSmem<256> sm;
   for (int i = threadIdx.x; i < P.ngroups; i += blockDim.x) sg[i] = P.groups[i];
   __syncthreads();
-  shade_tile<256>(P, sg, blockIdx.x * TILE, blockIdx.y * TILE, sm);
+  shade_tile<256, NRM>(P, sg, blockIdx.x * TILE, blockIdx.y * TILE, sm);
 }
 
 __global__ void k_ids(const uint64_t *__restrict__ keys, int n, int32_t *tri_id, uint8_t *cov) {

@@ -14,8 +14,10 @@
 
 namespace axr {
 
-// F_MULTI: av_draw_multi.c's 4-way blend with the next three groups' textures
-enum { F_MIP = 1, F_ALPHA = 2, F_SHADOW = 4, F_CULL = 8, F_MULTI = 16 };
+// F_MULTI: av_draw_multi.c's 4-way blend with the next three groups' textures;
+// F_NORMAL: the normal-mapped materials (av_draw_normmap.c, with F_ALPHA
+// av_draw_normmap_alpha.c, with F_MIP av_draw_normmap_mip.c)
+enum { F_MIP = 1, F_ALPHA = 2, F_SHADOW = 4, F_CULL = 8, F_MULTI = 16, F_NORMAL = 32 };
 constexpr int TILE = 16;
 constexpr int SMALL_THRESH = 6;
 constexpr unsigned FULL = 0xffffffffu;
@@ -30,6 +32,12 @@ struct GroupDev {
   float mip_bias;
   int enabled;
   int pad_;
+  // F_NORMAL: normal map (R, G, B, unused) with one texel per texel of the
+  // texture or chain; the specular powers (int)exp2(12 (1 - roughness)) and
+  // (int)sqrt of it; the metal switch
+  const uchar4 *nm;
+  int spec_pow, spec_pow2, is_metal;
+  int pad2_;
 };
 
 struct ViewDev {

@@ -59,6 +59,8 @@ class CLDraw:
         self.texSize = []
         self._mip_bias = []       # mipBias per group, as the library holds it
         self._set_bias = []       # mipBias per group given by setMipBias (0 until set)
+        self.NM = {}              # normal maps by name (reference name), library ids
+        self._normal = {}         # group -> (map id, roughness, metal) as the library holds it
         self._tex_alpha = 0
         self.SHADOWMAP = {}
         self.ambLight = np.float32(0.2)
@@ -217,6 +219,42 @@ class CLDraw:
         check(self._L.axr_add_tex_alpha(self._h, _p(m), side, C.byref(out)), "addTexAlpha")
         return out.value
 
+    def addNrmMap(self, rgb, name, mip=False):
+        """CLDraw.addNrmMap(rgb, name) (Ops.py:299-302): an (N, N, 3) uint8
+        normal map (or RGBA bytes already laid out, one texel per texel of
+        the textures it is used with).  mip=True stores its createMips chain,
+        smallest level first, for the normal-mapped mip material."""
+        a = np.asarray(rgb)
+        if a.ndim == 3:
+            from .scenes import create_mips
+            flat = create_mips(a[..., :3]) if mip else a[..., :3].reshape(-1, 3)
+            out4 = np.zeros((flat.shape[0], 4), np.uint8)
+            out4[:, :3] = flat
+            a = out4
+        b = np.ascontiguousarray(a, np.uint8).reshape(-1)
+        if b.size % 4:
+            raise AxrError("addNrmMap: expected (N, N, 3) bytes or RGBA bytes")
+        out = C.c_int()
+        check(self._L.axr_add_normal_map(self._h, _p(b), b.size // 4, C.byref(out)), "addNrmMap")
+        self.NM[name] = out.value
+        return out.value
+
+    def _draw_normal_materials(self, shaders):
+        """The normal-mapped dict materials of one draw ({"normal": (name,
+        roughness), "metal": ...}, Ops.py:669-699) to the library."""
+        items = shaders.items() if isinstance(shaders, dict) else enumerate(shaders)
+        for i, sh in items:
+            if not (isinstance(sh, dict) and "normal" in sh):
+                continue
+            name, rough = sh["normal"][0], sh["normal"][1]
+            if name not in self.NM:
+                raise AxrError(f"drawAll: normal map {name!r} was not added")
+            want = (self.NM[name], float(np.float32(rough)), int("metal" in sh and bool(sh["metal"])))
+            if self._normal.get(int(i)) != want:
+                check(self._L.axr_set_normal_material(self._h, int(i), want[0], C.c_float(want[1]), want[2]),
+                      "setNormalMaterial")
+                self._normal[int(i)] = want
+
     def setPrimaryLight(self, dirI, dirD):
         i = _f32(np.asarray(dirI).reshape(-1, 3)[0])
         d = _f32(np.asarray(dirD).reshape(-1, 3)[0])
@@ -274,6 +312,7 @@ class CLDraw:
     def drawAll(self, shaders, mask=None, shadowIds=(0, 1), useOpacitySM=False):
         flags, aidx = self._material_args(shaders)
         self._draw_mip_biases(shaders)
+        self._draw_normal_materials(shaders)
         m = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
         ids = [int(i) for i in shadowIds if int(i) in self.SHADOWMAP][:2]
         sid = np.asarray(ids + [0, 0], np.int32)[:2]
@@ -484,9 +523,12 @@ class CLDraw:
                     "setBoneTransform", "boneTransform", "setupWave", "updateWave",
                     "highlight", "drawDirectional", "getGIM", "addOpacityMap", "clearShadowOpMap",
                     "shadowClouds", "shadowCloudsOpacity", "tonemap", "mipShadowMap", "setPSTex", "drawPS",
-                    "addNrmMap", "addRghMap", "getBoneWeights", "initBoneOrigin", "invbt", "genVoxels",
+                    "getBoneWeights", "initBoneOrigin", "invbt", "genVoxels",
                     "getVoxels", "voxCopy", "voxLight", "voxTerrain"):
             raise NotImplementedError(f"CLDraw.{name} belongs to an effect outside the rasterizer hot path")
+        if name == "addRghMap":
+            raise NotImplementedError("CLDraw.addRghMap: only the normal_mip dispatch passes a roughness map "
+                                      "(Ops.py:683), and its kernel source av_draw_normmap_mip.c takes none")
         if name in ("exposure", "blurTest"):
             raise NotImplementedError(f"CLDraw.{name} runs a kernel file the reference snapshot does not ship")
         if name in ("getBuffers", "getShadow", "getArgs"):
@@ -521,10 +563,22 @@ class SceneRenderer:
         for k, g in enumerate(scene.groups):
             if g.mip_bias:
                 self.draw.setMipBias(k, g.mip_bias)
-        # the mipBias goes through setMipBias; a dict's "mip" is a flag
+        # the mipBias goes through setMipBias; a dict's "mip" is a flag,
+        # except in the normal-mapped mip material, which carries its bias
         self.shaders = [{"alpha": g.alpha_index, **{k: 1 for k, b in names if g.flags & b}} if g.flags & 2 else
                         " ".join(k for k, b in names if g.flags & b)
                         for g in scene.groups]
+        for k, g in enumerate(scene.groups):
+            if g.flags & 32:              # scenes.NORMAL
+                self.draw.addNrmMap(g.nm, f"group{k}")
+                sh = {"normal": (f"group{k}", g.roughness), **{n: 1 for n, b in names if g.flags & b}}
+                if g.flags & 2:
+                    sh["alpha"] = g.alpha_index
+                if g.metal:
+                    sh["metal"] = 1
+                if g.flags & 1:
+                    sh["mip"] = np.float32(g.mip_bias)
+                self.shaders[k] = sh
 
     def shadow_pass(self):
         for k in range(len(self.scene.shadows)):

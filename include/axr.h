@@ -126,6 +126,23 @@ int axr_copy_to(axr_ctx *ctx, int group, const float *xyz, const float *vn, int 
 /* CLDraw.addTexAlpha(a) (Ops.py:454-456): boolean alpha mask side x side. */
 int axr_add_tex_alpha(axr_ctx *ctx, const uint8_t *mask, int side, int *out_id);
 
+/* CLDraw.addNrmMap(rgb, name) (Ops.py:299-302): a normal map of ntexels
+ * texels as RGBA bytes (the reference's align34 layout; A unused), one
+ * texel per texel of the textures it is used with (a full chain, smallest
+ * level first, for the mip variant).  Returns its id. */
+int axr_add_normal_map(axr_ctx *ctx, const uint8_t *rgba, long ntexels, int *out_id);
+
+/* The normal-mapped materials of group `group` (material flag 32, the
+ * reference's dict material {"normal": (name, roughness), "metal": ...},
+ * Ops.py:669-699, 772-805): its normal map (-1: none), roughness and metal
+ * switch.  A drawAll of the material needs a normal map with at least as
+ * many texels as the group's texture.  It combines with alpha
+ * (av_draw_normmap_alpha.c) or mip (av_draw_normmap_mip.c, whose
+ * arguments carry no roughness or metal), not both; its sampleShadow,
+ * which the reference defines nowhere, counts the five taps of the draw's
+ * first cascade (0.2 each). */
+int axr_set_normal_material(axr_ctx *ctx, int group, int map, float roughness, int metal);
+
 /* CLDraw.setPrimaryLight(dirI, dirD) (Ops.py:1143-1151) */
 int axr_set_primary_light(axr_ctx *ctx, const float dir_int[3], const float dir_dir[3]);
 

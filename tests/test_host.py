@@ -78,24 +78,31 @@ def test_mip_bias_per_draw_as_the_reference_passes_it():
             calls.append(("bias", tn, float(b.value)))
             return 0
 
+        def axr_set_normal_material(self, h, tn, m, r, metal):
+            calls.append(("normal", tn, m, float(r.value), metal))
+            return 0
+
     class Fake:
         gSize = [3, 3, 3, 3]
         SHADOWMAP = {}
+        NM = {0: 7}
         _h = None
         _L = FakeLib()
         _material_args = CLDraw._material_args
         _dict_mip_biases = staticmethod(CLDraw._dict_mip_biases)
         _draw_mip_biases = CLDraw._draw_mip_biases
+        _draw_normal_materials = CLDraw._draw_normal_materials
         _apply_mip_bias = CLDraw._apply_mip_bias
         setMipBias = CLDraw.setMipBias
 
     f = Fake()
+    f._normal = {}
     f._mip_bias = [np.float32(0)] * 4
     f._set_bias = [np.float32(0)] * 4
     shaders = ["mip shadow", {"alpha": 0, "mip": 1}, {"normal": (0, 1.0), "roughness": 0, "mip": 0.5},
                {"alpha": 0}]
     CLDraw.drawAll(f, shaders, shadowIds=[])
-    assert calls == [("bias", 2, 0.5), ("draw",)]
+    assert calls == [("bias", 2, 0.5), ("normal", 2, 7, 1.0, 0), ("draw",)]
     calls.clear()
     CLDraw.drawAll(f, shaders, shadowIds=[])          # unchanged: no library call
     assert calls == [("draw",)]
