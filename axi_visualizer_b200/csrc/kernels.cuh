@@ -105,21 +105,45 @@ __global__ void k_init_keys(const float *__restrict__ db, uint64_t *__restrict__
   for (; i < n; i += gridDim.x * blockDim.x) keys[i] = ((uint64_t)depth_key(db[i]) << 32) | 0xffffffffull;
 }
 
-// clearzb.c:10-22 over lenP x lenP work-items of (w/lenP) x (h/lenP) blocks
+// clearzb.c:10-22 over lenP x lenP work-items of (w/lenP) x (h/lenP)
+// blocks: columns [0, bw) of rows [0, bh) := 65535.  When bw == w those rows
+// are one contiguous range, written with 16-byte stores.
 __global__ void k_clear_depth(float *__restrict__ f, int w, int h, int lenP) {
   int bw = (w / lenP) * lenP, bh = (h / lenP) * lenP;
+  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  if (bw == w && ((uintptr_t)f & 15) == 0) {
+    size_t n = (size_t)w * bh, n4 = n >> 2;
+    const float4 v = make_float4(65535.f, 65535.f, 65535.f, 65535.f);
+    for (size_t i = tid; i < n4; i += stride) reinterpret_cast<float4 *>(f)[i] = v;
+    for (size_t i = (n4 << 2) + tid; i < n; i += stride) f[i] = 65535.f;
+    return;
+  }
   int n = bw * bh;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = (int)tid; i < n; i += (int)stride) {
     int y = i / bw, x = i - y * bw;
     f[(size_t)w * y + x] = 65535.f;
   }
 }
 
 // Colour half of the current reference's clearZBuffer (Ops.py:939-946):
-// every pixel of the three colour planes := (r, g, b).
+// every pixel of the three colour planes := (r, g, b); 16-byte stores when
+// the planes are 16-byte aligned.
 __global__ void k_fill_rgb(uint16_t *__restrict__ ro, uint16_t *__restrict__ go, uint16_t *__restrict__ bo, int n,
                            uint16_t r, uint16_t g, uint16_t b) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  size_t done = 0;
+  if ((((uintptr_t)ro | (uintptr_t)go | (uintptr_t)bo) & 15) == 0) {
+    size_t n8 = (size_t)n >> 3;
+    uint32_t rr = r * 0x10001u, gg = g * 0x10001u, bb = b * 0x10001u;
+    const uint4 vr = make_uint4(rr, rr, rr, rr), vg = make_uint4(gg, gg, gg, gg), vb = make_uint4(bb, bb, bb, bb);
+    for (size_t i = tid; i < n8; i += stride) {
+      reinterpret_cast<uint4 *>(ro)[i] = vr;
+      reinterpret_cast<uint4 *>(go)[i] = vg;
+      reinterpret_cast<uint4 *>(bo)[i] = vb;
+    }
+    done = n8 << 3;
+  }
+  for (size_t i = done + tid; i < (size_t)n; i += stride) {
     ro[i] = r;
     go[i] = g;
     bo[i] = b;
@@ -665,19 +689,19 @@ __device__ __forceinline__ void fill_round(Q &q, int lane, int cnt, F &&pix) {
 }
 
 // Writes lane's span record: row offset cyw, first pixel lo, ends cx1 / cx2.
-// Returns false when the span must be drawn by its own lane (span_queueable).
+// Returns false when the span must be drawn by its own lane (span_queue_form).
 template <bool ALPHA>
 __device__ __forceinline__ bool vis_put(VisQ<ALPHA> &q, int lane, int cyw, int lo, uint32_t ord, float cx1, float cx2,
                                         float cz1, float cz2, V2 cu1, V2 cu2, int g) {
-  float d = cx1 - cx2;
-  float y = span_recip_exact(d, cx2, lo);
-  q.a[lane] = make_float4(cx2, d, y, cz1);
+  float qx, qd, qy;
+  bool ok = span_queue_form(cx2, cx1 - cx2, lo, qx, qd, qy);
+  q.a[lane] = make_float4(qx, qd, qy, cz1);
   q.b[lane] = make_float4(cz2, __int_as_float(cyw + lo), __int_as_float(lo), __uint_as_float(ord));
   if (ALPHA) {
     q.c[lane] = make_float4(cu1.x, cu1.y, cu2.x, cu2.y);
     q.g[lane] = g;
   }
-  return span_queueable(d, y);
+  return ok;
 }
 
 // Per-fragment visibility: alpha test (av_draw_alpha.c:80-97) then the
@@ -1120,7 +1144,7 @@ struct TileLane {
     return live_half;
   }
 
-  // queues the row's span, or draws it with the lane alone (span_queueable);
+  // queues the row's span, or draws it with the lane alone (span_queue_form);
   // returns the pixels queued
   __device__ __forceinline__ int put(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, int lo,
                                      int cnt) {
@@ -2156,15 +2180,14 @@ struct ShadowLane {
       int lo = a0 < 0 ? 0 : a0, hi = a1 > dim - 1 ? dim - 1 : a1;
       cnt = hi >= lo ? hi - lo + 1 : 0;
       if (cnt) {
-        float d = cx1 - cx2;
-        float y = span_recip_exact(d, cx2, lo);
-        q.a[lane] = make_float4(cx2, d, y, cz1);
+        float qx, qd, qy;
+        serial = !span_queue_form(cx2, cx1 - cx2, lo, qx, qd, qy);
+        q.a[lane] = make_float4(qx, qd, qy, cz1);
         q.b[lane] = make_float4(cz2, __int_as_float(cy * dim + lo), __int_as_float(lo), 0.f);
         if (ALPHA) {
           q.c[lane] = make_float4(cu1, cv1, cu2, cv2);
           q.g[lane] = g;
         }
-        serial = !span_queueable(d, y);
       }
     }
     skip_row();
@@ -2193,10 +2216,9 @@ struct ShadowLane {
     }
     serial = false;
     if (cnt) {
-      float d = cx1 - cx2;
-      float y = span_recip_exact(d, cx2, lo);
-      serial = !span_queueable(d, y);   // then the caller draws the span with this lane alone
-      q.a[lane] = make_float4(cx2, d, y, cz1);
+      float qx, qd, qy;
+      serial = !span_queue_form(cx2, cx1 - cx2, lo, qx, qd, qy);   // then the caller draws it with this lane alone
+      q.a[lane] = make_float4(qx, qd, qy, cz1);
       q.b[lane] = make_float4(cz2, __int_as_float((cy - ty0) * TROW + (lo - tx0)), __int_as_float(lo),
                               __int_as_float(floor_bits));
       if (ALPHA) {
@@ -2217,14 +2239,15 @@ struct ShadowLane {
 
 // drawmin.c:71-76 / drawminalpha.c:83-97 for pixel number p of span s: the
 // depth tz, or false when nothing is written (NaN depth, alpha discard)
-template <bool ALPHA, bool DIV = false>
+template <bool ALPHA, bool DIV = false, bool EZ = false>
 __device__ __forceinline__ bool shadow_depth(const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p, float4 b,
-                                             float &tz) {
+                                             float &tz, float cur = 0.f) {
   const float4 a = q.a[s];
   float n = (float)(p + __float_as_int(b.z)) - a.x;
   float t = DIV ? clamp_t(n / a.y) : span_t(n, a.y, a.z);
   tz = __frcp_rn((1 - t) * b.x + t * a.w);
   if (tz != tz) return false;
+  if (EZ && !(cur > tz)) return false;
   if (ALPHA) {
     const float4 c = q.c[s];
     const GroupDev &G = sg[q.g[s]];
@@ -2243,8 +2266,14 @@ __device__ __forceinline__ bool shadow_depth(const GroupDev *sg, const ShadowQ<A
 template <bool ALPHA, bool DIV = false>
 __device__ __forceinline__ void shadow_pixel(float *map, const GroupDev *sg, const ShadowQ<ALPHA> &q, int s, int p) {
   const float4 b = q.b[s];
+  float *addr = map + (size_t)(p + __float_as_int(b.y));
+  // alpha-tested casters read the texel first: one that already holds a
+  // depth <= tz (most of them, behind the opaque casters) skips the mask
+  // lookup.  Texels only decrease, so any value read bounds the final one.
+  float cur = 0.f;
+  if (ALPHA) cur = __ldcg(addr);
   float tz;
-  if (shadow_depth<ALPHA, DIV>(sg, q, s, p, b, tz)) atomic_min_depth(map + (size_t)(p + __float_as_int(b.y)), tz);
+  if (shadow_depth<ALPHA, DIV, ALPHA>(sg, q, s, p, b, tz, cur)) atomic_min_depth(addr, tz);
 }
 
 template <bool ALPHA>

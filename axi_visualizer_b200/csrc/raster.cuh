@@ -137,19 +137,35 @@ __device__ __forceinline__ float quot_fast(float n, float d, float y) {
   return __fmaf_rn(r, y, q);
 }
 
-// t = clamp(n / d, 0, 1) of a pixel of a span queued with its reciprocal y
-// (span_recip_exact).  y != 0: the quotient through the reciprocal.  y == 0
-// is queued only for d = +-0, where n / d is an infinity whose sign is
-// sign(n) xor sign(d) (clamped to 1 or 0), or NaN for n = 0 (clamped to 1),
-// so no pixel of a queued span divides.
+// t = clamp(n / d, 0, 1) of a pixel of a span queued by span_queue_form.
+// The operands are in range there (finite, d and y nonzero), so the
+// quotient is never NaN and the clamp needs no NaN rule.
 __device__ __forceinline__ float span_t(float n, float d, float y) {
-  if (y != 0.f) return clamp_t(quot_fast(n, d, y));
-  return (n == 0.f || ((__float_as_uint(n) ^ __float_as_uint(d)) & 0x80000000u) == 0u) ? 1.f : 0.f;
+  return fmaxf(0.f, fminf(1.f, quot_fast(n, d, y)));
 }
-// Whether every pixel of a span can take span_t: otherwise (a reciprocal out
-// of the safe range with d != 0, which real scenes almost never produce)
-// the span's own lane draws it with the true division.
-__device__ __forceinline__ bool span_queueable(float d, float y) { return y != 0.f || d == 0.f; }
+
+// The (cx2, d, y) a span with first pixel lo is queued with, so that every
+// pixel x of it takes t = span_t(x - cx2, d, y).  Usually (cx2, d, RN(1/d)).
+// d = cx1 - cx2 = +-0 means cx1 and cx2 are equal (or both zero), so the
+// span is the one pixel lo: its n / d is an infinity of sign sign(n) xor
+// sign(d), clamped to 1 or 0, or NaN for n = 0, clamped to 1; that t is
+// fixed here as cx2 = lo - 1 (t = 1) or lo + 1 (t = 0) with d = y = 1.
+// Returns false when a pixel might need the true division (a reciprocal out
+// of the safe range with d != 0, which real scenes almost never produce):
+// the span's own lane then draws it with the true cx2 and d.
+__device__ __forceinline__ bool span_queue_form(float cx2, float d, int lo, float &qx, float &qd, float &qy) {
+  qx = cx2;
+  qd = d;
+  qy = span_recip_exact(d, cx2, lo);
+  if (qy != 0.f) return true;
+  if (d != 0.f) return false;
+  float n = (float)lo - cx2;
+  bool one = n == 0.f || ((__float_as_uint(n) ^ __float_as_uint(d)) & 0x80000000u) == 0u;
+  qx = (float)lo - (one ? 1.f : -1.f);
+  qd = 1.f;
+  qy = 1.f;
+  return true;
+}
 
 __device__ __forceinline__ float quot_by_recip(float n, float d, float y) {
   float an = fabsf(n);
