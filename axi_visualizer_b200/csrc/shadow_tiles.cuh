@@ -333,7 +333,7 @@ __device__ __forceinline__ void tile_units(const ShadowParams &S, const GroupDev
           cnt = 0;
         }
       }
-      fill_round(q, lane, cnt, [&](int s, int p) { tile_pixel<ALPHA>(tile, sg, q, s, p); });
+      fill_round(q, lane, cnt, L.pb, [&](int s, int p) { tile_pixel<ALPHA>(tile, sg, q, s, p); });
     }
   }
 }
