@@ -1002,6 +1002,7 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   P.units = c->units; P.ctr = c->ctr;
   P.cap_list = c->cap_list; P.cap_units = c->cap_units;
   P.min_chunk = c->min_chunk;
+  P.claim_k = 2;
   P.mipc = c->mipc;
   long npix = (long)c->w * c->h;
   cudaStream_t s = c->stream;
@@ -1394,6 +1395,7 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
   memcpy(S.sh.vv, sm.vv, sizeof sm.vv);
   S.map = sm.map; S.bias = bias; S.list = sm.list; S.cap_list = sm.cap; S.ctr = sm.ctr;
   S.min_chunk = c->min_chunk;
+  S.claim_k = 2;
   const size_t nt = (size_t)sm.ntx * sm.ntx;
   if (tiled) {
     S.rec = sm.rec;
@@ -1573,6 +1575,7 @@ struct axr_batch {
   cudaStream_t side = nullptr;  // phased form: the alpha-tested branch
   cudaEvent_t done = nullptr, read_done = nullptr, ev_fork = nullptr, ev_coarse = nullptr, ev_join = nullptr;
   int mode = AXR_BATCH_PERSISTENT;
+  bool shade_nrm = true;   // the shade variant launched (and captured): with the normal-mapped core
   int phantom = 0;                  // fault injection: barrier waits for blocks never launched
   long spin_limit = BARRIER_SPIN_LIMIT;
   bool graph = false, pending = false, reads = false;
@@ -1743,7 +1746,8 @@ int batch_enqueue(axr_batch *b) {
   B.bar = b->d_bar; B.nblocks = (uint32_t)(b->grid + b->phantom); B.spin_limit = b->spin_limit;
   if (b->mode == AXR_BATCH_PERSISTENT) {
     void *args[] = {&B};
-    CK(cudaLaunchCooperativeKernel((const void *)k_batch, dim3(b->grid), dim3(128), args, 0, s));
+    const void *kern = b->shade_nrm ? (const void *)k_batch<true> : (const void *)k_batch<false>;
+    CK(cudaLaunchCooperativeKernel(kern, dim3(b->grid), dim3(128), args, 0, s));
   } else {
     // phased: clear, setup | opaque raster -> tiled opaque | (fork) alpha
     // raster -> (after the coarse units) tiled alpha | (join) fallback, shade
@@ -1761,7 +1765,8 @@ int batch_enqueue(axr_batch *b) {
     kb_tiled<false><<<sms * 8, 128, 0, s>>>(B);
     CK(cudaStreamWaitEvent(s, b->ev_join, 0));
     kb_fallback<<<sms * 4, 128, 0, s>>>(B);
-    kb_shade<<<sms * 4, 256, 0, s>>>(B);
+    if (b->shade_nrm) kb_shade<true><<<sms * 4, 256, 0, s>>>(B);
+    else kb_shade<false><<<sms * 4, 256, 0, s>>>(B);
     CK(cudaGetLastError());
   }
   for (size_t k = 0; k < nv; k++)
@@ -1862,9 +1867,13 @@ int axr_batch_create(axr_ctx *c, const axr_view_desc *views, int nviews, axr_bat
   b->bytes += (int64_t)(sizeof(BatchView) * nviews + 2 * sizeof(GroupDev) * ng + sizeof(uint32_t) * BAR_WORDS);
   if (!rc) rc = batch_alloc(b, units0);
   if (!rc) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, 128, 0) != cudaSuccess || per_sm < 1)
+    // the grid must be co-resident for either shade variant of the kernel
+    int per_sm = 0, per_sm2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<true>, 128, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_batch<false>, 128, 0) != cudaSuccess ||
+        std::min(per_sm, per_sm2) < 1)
       rc = fail(AXR_ECUDA, "batch kernel occupancy");
+    per_sm = std::min(per_sm, per_sm2);
     b->per_sm_max = per_sm;
     b->grid = per_sm * c->sms;
   }
@@ -1942,6 +1951,19 @@ int axr_batch_render(axr_batch *b, const int32_t *flags, const int32_t *alpha_in
     b->goff[k] = seg_off[j];
   }
   batch_fill_views(b);
+  // the shade variant: with the normal-mapped core only when a shaded view
+  // draws such a material (a change rebuilds the captured graph)
+  bool nrm = false;
+  for (auto &v : b->desc) {
+    if (v.kind != AXR_VIEW_SHADED || !flags) continue;
+    int gf, gn;
+    view_range(c, v, gf, gn);
+    for (int g = gf; g < gf + gn; g++) nrm = nrm || (flags[g] & F_NORMAL) != 0;
+  }
+  if (nrm != b->shade_nrm) {
+    b->shade_nrm = nrm;
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  }
   // shaded views sampling the handle's own shadow maps wait for their writers
   for (auto &v : b->desc)
     for (int j = 0; j < v.ncascades; j++)

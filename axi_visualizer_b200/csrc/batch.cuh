@@ -169,8 +169,10 @@ __device__ __forceinline__ void batch_raster(const BatchParams &B, const GroupDe
   }
 }
 
-// phase 4: shading, tile by tile (16 x NT/16 pixels per block and tile)
-template <int NT>
+// phase 4: shading, tile by tile (16 x NT/16 pixels per block and tile);
+// NRM: some view draws a normal-mapped material (else the shade without
+// that core, which runs with fewer registers)
+template <int NT, bool NRM>
 __device__ __forceinline__ void batch_shade(const BatchParams &B, const GroupDev *sgd, ShadeSmem<NT> &sm) {
   constexpr int TH = NT / 16;
   for (int v = 0; v < B.nviews; v++) {
@@ -178,10 +180,11 @@ __device__ __forceinline__ void batch_shade(const BatchParams &B, const GroupDev
     if (V.kind != VIEW_SHADED) continue;
     int tw = (V.w + 15) / 16, th = (V.h + TH - 1) / TH;
     for (int t = blockIdx.x; t < tw * th; t += gridDim.x)
-      shade_tile<NT>(V.dp, sgd + V.goff, (t % tw) * 16, (t / tw) * TH, sm);
+      shade_tile<NT, NRM>(V.dp, sgd + V.goff, (t % tw) * 16, (t / tw) * TH, sm);
   }
 }
 
+template <bool NRM>
 __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   __shared__ GroupDev sgd[BATCH_TABLE], sgs[BATCH_TABLE];
   __shared__ union U { WarpQueue wq[4]; ShadeSmem<128> sh; } u;   // phases 2-3 / phase 4
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(128, 4) k_batch(BatchParams B) {
   if (!grid_sync(B.bar, B.nblocks, B.spin_limit)) return;
   stamp(B.bar, 4);
 
-  batch_shade<128>(B, sgd, u.sh);
+  batch_shade<128, NRM>(B, sgd, u.sh);
   // the last block to finish stamps the end
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -279,12 +282,13 @@ __global__ void __launch_bounds__(128) kb_fallback(BatchParams B) {
   }
 }
 
+template <bool NRM>
 __global__ void __launch_bounds__(256, 4) kb_shade(BatchParams B) {
   __shared__ GroupDev sgd[BATCH_TABLE];
   __shared__ ShadeSmem<256> sm;
   for (int i = threadIdx.x; i < B.ngroups; i += blockDim.x) sgd[i] = B.groups_draw[i];
   __syncthreads();
-  batch_shade<256>(B, sgd, sm);
+  batch_shade<256, NRM>(B, sgd, sm);
 }
 
 }  // namespace axr

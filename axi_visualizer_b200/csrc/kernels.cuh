@@ -42,6 +42,7 @@ struct DrawParams {
   uint32_t *ctr;         // see CTR_*
   uint32_t cap_list, cap_units;
   int min_chunk;         // rows per small-triangle work item (at least; tuning knob)
+  int claim_k;           // claim_size's k for the short queues (0: 32 items per claim)
   float2 *mipc;          // per triangle of a mip group: (mip fraction, mip level), written by
                          // the setup, read by the shade; null: the shade computes them
 };
@@ -99,7 +100,10 @@ __device__ __forceinline__ int small_rows(int y1, int y3) { return y3 - y1 + 2; 
 // same for every warp.  On the 1080p scene this took the alpha-tested
 // tiled raster from 133 to 100 us and the alpha casters from 103 to 92 us;
 // the opaque rasterizers stay at 32 (fewer per claim made them slower).
+// k = 0: always 32 -- the batched launches, whose warps move on to the
+// next view's queue when one runs dry, so no warp idles.
 __device__ __forceinline__ uint32_t claim_size(uint32_t n, uint32_t k) {
+  if (k == 0) return 32u;
   uint32_t nw = gridDim.x * (blockDim.x >> 5) * k;
   uint32_t per = (n + nw - 1) / nw;
   return per < 1u ? 1u : (per > 32u ? 32u : per);
@@ -896,7 +900,7 @@ template <bool ALPHA>
 __device__ __forceinline__ void raster_small_loop(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane) {
   uint32_t n = P.ctr[ALPHA ? CTR_ITEMS_A : CTR_ITEMS];
   uint32_t cap_items = P.cap_list * MAX_CHUNKS;
-  const uint32_t per = ALPHA ? claim_size(n, 2) : 32u;
+  const uint32_t per = ALPHA ? claim_size(n, (uint32_t)P.claim_k) : 32u;
   while (true) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&P.ctr[ALPHA ? CTR_WORK_SMALL_A : CTR_WORK_SMALL], per);
@@ -996,7 +1000,7 @@ __device__ __forceinline__ void coarse_walk(const float sx[3], const float sy[3]
 __device__ __forceinline__ void coarse_loop(const DrawParams &P, const GroupDev *sg, int lane) {
   uint32_t n = P.ctr[CTR_LARGE];
   int wc = P.view.w / TILE, hc = P.view.h / TILE;
-  const uint32_t per = claim_size(n, 1);
+  const uint32_t per = claim_size(n, P.claim_k > 0 ? 1u : 0u);
   while (true) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&P.ctr[CTR_WORK_LARGE], per);
@@ -1211,7 +1215,7 @@ template <bool ALPHA>
 __device__ __forceinline__ void raster_tiled_loop(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane) {
   if (P.ctr[CTR_OVERFLOW]) return;
   uint32_t n = P.ctr[ALPHA ? CTR_UNITS_A : CTR_UNITS];
-  const uint32_t per = ALPHA ? claim_size(n, 2) : 32u;
+  const uint32_t per = ALPHA ? claim_size(n, (uint32_t)P.claim_k) : 32u;
   while (true) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&P.ctr[ALPHA ? CTR_WORK_UNITS_A : CTR_WORK_UNITS], per);
@@ -1839,6 +1843,7 @@ struct ShadowParams {
   uint32_t *items;     // row chunks of the casters, same two ends (cap_list * MAX_CHUNKS);
                        // null: one work item per caster
   int min_chunk;       // rows per chunk (at least)
+  int claim_k;         // claim_size's k (0: 32 items per claim)
   // tiled pass (rec != null): one record per caster at its list position,
   // per-tile unit counts (opaque [0, ntiles), alpha [ntiles, 2 ntiles)),
   // offsets, scatter cursors and claim counters (opaque, alpha per tile),
@@ -2318,7 +2323,7 @@ __device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const Gr
   uint32_t n = chunked ? S.ctr[ALPHA ? CTR_SH_ITEMS_A : CTR_SH_ITEMS] : S.ctr[ctr_list];
   uint32_t cap_items = S.cap_list * MAX_CHUNKS;
   int dim = S.sh.dim;
-  const uint32_t per = claim_size(n, 2);
+  const uint32_t per = claim_size(n, (uint32_t)S.claim_k);
   while (true) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&S.ctr[ctr_work], per);
