@@ -36,15 +36,30 @@ W, H = 1920, 1080
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
-# each kernel on this workload: (bytes, the summary under profiles/ that
-# gives the capture).  A kernel changed since its capture has no entry.
+# From the ncu capture summarised in profiles/ncu_kernels_1080p_1m.md (the
+# same frame, one launch per kernel, both cascades averaged for the shadow
+# kernels, as bench.py averages them): per launch, DRAM traffic
+# (dram__bytes_read.sum + dram__bytes_write.sum) and issued warp
+# instructions (smsp__inst_issued.sum).  A kernel changed since its capture
+# has no entry.
+NCU_CAPTURE = "profiles/ncu_kernels_1080p_1m.md"
 NCU_TRAFFIC = {
-    "k_raster_small": (33614848, "profiles/ncu_kernels_1080p_1m.md"),
-    "k_raster_small_alpha": (13604608, "profiles/ncu_kernels_1080p_1m.md"),
-    "k_shadow_raster": (48411392 + 18432, "profiles/ncu_kernels_1080p_1m.md"),
-    "k_shadow_raster_alpha": (10116608, "profiles/ncu_kernels_1080p_1m.md"),
+    "k_raster_small": 33619712,
+    "k_raster_small_alpha": 13611264,
+    "k_shadow_raster": (48455936 + 51622656) // 2,
+    "k_shadow_raster_alpha": (10654464 + 4552192) // 2,
+    "k_shade": 35126016,
+    "k_raster_tiled_alpha": 8156672,
 }
+NCU_ISSUED = {
+    "k_raster_small": 162938857,
+    "k_raster_small_alpha": 99548185,
+    "k_shadow_raster": (278526089 + 185207050) // 2,
+    "k_shadow_raster_alpha": (56262372 + 28985298) // 2,
+    "k_shade": 95340569,
+    "k_raster_tiled_alpha": 48432233,
+}
+ISSUE_PER_SM_PER_CLK = 4     # warp instructions: one per scheduler (4 per SM) per cycle
 
 
 def progress(msg):
@@ -154,17 +169,31 @@ def algorithmic_bytes(scene, q, shadow_q, visible_tris):
     }
 
 
-def roofline_of(kernel, ktimes, alg, hbm, peak_kind, steps):
+def issue_of(kernel, avg_s, sms, sm_mhz):
+    """The instruction-issue roofline of a kernel: its issued warp
+    instructions per launch (ncu) / its CUDA-event launch time, against
+    sms x 4 schedulers x the SM clock sampled during the run."""
+    n = NCU_ISSUED.get(kernel)
+    if n is None or not avg_s:
+        return None
+    peak = sms * ISSUE_PER_SM_PER_CLK * sm_mhz * 1e6
+    return {"warp_inst_per_launch": n, "achieved_winst_per_s": n / avg_s, "peak_winst_per_s": peak,
+            "frac": n / avg_s / peak, "sm_mhz": sm_mhz, "capture": NCU_CAPTURE}
+
+
+def roofline_of(kernel, ktimes, alg, hbm, peak_kind, steps, sms=148, sm_mhz=1965.0):
     """achieved = the kernel's algorithmic bytes per launch / its average
-    CUDA-event launch time; frac against the measured HBM peak."""
+    CUDA-event launch time; frac against the measured HBM peak.  `issue`
+    is the same launch against the instruction-issue peak."""
     ms, n = ktimes[kernel]
     avg_s = ms / n / 1000.0
     a = alg.get(kernel, 0)
     achieved = a / avg_s / 1e9
+    t = NCU_TRAFFIC.get(kernel)
     return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "peak_source": peak_kind, "traffic": NCU_TRAFFIC.get(kernel, (None,))[0],
-            "traffic_capture": NCU_TRAFFIC.get(kernel, (None, None))[1], "algorithmic_bytes": a,
-            "avg_us": 1e6 * avg_s, "launches_per_frame": n / steps}
+            "frac": achieved / hbm, "peak_source": peak_kind, "traffic": t,
+            "traffic_capture": NCU_CAPTURE if t is not None else None, "algorithmic_bytes": a,
+            "avg_us": 1e6 * avg_s, "launches_per_frame": n / steps, "issue": issue_of(kernel, avg_s, sms, sm_mhz)}
 
 
 def frame_bytes(scene):
@@ -885,10 +914,16 @@ def main():
         if k in alg:
             per_kernel[k]["frac_of_hbm"] = alg[k] / (ms / n / 1000.0) / 1e9 / hbm
     # the dominant kernel by its share of the frame, and by its time per launch
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = clk["sm_mhz"] if clk else 1965.0
+    for k, (ms, n) in ktimes.items():
+        iss = issue_of(k, ms / n / 1000.0, sms, sm_mhz)
+        if iss:
+            per_kernel[k]["issue_frac"] = iss["frac"]
     dom = max(ktimes.items(), key=lambda kv: kv[1][0])[0]
     dom_launch = max(ktimes.items(), key=lambda kv: kv[1][0] / kv[1][1])[0]
-    roofline = roofline_of(dom, ktimes, alg, hbm, peak_kind, args.steps)
-    roofline["by_launch"] = roofline_of(dom_launch, ktimes, alg, hbm, peak_kind, args.steps)
+    roofline = roofline_of(dom, ktimes, alg, hbm, peak_kind, args.steps, sms, sm_mhz)
+    roofline["by_launch"] = roofline_of(dom_launch, ktimes, alg, hbm, peak_kind, args.steps, sms, sm_mhz)
     fb = frame_bytes(scene)
     frame_roof = {"bytes": fb, "achieved_gbs": fb / (t_ms / args.steps / 1000.0) / 1e9}
     frame_roof["frac"] = frame_roof["achieved_gbs"] / hbm

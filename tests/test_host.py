@@ -33,6 +33,23 @@ def test_frame_bytes_formula():
     assert 268e6 < want < 270e6
 
 
+def test_issue_roofline():
+    """The instruction-issue roofline: issued warp instructions per launch
+    (from the ncu capture) / launch time, against SMs x 4 schedulers x the
+    sampled SM clock; kernels without a captured count get none."""
+    import bench
+    n = bench.NCU_ISSUED["k_shadow_raster"]
+    r = bench.issue_of("k_shadow_raster", 250e-6, 148, 1965.0)
+    assert r["warp_inst_per_launch"] == n
+    assert r["peak_winst_per_s"] == 148 * 4 * 1965e6
+    assert abs(r["frac"] - n / 250e-6 / (148 * 4 * 1965e6)) < 1e-12
+    assert 0.5 < r["frac"] < 1.0
+    assert bench.issue_of("k_clear_shadow", 10e-6, 148, 1965.0) is None
+    roof = bench.roofline_of("k_shade", {"k_shade": (2.0, 10)}, {"k_shade": 50e6}, 6500.0, "measured", 10)
+    assert abs(roof["avg_us"] - 200.0) < 1e-9 and abs(roof["achieved"] - 250.0) < 1e-9
+    assert roof["traffic"] == bench.NCU_TRAFFIC["k_shade"] and roof["issue"]["frac"] > 0
+
+
 def test_camera_bases_orthonormal():
     for a, b in ((0.3, 0.2), (1.7 * math.pi, 0.52), (-2.0, -0.7)):
         for m in (S.camera_basis(a, b), S.view_mat(a, b)):
