@@ -553,6 +553,36 @@ __global__ void k_vert_light(const float *__restrict__ xyz, const float *__restr
 
 // one thread per triangle of every enabled group; lists hold global ids.
 // `first`/`step` give the block's grid-stride over the triangles.
+// One reservation per block and counter in a grid-stride loop that every
+// thread of the block runs in step: warp w's totals v[k] (the same in all
+// its lanes) become offsets out[k] into the counters ctr[idx[k]].  The
+// counters are the same few addresses for the whole launch, so one
+// atomicAdd per block instead of one per warp keeps them from serialising.
+template <int K>
+__device__ __forceinline__ void block_reserve(const uint32_t (&v)[K], const int (&idx)[K], uint32_t *ctr,
+                                              uint32_t (&out)[K]) {
+  __shared__ uint32_t part[32][K];
+  __shared__ uint32_t base[K];
+  const int w = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) part[w][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < K) {
+    const int k = threadIdx.x;
+    uint32_t run = 0;
+    for (int i = 0; i < nw; i++) {
+      uint32_t x = part[i][k];
+      part[i][k] = run;
+      run += x;
+    }
+    base[k] = run ? atomicAdd(&ctr[idx[k]], run) : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) out[k] = base[k] + part[w][k];
+}
+
 __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev *sg, int first, int step) {
   int lane = threadIdx.x & 31;
   for (int base = first; base < P.total_tris; base += step) {
@@ -585,20 +615,6 @@ __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev 
     }
     unsigned ms = __ballot_sync(FULL, cls == 1 && !alpha), ma = __ballot_sync(FULL, cls == 1 && alpha);
     unsigned ml = __ballot_sync(FULL, cls == 2);
-    uint32_t bs = 0, ba = 0, bl = 0;
-    if (lane == 0) {
-      if (ms) bs = atomicAdd(&P.ctr[CTR_SMALL], __popc(ms));
-      if (ma) ba = atomicAdd(&P.ctr[CTR_SMALL_A], __popc(ma));
-      if (ml) bl = atomicAdd(&P.ctr[CTR_LARGE], __popc(ml));
-    }
-    bs = __shfl_sync(FULL, bs, 0);
-    ba = __shfl_sync(FULL, ba, 0);
-    bl = __shfl_sync(FULL, bl, 0);
-    unsigned lt = (1u << lane) - 1;
-    uint32_t pos = 0;
-    if (cls == 1 && !alpha) { pos = bs + __popc(ms & lt); P.small_list[pos] = (uint32_t)t; }
-    if (cls == 1 && alpha) { pos = ba + __popc(ma & lt); P.small_list[P.cap_list - 1 - pos] = (uint32_t)t; }
-    if (cls == 2) P.large_list[bl + __popc(ml & lt)] = (uint32_t)t;
     // row chunks of the small triangles
     int nch = 0;
     if (cls == 1) {
@@ -615,13 +631,17 @@ __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev 
       if (lane >= o) { io += v; ia += va; }
     }
     uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
-    uint32_t oo = 0, oa = 0;
-    if (lane == 31) {
-      if (to) oo = atomicAdd(&P.ctr[CTR_ITEMS], to);
-      if (ta) oa = atomicAdd(&P.ctr[CTR_ITEMS_A], ta);
-    }
-    oo = __shfl_sync(FULL, oo, 31) + (uint32_t)(io - co);
-    oa = __shfl_sync(FULL, oa, 31) + (uint32_t)(ia - ca);
+    const uint32_t want[5] = {(uint32_t)__popc(ms), (uint32_t)__popc(ma), (uint32_t)__popc(ml), to, ta};
+    const int idx[5] = {CTR_SMALL, CTR_SMALL_A, CTR_LARGE, CTR_ITEMS, CTR_ITEMS_A};
+    uint32_t got[5];
+    block_reserve<5>(want, idx, P.ctr, got);
+    uint32_t bs = got[0], ba = got[1], bl = got[2];
+    unsigned lt = (1u << lane) - 1;
+    uint32_t pos = 0;
+    if (cls == 1 && !alpha) { pos = bs + __popc(ms & lt); P.small_list[pos] = (uint32_t)t; }
+    if (cls == 1 && alpha) { pos = ba + __popc(ma & lt); P.small_list[P.cap_list - 1 - pos] = (uint32_t)t; }
+    if (cls == 2) P.large_list[bl + __popc(ml & lt)] = (uint32_t)t;
+    uint32_t oo = got[3] + (uint32_t)(io - co), oa = got[4] + (uint32_t)(ia - ca);
     uint32_t cap_items = P.cap_list * MAX_CHUNKS;
     for (int c = 0; c < nch; c++) {
       uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
@@ -1889,22 +1909,9 @@ __device__ __forceinline__ void shadow_classify(const GroupDev *sg, const Shadow
 __device__ __forceinline__ uint32_t shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int rows,
                                                   int lane) {
   unsigned mo = __ballot_sync(FULL, ok && !alpha), ma = __ballot_sync(FULL, ok && alpha);
-  uint32_t bo = 0, ba = 0;
-  if (lane == 0) {
-    if (mo) bo = atomicAdd(&S.ctr[CTR_SH_LIST], __popc(mo));
-    if (ma) ba = atomicAdd(&S.ctr[CTR_SH_LIST_A], __popc(ma));
-  }
-  bo = __shfl_sync(FULL, bo, 0);
-  ba = __shfl_sync(FULL, ba, 0);
-  unsigned lt = (1u << lane) - 1;
-  uint32_t pos = 0;
-  if (ok && !alpha) { pos = bo + __popc(mo & lt); S.list[pos] = (uint32_t)t; }
-  if (ok && alpha) { pos = ba + __popc(ma & lt); S.list[S.cap_list - 1 - pos] = (uint32_t)t; }
-  uint32_t slot = alpha ? S.cap_list - 1 - pos : pos;
-  if (!S.items) return slot;
   // row chunks of the casters, as for the small triangles of the view
   int nch = 0;
-  if (ok) {
+  if (ok && S.items) {
     int cl = chunk_len(rows, shadow_min_chunk(S, alpha));
     nch = (rows + cl - 1) / cl;
   }
@@ -1916,13 +1923,17 @@ __device__ __forceinline__ uint32_t shadow_append(const ShadowParams &S, int t, 
     if (lane >= o) { io += v; ia += va; }
   }
   uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
-  uint32_t oo = 0, oa = 0;
-  if (lane == 31) {
-    if (to) oo = atomicAdd(&S.ctr[CTR_SH_ITEMS], to);
-    if (ta) oa = atomicAdd(&S.ctr[CTR_SH_ITEMS_A], ta);
-  }
-  oo = __shfl_sync(FULL, oo, 31) + (uint32_t)(io - co);
-  oa = __shfl_sync(FULL, oa, 31) + (uint32_t)(ia - ca);
+  const uint32_t want[4] = {(uint32_t)__popc(mo), (uint32_t)__popc(ma), to, ta};
+  const int idx[4] = {CTR_SH_LIST, CTR_SH_LIST_A, CTR_SH_ITEMS, CTR_SH_ITEMS_A};
+  uint32_t got[4];
+  block_reserve<4>(want, idx, S.ctr, got);
+  unsigned lt = (1u << lane) - 1;
+  uint32_t pos = 0;
+  if (ok && !alpha) { pos = got[0] + __popc(mo & lt); S.list[pos] = (uint32_t)t; }
+  if (ok && alpha) { pos = got[1] + __popc(ma & lt); S.list[S.cap_list - 1 - pos] = (uint32_t)t; }
+  uint32_t slot = alpha ? S.cap_list - 1 - pos : pos;
+  if (!S.items) return slot;
+  uint32_t oo = got[2] + (uint32_t)(io - co), oa = got[3] + (uint32_t)(ia - ca);
   uint32_t cap_items = S.cap_list * MAX_CHUNKS;
   for (int c = 0; c < nch; c++) {
     uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
