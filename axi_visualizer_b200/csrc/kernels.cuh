@@ -64,6 +64,7 @@ enum {
 // which the host reports as an error.
 constexpr int LOOP_LIMIT = 1 << 16;
 
+
 // ------------------------------------------------------------ helpers
 
 __device__ __forceinline__ int find_group(const GroupDev *__restrict__ gs, int ng, uint32_t gtri) {
@@ -707,10 +708,52 @@ __device__ __forceinline__ void fill_windows(int total, int cnt, int pre, int la
   }
 }
 
+// fill_windows for a pixel function in two stages: first(span, p) issues
+// the pixel's dependent load and returns a state, second(state) consumes
+// it.  Window k's second stage runs after window k + 1's first, so the
+// load's latency overlaps the next window's lookup and arithmetic.
+template <class St, class F1, class F2>
+__device__ __forceinline__ void fill_windows2(int total, int cnt, int pre, int lane, const int *r2l, F1 &&first,
+                                              F2 &&second) {
+  const unsigned upto = 0xffffffffu >> (31 - lane);
+  St cur;
+  bool have = false;
+  for (int base = 0; base < total; base += 32) {
+    int rel = pre - base;
+    unsigned bit = (cnt > 0 && (unsigned)rel < 32u) ? (1u << rel) : 0u;
+    unsigned starts = __reduce_or_sync(FULL, bit);
+    int before = __popc(__ballot_sync(FULL, cnt > 0 && rel < 0));
+    int p = base + lane;
+    St nxt;
+    bool hn = p < total;
+    if (hn) nxt = first(r2l[before + __popc(starts & upto) - 1], p);
+    if (have) second(cur);
+    cur = nxt;
+    have = hn;
+  }
+  if (have) second(cur);
+}
+
 // One round of a span queue: numbering, the record's second half written
 // with its address and x made relative to the span's first pixel number
 // (the emitter keeps `pb` in registers until the numbering is known), then
 // the pixel-parallel fill.
+template <class Q, class F>
+__device__ __forceinline__ void fill_round(Q &q, int lane, int cnt, float4 pb, F &&pix);
+template <class St, class Q, class F1, class F2>
+__device__ __forceinline__ void fill_round2(Q &q, int lane, int cnt, float4 pb, F1 &&first, F2 &&second) {
+  int pre;
+  int total = fill_prepare(cnt, lane, q.r2l, pre);
+  if (total == 0) return;
+  if (cnt) {
+    pb.y = __int_as_float(__float_as_int(pb.y) - pre);
+    pb.z = __int_as_float(__float_as_int(pb.z) - pre);
+    q.b[lane] = pb;
+  }
+  __syncwarp();
+  fill_windows2<St>(total, cnt, pre, lane, q.r2l, first, second);
+  __syncwarp();
+}
 template <class Q, class F>
 __device__ __forceinline__ void fill_round(Q &q, int lane, int cnt, float4 pb, F &&pix) {
   int pre;
@@ -768,6 +811,46 @@ __device__ __forceinline__ void vis_pixel(const DrawParams &P, const GroupDev *s
             (unsigned long long)frag_key(tz, __float_as_uint(b.w)));
 }
 
+// vis_pixel<true> in two stages for fill_windows2: the first stage takes
+// the depth, the alpha footprint's weights and the order key, and issues
+// the load of the packed mask quad; the second tests the bilinear alpha
+// and resolves the visibility word.
+struct AlphaFrag {
+  unsigned long long key;
+  uint32_t addr;
+  unsigned m;          // the packed 2 x 2 mask quad (loaded in stage one)
+  float r1, r2;        // bilinear fractions
+  bool live;
+};
+__device__ __forceinline__ AlphaFrag vis_alpha_first(const DrawParams &P, const GroupDev *sg, const VisQ<true> &q,
+                                                     int s, int p) {
+  AlphaFrag f;
+  const float4 a = q.a[s], b = q.b[s];
+  float n = (float)(p + __float_as_int(b.z)) - a.x;
+  float t = span_t(n, a.y, a.z);
+  float tz = __frcp_rn((1 - t) * b.x + t * a.w);
+  f.live = tz == tz;
+  const float4 c = q.c[s];
+  const GroupDev &G = sg[q.g[s]];
+  float omt = 1 - t;
+  V2 uvi{omt * c.z + t * c.x, omt * c.w + t * c.y};
+  Taps tp = make_taps(uvi, tz, G.alen, 0);
+  f.m = f.live ? (unsigned)__ldg(G.aquad + tp.tex) : 0u;
+  f.r1 = tp.texr1;
+  f.r2 = tp.texr2;
+  f.key = frag_key(tz, __float_as_uint(b.w));
+  f.addr = (uint32_t)(p + __float_as_int(b.y));
+  return f;
+}
+__device__ __forceinline__ void vis_alpha_second(const DrawParams &P, const AlphaFrag &f) {
+  if (!f.live) return;
+  float i1 = 1 - f.r1, i2 = 1 - f.r2;
+  float ca = i1 * i2 * (float)(f.m & 1) + f.r1 * i2 * (float)((f.m >> 1) & 1) + i1 * f.r2 * (float)((f.m >> 2) & 1) +
+             f.r1 * f.r2 * (float)((f.m >> 3) & 1);
+  if (!(ca > 0.5f)) return;
+  atomicMin((unsigned long long *)&P.keys[f.addr], f.key);
+}
+
 // The lane's own span record, drawn by the lane alone with the true division.
 template <bool ALPHA>
 __device__ __forceinline__ void vis_serial(const DrawParams &P, const GroupDev *sg, const VisQ<ALPHA> &q, int lane,
@@ -775,10 +858,17 @@ __device__ __forceinline__ void vis_serial(const DrawParams &P, const GroupDev *
   for (int j = 0; j < cnt; j++) vis_pixel<ALPHA, true>(P, sg, q, lane, j);
 }
 
-template <bool ALPHA>
+// PIPE: alpha-tested fragments through the two-stage pipeline (the small
+// triangles' raster: 407 -> 390 us in the 1080p frame; the tiled raster,
+// whose spans are at most 16 pixels, was 3 us slower with it).
+template <bool ALPHA, bool PIPE = false>
 __device__ __forceinline__ void vis_fill(const DrawParams &P, const GroupDev *sg, VisQ<ALPHA> &q, int lane, int cnt,
                                          float4 pb) {
-  fill_round(q, lane, cnt, pb, [&](int s, int p) { vis_pixel<ALPHA>(P, sg, q, s, p); });
+  if constexpr (ALPHA && PIPE)
+    fill_round2<AlphaFrag>(q, lane, cnt, pb, [&](int s, int p) { return vis_alpha_first(P, sg, q, s, p); },
+                           [&](const AlphaFrag &f) { vis_alpha_second(P, f); });
+  else
+    fill_round(q, lane, cnt, pb, [&](int s, int p) { vis_pixel<ALPHA>(P, sg, q, s, p); });
 }
 
 // ------------------------------------------------------------ small triangles
@@ -941,7 +1031,7 @@ __device__ __forceinline__ void raster_small_loop(const DrawParams &P, const Gro
       }
       int cnt = 0;
       if (live) cnt = L.emit(P, sg, q, lane, live);
-      vis_fill<ALPHA>(P, sg, q, lane, cnt, L.pb);
+      vis_fill<ALPHA, true>(P, sg, q, lane, cnt, L.pb);
     }
   }
 }
