@@ -45,7 +45,8 @@ FALLBACK_HBM_GBS = 6650.0
 NCU_CAPTURE = "profiles/ncu_kernels_1080p_1m.md"
 NCU_TRAFFIC = {
     "k_raster_small": 33619712,
-    "k_raster_small_alpha": 13611264,
+    "k_raster_small_alpha": 13612800,
+    "k_shadow_setup": (37623296 + 37645312) // 2,
     "k_shadow_raster": (48455936 + 51622656) // 2,
     "k_shadow_raster_alpha": (10654464 + 4552192) // 2,
     "k_shade": 35126016,
@@ -53,7 +54,8 @@ NCU_TRAFFIC = {
 }
 NCU_ISSUED = {
     "k_raster_small": 162938857,
-    "k_raster_small_alpha": 99548185,
+    "k_raster_small_alpha": 114658827,
+    "k_shadow_setup": (14254644 + 14389846) // 2,
     "k_shadow_raster": (278526089 + 185207050) // 2,
     "k_shadow_raster_alpha": (56262372 + 28985298) // 2,
     "k_shade": 95340569,
