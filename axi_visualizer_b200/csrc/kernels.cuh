@@ -584,6 +584,56 @@ __device__ __forceinline__ void block_reserve(const uint32_t (&v)[K], const int 
   for (int k = 0; k < K; k++) out[k] = base[k] + part[w][k];
 }
 
+// Writes the row-chunk work items of a block's triangles (or casters),
+// sorted by their row count, longest first, into one region per kind and
+// block (opaque items from the front of `items`, alpha-tested ones from the
+// back).  A warp of the raster claims 32 consecutive items, so sorted items
+// give it rows of about the same count, and fewer lanes idle while the
+// longest item of the claim finishes.  The raster's results do not depend
+// on the order.  Every thread of the block calls it in step; a thread adds
+// the nch items of its list entry `pos` (chunk c has min(cl, rows - c cl)
+// rows).
+constexpr int LEN_BUCKETS = 16;
+__device__ __forceinline__ void block_items(uint32_t *items, uint32_t cap_items, uint32_t *ctr, int ctr_o, int ctr_a,
+                                            uint32_t pos, bool alpha, int rows, int cl, int nch) {
+  __shared__ uint32_t hist[2][LEN_BUCKETS];
+  __shared__ uint32_t bbase[2];
+  for (int i = threadIdx.x; i < 2 * LEN_BUCKETS; i += blockDim.x) hist[i / LEN_BUCKETS][i % LEN_BUCKETS] = 0;
+  __syncthreads();
+  const int k = alpha ? 1 : 0;
+  uint32_t rk[MAX_CHUNKS];
+#pragma unroll
+  for (int c = 0; c < MAX_CHUNKS; c++) {
+    rk[c] = 0;
+    if (c < nch) {
+      int len = min(cl, rows - c * cl);
+      rk[c] = atomicAdd(&hist[k][LEN_BUCKETS - 1 - min(len, LEN_BUCKETS - 1)], 1u);   // bucket 0: the longest
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    uint32_t run = 0;
+    for (int b = 0; b < LEN_BUCKETS; b++) {
+      uint32_t x = hist[threadIdx.x][b];
+      hist[threadIdx.x][b] = run;
+      run += x;
+    }
+    bbase[threadIdx.x] = run ? atomicAdd(&ctr[threadIdx.x ? ctr_a : ctr_o], run) : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < MAX_CHUNKS; c++) {
+    if (c < nch) {
+      int len = min(cl, rows - c * cl);
+      uint32_t p = bbase[k] + hist[k][LEN_BUCKETS - 1 - min(len, LEN_BUCKETS - 1)] + rk[c];
+      uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
+      if (!alpha) items[p] = item;
+      else items[cap_items - 1 - p] = item;
+    }
+  }
+  __syncthreads();   // the next call reuses hist and bbase
+}
+
 __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev *sg, int first, int step) {
   int lane = threadIdx.x & 31;
   for (int base = first; base < P.total_tris; base += step) {
@@ -616,39 +666,24 @@ __device__ __forceinline__ void setup_phase(const DrawParams &P, const GroupDev 
     }
     unsigned ms = __ballot_sync(FULL, cls == 1 && !alpha), ma = __ballot_sync(FULL, cls == 1 && alpha);
     unsigned ml = __ballot_sync(FULL, cls == 2);
-    // row chunks of the small triangles
-    int nch = 0;
-    if (cls == 1) {
-      int y0 = min(iy0, min(iy1, iy2)), y3 = max(iy0, max(iy1, iy2));
-      int rows = small_rows(y0, y3);
-      int cl = chunk_len(rows, P.min_chunk);
-      nch = (rows + cl - 1) / cl;
-    }
-    int co = (cls == 1 && !alpha) ? nch : 0, ca = (cls == 1 && alpha) ? nch : 0;
-    int io = co, ia = ca;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(FULL, io, o), va = __shfl_up_sync(FULL, ia, o);
-      if (lane >= o) { io += v; ia += va; }
-    }
-    uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
-    const uint32_t want[5] = {(uint32_t)__popc(ms), (uint32_t)__popc(ma), (uint32_t)__popc(ml), to, ta};
-    const int idx[5] = {CTR_SMALL, CTR_SMALL_A, CTR_LARGE, CTR_ITEMS, CTR_ITEMS_A};
-    uint32_t got[5];
-    block_reserve<5>(want, idx, P.ctr, got);
-    uint32_t bs = got[0], ba = got[1], bl = got[2];
+    const uint32_t want[3] = {(uint32_t)__popc(ms), (uint32_t)__popc(ma), (uint32_t)__popc(ml)};
+    const int idx[3] = {CTR_SMALL, CTR_SMALL_A, CTR_LARGE};
+    uint32_t got[3];
+    block_reserve<3>(want, idx, P.ctr, got);
     unsigned lt = (1u << lane) - 1;
     uint32_t pos = 0;
-    if (cls == 1 && !alpha) { pos = bs + __popc(ms & lt); P.small_list[pos] = (uint32_t)t; }
-    if (cls == 1 && alpha) { pos = ba + __popc(ma & lt); P.small_list[P.cap_list - 1 - pos] = (uint32_t)t; }
-    if (cls == 2) P.large_list[bl + __popc(ml & lt)] = (uint32_t)t;
-    uint32_t oo = got[3] + (uint32_t)(io - co), oa = got[4] + (uint32_t)(ia - ca);
-    uint32_t cap_items = P.cap_list * MAX_CHUNKS;
-    for (int c = 0; c < nch; c++) {
-      uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
-      if (!alpha) P.items[oo + c] = item;
-      else P.items[cap_items - 1 - (oa + c)] = item;
+    if (cls == 1 && !alpha) { pos = got[0] + __popc(ms & lt); P.small_list[pos] = (uint32_t)t; }
+    if (cls == 1 && alpha) { pos = got[1] + __popc(ma & lt); P.small_list[P.cap_list - 1 - pos] = (uint32_t)t; }
+    if (cls == 2) P.large_list[got[2] + __popc(ml & lt)] = (uint32_t)t;
+    // row chunks of the small triangles
+    int rows = 0, cl = 1, nch = 0;
+    if (cls == 1) {
+      int y0 = min(iy0, min(iy1, iy2)), y3 = max(iy0, max(iy1, iy2));
+      rows = small_rows(y0, y3);
+      cl = chunk_len(rows, P.min_chunk);
+      nch = (rows + cl - 1) / cl;
     }
+    block_items(P.items, P.cap_list * MAX_CHUNKS, P.ctr, CTR_ITEMS, CTR_ITEMS_A, pos, alpha, rows, cl, nch);
   }
 }
 
@@ -1999,37 +2034,23 @@ __device__ __forceinline__ void shadow_classify(const GroupDev *sg, const Shadow
 __device__ __forceinline__ uint32_t shadow_append(const ShadowParams &S, int t, bool ok, bool alpha, int rows,
                                                   int lane) {
   unsigned mo = __ballot_sync(FULL, ok && !alpha), ma = __ballot_sync(FULL, ok && alpha);
-  // row chunks of the casters, as for the small triangles of the view
-  int nch = 0;
-  if (ok && S.items) {
-    int cl = chunk_len(rows, shadow_min_chunk(S, alpha));
-    nch = (rows + cl - 1) / cl;
-  }
-  int co = (ok && !alpha) ? nch : 0, ca = (ok && alpha) ? nch : 0;
-  int io = co, ia = ca;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int v = __shfl_up_sync(FULL, io, o), va = __shfl_up_sync(FULL, ia, o);
-    if (lane >= o) { io += v; ia += va; }
-  }
-  uint32_t to = (uint32_t)__shfl_sync(FULL, io, 31), ta = (uint32_t)__shfl_sync(FULL, ia, 31);
-  const uint32_t want[4] = {(uint32_t)__popc(mo), (uint32_t)__popc(ma), to, ta};
-  const int idx[4] = {CTR_SH_LIST, CTR_SH_LIST_A, CTR_SH_ITEMS, CTR_SH_ITEMS_A};
-  uint32_t got[4];
-  block_reserve<4>(want, idx, S.ctr, got);
+  const uint32_t want[2] = {(uint32_t)__popc(mo), (uint32_t)__popc(ma)};
+  const int idx[2] = {CTR_SH_LIST, CTR_SH_LIST_A};
+  uint32_t got[2];
+  block_reserve<2>(want, idx, S.ctr, got);
   unsigned lt = (1u << lane) - 1;
   uint32_t pos = 0;
   if (ok && !alpha) { pos = got[0] + __popc(mo & lt); S.list[pos] = (uint32_t)t; }
   if (ok && alpha) { pos = got[1] + __popc(ma & lt); S.list[S.cap_list - 1 - pos] = (uint32_t)t; }
   uint32_t slot = alpha ? S.cap_list - 1 - pos : pos;
   if (!S.items) return slot;
-  uint32_t oo = got[2] + (uint32_t)(io - co), oa = got[3] + (uint32_t)(ia - ca);
-  uint32_t cap_items = S.cap_list * MAX_CHUNKS;
-  for (int c = 0; c < nch; c++) {
-    uint32_t item = (pos << CHUNK_BITS) | (uint32_t)c;
-    if (!alpha) S.items[oo + c] = item;
-    else S.items[cap_items - 1 - (oa + c)] = item;
+  // row chunks of the casters, as for the small triangles of the view
+  int cl = 1, nch = 0;
+  if (ok) {
+    cl = chunk_len(rows, shadow_min_chunk(S, alpha));
+    nch = (rows + cl - 1) / cl;
   }
+  block_items(S.items, S.cap_list * MAX_CHUNKS, S.ctr, CTR_SH_ITEMS, CTR_SH_ITEMS_A, pos, alpha, rows, cl, nch);
   return slot;
 }
 
