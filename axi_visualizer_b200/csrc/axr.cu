@@ -1012,7 +1012,7 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
   if (c->total_tris > 0) {
     // visibility: opaque rasterizers on the main stream, alpha-tested ones
     // concurrently on a side stream (all of them atomicMin the same buffer)
-    launch(c, s, "k_setup", [&] { k_setup<<<grid_for(c, c->total_tris, 256, 16), 256, 0, s>>>(P); }); nk++;
+    launch(c, s, "k_setup", [&] { k_setup<<<grid_for(c, c->total_tris, SETUP_THREADS, 8), SETUP_THREADS, 0, s>>>(P); }); nk++;
     if (any_alpha) {
       CK(cudaEventRecord(c->ev_setup, s));
       CK(cudaStreamWaitEvent(sa, c->ev_setup, 0));
