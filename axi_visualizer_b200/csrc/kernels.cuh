@@ -1263,19 +1263,28 @@ struct TileLane {
     ybound = clampf_(y2, yMin, yMax);
     live_half = (y2 > yMin) && ((float)cy <= ybound);
   }
+  // The second half's slopes are computed at set-up (see ShadowLane), so
+  // that the lanes reaching the middle row during the walk do less while
+  // the others wait.
+  float hs1, hs2, hsz1, hsz2;
+  V2 hsu1, hsu2;
+  __device__ __forceinline__ void half1_slopes() {
+    float yd = 1.0f / (y3 - y2);
+    hs1 = (x3 - x2) * yd;
+    hs2 = (x3 - x4) * yd;
+    hsz1 = (z3 - z2) * yd;
+    hsz2 = (z3 - z4) * yd;
+    if (ALPHA) { hsu1 = mul2(neg2(sub2(uv2, uv3)), yd); hsu2 = mul2(neg2(sub2(uv4, uv3)), yd); }
+    if (hs1 < hs2) {
+      float t = hs1; hs1 = hs2; hs2 = t;
+      t = hsz1; hsz1 = hsz2; hsz2 = t;
+      if (ALPHA) { V2 tv = hsu1; hsu1 = hsu2; hsu2 = tv; }
+    }
+  }
   __device__ __forceinline__ void start_half1() {
     half = 1;
-    float yd = 1.0f / (y3 - y2);
-    s1 = (x3 - x2) * yd;
-    s2 = (x3 - x4) * yd;
-    sz1 = (z3 - z2) * yd;
-    sz2 = (z3 - z4) * yd;
-    if (ALPHA) { su1 = mul2(neg2(sub2(uv2, uv3)), yd); su2 = mul2(neg2(sub2(uv4, uv3)), yd); }
-    if (s1 < s2) {
-      float t = s1; s1 = s2; s2 = t;
-      t = sz1; sz1 = sz2; sz2 = t;
-      if (ALPHA) { V2 tv = su1; su1 = su2; su2 = tv; }
-    }
+    s1 = hs1; s2 = hs2; sz1 = hsz1; sz2 = hsz2;
+    if (ALPHA) { su1 = hsu1; su2 = hsu2; }
     cy = f2i(clampf_(y3, yMin, yMax));
     float dy = (float)cy - y3;
     cx1 = x3 + dy * s1; cx2 = x3 + dy * s2;
@@ -1324,6 +1333,7 @@ struct TileLane {
     xMax = ((float)tileX + 1.f) * 16.f - 1.f;
     yMin = (float)tileY * 16.f;
     yMax = ((float)tileY + 1.f) * 16.f - 1.f;
+    half1_slopes();
     start_half0();
     if (!live_half) start_half1();
     return live_half;
