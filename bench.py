@@ -44,22 +44,24 @@ FALLBACK_HBM_GBS = 6650.0
 # has no entry.
 NCU_CAPTURE = "profiles/ncu_kernels_1080p_1m.md"
 NCU_TRAFFIC = {
-    "k_raster_small": 33619712,
-    "k_raster_small_alpha": 13612800,
-    "k_shadow_setup": (37623296 + 37645312) // 2,
-    "k_shadow_raster": (48455936 + 51622656) // 2,
-    "k_shadow_raster_alpha": (10654464 + 4552192) // 2,
+    "k_raster_small": 33617664,
+    "k_raster_small_alpha": 13615872,
+    "k_shadow_raster": (48459776 + 52110336) // 2,
+    "k_shadow_raster_alpha": (10673152 + 4569600) // 2,
     "k_shade": 35126016,
-    "k_raster_tiled_alpha": 8156672,
+    "k_raster_tiled_alpha": 8154624,
+    "k_shadow_setup": (37651968 + 37644800) // 2,
+    "k_setup": 55719424,
 }
 NCU_ISSUED = {
-    "k_raster_small": 162938857,
-    "k_raster_small_alpha": 114658827,
-    "k_shadow_setup": (14254644 + 14389846) // 2,
-    "k_shadow_raster": (278526089 + 185207050) // 2,
-    "k_shadow_raster_alpha": (56262372 + 28985298) // 2,
+    "k_raster_small": 144542785,
+    "k_raster_small_alpha": 101457125,
+    "k_shadow_raster": (222796448 + 129703233) // 2,
+    "k_shadow_raster_alpha": (45585055 + 18893632) // 2,
     "k_shade": 95340569,
-    "k_raster_tiled_alpha": 48432233,
+    "k_raster_tiled_alpha": 47031883,
+    "k_shadow_setup": (16162323 + 16116092) // 2,
+    "k_setup": 16814245,
 }
 ISSUE_PER_SM_PER_CLK = 4     # warp instructions: one per scheduler (4 per SM) per cycle
 
