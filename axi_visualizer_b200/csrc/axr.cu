@@ -173,6 +173,10 @@ struct axr_ctx {
   // launch accounting and optional per-kernel CUDA-event timing
   int64_t launches = 0;
   int min_chunk = MIN_CHUNK;
+  // resident blocks per SM of the persistent rasterizers (their grids are
+  // one full wave): small opaque / alpha, tiled opaque / alpha, casters
+  // opaque / alpha
+  int occ[6] = {8, 6, 8, 6, 8, 6};
   int shadow_mode = 0;                       // 0: per caster; tiled shadow pass where the map allows it
                                              // (2: units front first, 1: as binned)
   int shadow_slice = 512;                    // units per block of a tile in the tiled pass
@@ -546,6 +550,16 @@ int axr_create(int w, int h, int device, axr_ctx **out) {
   axr_ctx *c = new axr_ctx();
   c->device = device; c->w = w; c->h = h;
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  {
+    const void *kern[6] = {(const void *)k_raster_small<false>, (const void *)k_raster_small<true>,
+                           (const void *)k_raster_tiled<false>, (const void *)k_raster_tiled<true>,
+                           (const void *)k_shadow_raster<false>, (const void *)k_shadow_raster<true>};
+    for (int k = 0; k < 6; k++) {
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern[k], 128, 0) == cudaSuccess && n > 0) c->occ[k] = n;
+      else cudaGetLastError();
+    }
+  }
   size_t n = (size_t)w * h;
   int rc = 0;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1016,16 +1030,16 @@ int axr_draw_all(axr_ctx *c, const int32_t *flags, const int32_t *alpha_index, c
     if (any_alpha) {
       CK(cudaEventRecord(c->ev_setup, s));
       CK(cudaStreamWaitEvent(sa, c->ev_setup, 0));
-      launch(c, sa, "k_raster_small_alpha", [&] { k_raster_small<true><<<c->sms * 6, 128, 0, sa>>>(P); }); nk++;
+      launch(c, sa, "k_raster_small_alpha", [&] { k_raster_small<true><<<c->sms * c->occ[1], 128, 0, sa>>>(P); }); nk++;
     }
-    launch(c, s, "k_raster_small", [&] { k_raster_small<false><<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
+    launch(c, s, "k_raster_small", [&] { k_raster_small<false><<<c->sms * c->occ[0], 128, 0, s>>>(P); }); nk++;
     launch(c, s, "k_coarse", [&] { k_coarse<<<c->sms * 4, 128, 0, s>>>(P); }); nk++;
     if (any_alpha) {
       CK(cudaEventRecord(c->ev_coarse, s));
       CK(cudaStreamWaitEvent(sa, c->ev_coarse, 0));
-      launch(c, sa, "k_raster_tiled_alpha", [&] { k_raster_tiled<true><<<c->sms * 6, 128, 0, sa>>>(P); }); nk++;
+      launch(c, sa, "k_raster_tiled_alpha", [&] { k_raster_tiled<true><<<c->sms * c->occ[3], 128, 0, sa>>>(P); }); nk++;
     }
-    launch(c, s, "k_raster_tiled", [&] { k_raster_tiled<false><<<c->sms * 8, 128, 0, s>>>(P); }); nk++;
+    launch(c, s, "k_raster_tiled", [&] { k_raster_tiled<false><<<c->sms * c->occ[2], 128, 0, s>>>(P); }); nk++;
     launch(c, s, "k_raster_tiled_fallback", [&] { k_raster_tiled_fallback<<<c->sms * 2, 128, 0, s>>>(P); }); nk++;
     if (any_alpha) {
       CK(cudaEventRecord(c->ev_alpha, sa));
@@ -1424,9 +1438,9 @@ int axr_shadow_map(axr_ctx *c, int i, const uint8_t *cast, const int32_t *flags,
     if (any_alpha)
       launch(c, st, "k_shadow_tiles_alpha", [&] { k_shadow_tiles<true><<<c->sms * 6, 128, 0, st>>>(S); });
   } else {
-    launch(c, st, "k_shadow_raster", [&] { k_shadow_raster<false><<<c->sms * 8, 128, 0, st>>>(S); });
+    launch(c, st, "k_shadow_raster", [&] { k_shadow_raster<false><<<c->sms * c->occ[4], 128, 0, st>>>(S); });
     if (any_alpha)
-      launch(c, st, "k_shadow_raster_alpha", [&] { k_shadow_raster<true><<<c->sms * 6, 128, 0, st>>>(S); });
+      launch(c, st, "k_shadow_raster_alpha", [&] { k_shadow_raster<true><<<c->sms * c->occ[5], 128, 0, st>>>(S); });
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(sm.ev_write, st));
