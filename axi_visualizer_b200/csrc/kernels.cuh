@@ -1947,8 +1947,12 @@ __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *
   if (tid == 0) sm.nent = 0;
   __syncthreads();
   int slot = 0;
-  if (valid) {
-    unsigned long long k = ((unsigned long long)ord << 32) | (uint32_t)cy;
+  // the lanes of a warp with the same (winner, row) -- often a whole row of
+  // the tile -- insert it once, through their first lane
+  unsigned long long k = valid ? (((unsigned long long)ord << 32) | (uint32_t)cy) : EMPTY;
+  const unsigned peers = __match_any_sync(FULL, k);
+  const int leader = __ffs(peers) - 1;
+  if (valid && (tid & 31) == leader) {
     uint32_t h = ((ord * 2654435761u) ^ ((uint32_t)cy * 40503u)) % NT;
     for (int i = 0; i < NT; i++) {       // at most NT keys: always finds a slot
       unsigned long long prev = atomicCAS(&sm.hkey[h], EMPTY, k);
@@ -1966,6 +1970,7 @@ __device__ __forceinline__ void shade_tile(const DrawParams &P, const GroupDev *
       h = (h + 1) % NT;
     }
   }
+  slot = __shfl_sync(FULL, slot, leader);
   __syncthreads();
   int ne = sm.nent;
   for (int j = tid; j < 2 * ne; j += NT) {   // two threads a pair, one edge chain each
