@@ -2521,10 +2521,11 @@ __device__ __forceinline__ void shadow_warp_loop(const ShadowParams &S, const Gr
   }
 }
 
-// The alpha-tested casters fit 7 blocks per SM in 72 registers without
-// spilling (84 -> 80 us per cascade against 6 blocks at 76 registers).
+// Blocks per SM: the opaque casters fit 9 in 56 registers and the
+// alpha-tested ones 7 in 72, neither spilling (204 -> 199 and 84 -> 80 us
+// per cascade against 8 and 6 blocks).
 template <bool ALPHA>
-__global__ void __launch_bounds__(128, ALPHA ? 7 : 8) k_shadow_raster(ShadowParams S) {
+__global__ void __launch_bounds__(128, ALPHA ? 7 : 9) k_shadow_raster(ShadowParams S) {
   __shared__ GroupDev sg[64];
   __shared__ ShadowQ<ALPHA> qs[4];
   for (int i = threadIdx.x; i < S.ngroups; i += blockDim.x) sg[i] = S.groups[i];
