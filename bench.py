@@ -46,8 +46,8 @@ NCU_CAPTURE = "profiles/ncu_kernels_1080p_1m.md"
 NCU_TRAFFIC = {
     "k_raster_small": 33623552,
     "k_raster_small_alpha": 13610240,
-    "k_shadow_raster": (48459776 + 52110336) // 2,
-    "k_shadow_raster_alpha": (10673152 + 4569600) // 2,
+    "k_shadow_raster": (48459520 + 52097024) // 2,
+    "k_shadow_raster_alpha": (10682368 + 4569856) // 2,
     "k_shade": 35214336,
     "k_raster_tiled_alpha": 8154624,
     "k_shadow_setup": (37651968 + 37644800) // 2,
@@ -56,8 +56,8 @@ NCU_TRAFFIC = {
 NCU_ISSUED = {
     "k_raster_small": 144550486,
     "k_raster_small_alpha": 101604329,
-    "k_shadow_raster": (222796448 + 129703233) // 2,
-    "k_shadow_raster_alpha": (45585055 + 18893632) // 2,
+    "k_shadow_raster": (224048127 + 130663712) // 2,
+    "k_shadow_raster_alpha": (48309342 + 21214830) // 2,
     "k_shade": 95960306,
     "k_raster_tiled_alpha": 47031883,
     "k_shadow_setup": (16162323 + 16116092) // 2,
