@@ -154,21 +154,30 @@ def test_api_errors_raise():
 
 
 def test_row_chunking_does_not_change_the_frame():
-    """Small triangles are cut into row chunks whose lanes replay the row
-    accumulation; every chunk size gives the same bits, on a scene with tall
-    small triangles and alpha-tested quads."""
+    """Small triangles and shadow casters are cut into row chunks (sorted by
+    length at setup, alpha-tested casters at half length) whose lanes replay
+    the row accumulation from the set-up slopes of both halves; every chunk
+    size gives the same bits -- frame, triangle ids and both cascades -- on a
+    scene with tall small triangles and alpha-tested quads, and the default
+    equals the oracle."""
     from axi_visualizer_b200.ops import SceneRenderer
     sc = S.scene_small(seed=5, flags=S.MIP | S.SHADOW, nquads=120)
     view = S.default_view(480, 272, pos=(0, 4, -14))
     R = SceneRenderer(sc, view.w, view.h)
-    R.shadow_pass()
     frames = []
-    for mc in (1, 4, 12, 16, 32, 256):
+    for mc in (12, 1, 2, 4, 16, 32, 256):
         R.draw._L.axr_set_tuning(R.draw._h, mc)
+        R.shadow_pass()
         R.set_view(view)
         R.draw.clearZBuffer()
         R.draw.drawAll(R.shaders, shadowIds=[0, 1])
-        frames.append([x.copy() for x in R.draw.getFrame()] + [R.draw.getIDs()[0]])
+        frames.append([x.copy() for x in R.draw.getFrame()] + [R.draw.getIDs()[0]] +
+                      [R.draw.getSHM(k) for k in range(len(sc.shadows))])
+    fr, smaps = O.render(sc, view)
+    for k, m in enumerate(smaps):
+        assert np.array_equal(frames[0][5 + k].view(np.uint32), m.view(np.uint32)), f"cascade {k}"
+    assert np.array_equal(frames[0][3].view(np.uint32), fr.db.view(np.uint32))
+    assert np.array_equal(frames[0][4], fr.tri_id)
     st = R.draw.lastStats()
     assert st["n_small"] > 0
     for f in frames[1:]:
