@@ -36,12 +36,12 @@ W, H = 1920, 1080
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# From the ncu capture summarised in profiles/ncu_kernels_1080p_1m.md (the
-# same frame, one launch per kernel, both cascades averaged for the shadow
-# kernels, as bench.py averages them): per launch, DRAM traffic
-# (dram__bytes_read.sum + dram__bytes_write.sum) and issued warp
-# instructions (smsp__inst_issued.sum).  A kernel changed since its capture
-# has no entry.
+# From one `ncu --set full` capture of this frame's kernels (one launch per
+# kernel; the two cascades averaged for the shadow kernels, as the per-kernel
+# event times are): per launch, DRAM traffic (dram__bytes_read.sum +
+# dram__bytes_write.sum) and issued warp instructions (smsp__inst_issued.sum).
+# A kernel whose code changed since its capture has no entry.  NCU_CAPTURE
+# names the committed summary of that capture, reported in the JSON line.
 NCU_CAPTURE = "profiles/ncu_kernels_1080p_1m.md"
 NCU_TRAFFIC = {
     "k_raster_small": 33623552,
